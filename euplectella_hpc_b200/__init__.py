@@ -1,0 +1,332 @@
+"""B200-native D3Q19 BGK lattice-Boltzmann time step for Euplectella_HPC.
+
+The product is the sm_100a shared library `_lib/libeup.so` with the C ABI of
+`include/eup.h`; this module is a thin ctypes mirror of that ABI used by the
+tests and the benchmark.  It never falls back to a CPU path: when the library
+is missing, importing raises, and every call that needs a GPU reports the
+library's error.
+
+Array conventions follow the reference (giacomofalcucci/Euplectella_HPC):
+populations are one numpy array of shape (19, n+2, m+2, l+2) -- the Fortran
+arrays a01..a19(0:l+1,0:m+1,0:n+1) of CODE/SRC/alloca.F90:94-132 stacked, last
+axis fastest -- and the solid mask is obs with shape (n, m, l), 1 = solid.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libeup.so")
+
+# Boundary flag codes (CODE/SRC/build.bcond.F90:11-17) and face order.
+PERIODIC, NOSLIP, LID, FREESLIP, INFLOW, OUTFLOW = range(6)
+FRONT, REAR, RIGHT, LEFT, UP, DOWN = range(6)
+# Precision modes.
+FP32, FP64, FP16_DEV, BF16_DEV = range(4)
+
+STATUS = {0: "EUP_OK", 1: "EUP_ERR_INVALID_ARG", 2: "EUP_ERR_CUDA", 3: "EUP_ERR_OOM", 4: "EUP_ERR_DIVERGED",
+          5: "EUP_ERR_UNSUPPORTED", 6: "EUP_ERR_IO", 7: "EUP_ERR_NO_DEVICE"}
+
+EXPORTED = [
+    "eup_abi_version", "eup_device_count", "eup_create", "eup_destroy", "eup_last_error", "eup_set_obstacles",
+    "eup_upload", "eup_download", "eup_step", "eup_step_profiled", "eup_synchronize", "eup_get_stream", "eup_get_launch_count",
+    "eup_get_itime", "eup_get_forces", "eup_get_force_series", "eup_get_cd_series", "eup_get_monitor",
+    "eup_get_probes", "eup_get_links", "eup_get_boundary_solid", "eup_read_obs_file", "eup_write_obs_file",
+    "eup_read_raw_state", "eup_write_raw_state", "eup_init_equilibrium", "eup_geometry_cylinder_z",
+    "eup_geometry_reticular_shell",
+]
+
+
+class EupError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class CConfig(ctypes.Structure):
+    _fields_ = [
+        ("lx", ctypes.c_int32), ("ly", ctypes.c_int32), ("lz", ctypes.c_int32),
+        ("bc", ctypes.c_int32 * 6),
+        ("svisc", ctypes.c_double), ("u0", ctypes.c_double), ("u_inflow", ctypes.c_double),
+        ("u00", ctypes.c_double),
+        ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("dev_scale", ctypes.c_double),
+        ("cd_rho0", ctypes.c_double), ("cd_uref", ctypes.c_double), ("cd_length", ctypes.c_double),
+        ("cd_span", ctypes.c_double),
+        ("series_capacity", ctypes.c_int64),
+    ]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python euplectella_hpc_b200/build.py` "
+                          "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    P19 = ctypes.c_void_p * 19
+    sig = {
+        "eup_abi_version": ([], i32), "eup_device_count": ([], i32),
+        "eup_create": ([ctypes.POINTER(CConfig), ctypes.POINTER(vp)], ctypes.c_int),
+        "eup_destroy": ([vp], ctypes.c_int), "eup_last_error": ([vp], ctypes.c_char_p),
+        "eup_set_obstacles": ([vp, vp], ctypes.c_int),
+        "eup_upload": ([vp, P19, i32, i64], ctypes.c_int), "eup_download": ([vp, P19, i32], ctypes.c_int),
+        "eup_step": ([vp, i32], ctypes.c_int), "eup_step_profiled": ([vp, i32, vp], ctypes.c_int),
+        "eup_synchronize": ([vp], ctypes.c_int), "eup_get_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
+        "eup_get_launch_count": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
+        "eup_get_itime": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
+        "eup_get_forces": ([vp, vp], ctypes.c_int),
+        "eup_get_force_series": ([vp, i64, i32, vp], ctypes.c_int),
+        "eup_get_cd_series": ([vp, i64, i32, vp], ctypes.c_int),
+        "eup_get_monitor": ([vp, vp], ctypes.c_int), "eup_get_probes": ([vp, i32, vp, vp], ctypes.c_int),
+        "eup_get_links": ([vp, vp], ctypes.c_int),
+        "eup_get_boundary_solid": ([vp, vp, i64, ctypes.POINTER(i64)], ctypes.c_int),
+        "eup_read_obs_file": ([ctypes.c_char_p, i32, i32, i32, vp, ctypes.POINTER(i64)], ctypes.c_int),
+        "eup_write_obs_file": ([ctypes.c_char_p, i32, i32, i32, vp], ctypes.c_int),
+        "eup_read_raw_state": ([ctypes.c_char_p, i32, i32, i32, i32, P19, ctypes.POINTER(i64)], ctypes.c_int),
+        "eup_write_raw_state": ([ctypes.c_char_p, i32, i32, i32, i32, P19, i64], ctypes.c_int),
+        "eup_init_equilibrium": ([i32, i32, i32, dbl, dbl, ctypes.c_uint64, i32, P19], ctypes.c_int),
+        "eup_geometry_cylinder_z": ([i32, i32, i32, dbl, dbl, dbl, vp], ctypes.c_int),
+        "eup_geometry_reticular_shell": ([i32, i32, i32, dbl, dbl, dbl, dbl, dbl, dbl, dbl, ctypes.c_uint64, vp],
+                                         ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    return L
+
+
+lib = _load()
+
+
+def _check(rc: int, handle=None):
+    if rc != 0:
+        raise EupError(rc, lib.eup_last_error(handle).decode(errors="replace"))
+
+
+def device_count() -> int:
+    return int(lib.eup_device_count())
+
+
+def _ptrs(arr: np.ndarray):
+    assert arr.ndim == 4 and arr.shape[0] == 19 and arr.flags["C_CONTIGUOUS"]
+    return (ctypes.c_void_p * 19)(*[arr[q].ctypes.data for q in range(19)])
+
+
+def _elem(arr: np.ndarray) -> int:
+    if arr.dtype == np.float32:
+        return 4
+    if arr.dtype == np.float64:
+        return 8
+    raise TypeError("populations must be float32 or float64")
+
+
+@dataclasses.dataclass
+class Config:
+    lx: int
+    ly: int
+    lz: int
+    bc: tuple = (OUTFLOW, INFLOW, FREESLIP, FREESLIP, PERIODIC, PERIODIC)
+    svisc: float = 0.01
+    u0: float = 0.0
+    u_inflow: float = 0.0
+    u00: float = 0.0
+    precision: int = FP32
+    device: int = 0
+    dev_scale: float = 0.0
+    cd_rho0: float = 1.0
+    cd_uref: float = 0.0
+    cd_length: float = 0.0
+    cd_span: float = 0.0
+    series_capacity: int = 0
+
+    def to_c(self) -> CConfig:
+        c = CConfig()
+        c.lx, c.ly, c.lz = self.lx, self.ly, self.lz
+        for f in range(6):
+            c.bc[f] = int(self.bc[f])
+        c.svisc, c.u0, c.u_inflow, c.u00 = self.svisc, self.u0, self.u_inflow, self.u00
+        c.precision, c.device, c.dev_scale = self.precision, self.device, self.dev_scale
+        c.cd_rho0, c.cd_uref, c.cd_length, c.cd_span = self.cd_rho0, self.cd_uref, self.cd_length, self.cd_span
+        c.series_capacity = self.series_capacity
+        return c
+
+
+class Solver:
+    """One lattice on one GPU: the Python face of an eup_handle."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        _check(lib.eup_create(ctypes.byref(cfg.to_c()), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib.eup_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        _check(rc, self._h)
+
+    @property
+    def shape(self):
+        return (19, self.cfg.lz + 2, self.cfg.ly + 2, self.cfg.lx + 2)
+
+    def set_obstacles(self, obs: np.ndarray):
+        obs = np.ascontiguousarray(obs, dtype=np.int32)
+        assert obs.shape == (self.cfg.lz, self.cfg.ly, self.cfg.lx)
+        self._ck(lib.eup_set_obstacles(self._h, obs.ctypes.data))
+
+    def upload(self, pops: np.ndarray, itime: int = 0):
+        pops = np.ascontiguousarray(pops)
+        assert pops.shape == self.shape
+        self._ck(lib.eup_upload(self._h, _ptrs(pops), _elem(pops), itime))
+
+    def upload_ptrs(self, ptrs, elem_bytes: int, itime: int = 0):
+        """Upload from 19 raw host pointers (e.g. pinned torch tensors)."""
+        self._ck(lib.eup_upload(self._h, (ctypes.c_void_p * 19)(*ptrs), elem_bytes, itime))
+
+    def download(self, dtype=np.float32) -> np.ndarray:
+        out = np.empty(self.shape, dtype=dtype)
+        self._ck(lib.eup_download(self._h, _ptrs(out), _elem(out)))
+        return out
+
+    def download_ptrs(self, ptrs, elem_bytes: int):
+        self._ck(lib.eup_download(self._h, (ctypes.c_void_p * 19)(*ptrs), elem_bytes))
+
+    def step(self, nsteps: int = 1):
+        self._ck(lib.eup_step(self._h, nsteps))
+
+    def step_profiled(self, nsteps: int) -> np.ndarray:
+        ms = np.zeros(4, dtype=np.float64)
+        self._ck(lib.eup_step_profiled(self._h, nsteps, ms.ctypes.data))
+        return ms
+
+    def synchronize(self):
+        self._ck(lib.eup_synchronize(self._h))
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._ck(lib.eup_get_stream(self._h, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    @property
+    def launches(self) -> int:
+        """Kernels launched so far by the time-step entry points."""
+        t = ctypes.c_int64()
+        self._ck(lib.eup_get_launch_count(self._h, ctypes.byref(t)))
+        return int(t.value)
+
+    @property
+    def itime(self) -> int:
+        t = ctypes.c_int64()
+        self._ck(lib.eup_get_itime(self._h, ctypes.byref(t)))
+        return int(t.value)
+
+    def forces(self) -> np.ndarray:
+        out = np.zeros(3, dtype=np.float64)
+        self._ck(lib.eup_get_forces(self._h, out.ctypes.data))
+        return out
+
+    def force_series(self, first: int, count: int) -> np.ndarray:
+        out = np.zeros((count, 3), dtype=np.float64)
+        self._ck(lib.eup_get_force_series(self._h, first, count, out.ctypes.data))
+        return out
+
+    def cd_series(self, first: int, count: int) -> np.ndarray:
+        out = np.zeros(count, dtype=np.float64)
+        self._ck(lib.eup_get_cd_series(self._h, first, count, out.ctypes.data))
+        return out
+
+    def monitor(self) -> np.ndarray:
+        out = np.zeros(5, dtype=np.float64)
+        self._ck(lib.eup_get_monitor(self._h, out.ctypes.data))
+        return out
+
+    def probes(self, ijk) -> np.ndarray:
+        ijk = np.ascontiguousarray(np.asarray(ijk, dtype=np.int32).reshape(-1, 3))
+        out = np.zeros((ijk.shape[0], 4), dtype=np.float64)
+        self._ck(lib.eup_get_probes(self._h, ijk.shape[0], ijk.ctypes.data, out.ctypes.data))
+        return out
+
+    def links(self) -> np.ndarray:
+        out = np.zeros((self.cfg.lz, self.cfg.ly, self.cfg.lx), dtype=np.uint32)
+        self._ck(lib.eup_get_links(self._h, out.ctypes.data))
+        return out
+
+    def boundary_solid(self) -> np.ndarray:
+        cnt = ctypes.c_int64()
+        self._ck(lib.eup_get_boundary_solid(self._h, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(max(cnt.value, 1), dtype=np.int64)
+        self._ck(lib.eup_get_boundary_solid(self._h, out.ctypes.data, cnt.value, ctypes.byref(cnt)))
+        return out[:cnt.value]
+
+
+# ---- host utilities ------------------------------------------------------------
+
+def init_equilibrium(l, m, n, u_in, amp, seed, dtype=np.float32) -> np.ndarray:
+    """Synthetic initial state: equilibrium at rho=1, u = inlet + seeded perturbation, halos included."""
+    out = np.empty((19, n + 2, m + 2, l + 2), dtype=dtype)
+    _check(lib.eup_init_equilibrium(l, m, n, float(u_in), float(amp), int(seed), _elem(out), _ptrs(out)))
+    return out
+
+
+def read_obs_file(path, l, m, n):
+    obs = np.zeros((n, m, l), dtype=np.int32)
+    cnt = ctypes.c_int64()
+    _check(lib.eup_read_obs_file(os.fsencode(path), l, m, n, obs.ctypes.data, ctypes.byref(cnt)))
+    return obs, int(cnt.value)
+
+
+def write_obs_file(path, obs: np.ndarray):
+    obs = np.ascontiguousarray(obs, dtype=np.int32)
+    n, m, l = obs.shape
+    _check(lib.eup_write_obs_file(os.fsencode(path), l, m, n, obs.ctypes.data))
+
+
+def read_raw_state(path, l, m, n, dtype=np.float32):
+    out = np.empty((19, n + 2, m + 2, l + 2), dtype=dtype)
+    it = ctypes.c_int64()
+    _check(lib.eup_read_raw_state(os.fsencode(path), l, m, n, _elem(out), _ptrs(out), ctypes.byref(it)))
+    return out, int(it.value)
+
+
+def write_raw_state(path, pops: np.ndarray, itime: int):
+    pops = np.ascontiguousarray(pops)
+    _, n2, m2, l2 = pops.shape
+    _check(lib.eup_write_raw_state(os.fsencode(path), l2 - 2, m2 - 2, n2 - 2, _elem(pops), _ptrs(pops), itime))
+
+
+def geometry_cylinder_z(l, m, n, xc, yc, r) -> np.ndarray:
+    obs = np.zeros((n, m, l), dtype=np.int32)
+    _check(lib.eup_geometry_cylinder_z(l, m, n, float(xc), float(yc), float(r), obs.ctypes.data))
+    return obs
+
+
+def geometry_reticular_shell(l, m, n, x0, length, yc, zc, outer_d, strut_d, pitch, seed) -> np.ndarray:
+    obs = np.zeros((n, m, l), dtype=np.int32)
+    _check(lib.eup_geometry_reticular_shell(l, m, n, float(x0), float(length), float(yc), float(zc),
+                                            float(outer_d), float(strut_d), float(pitch), int(seed),
+                                            obs.ctypes.data))
+    return obs

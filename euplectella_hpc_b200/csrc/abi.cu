@@ -1,0 +1,560 @@
+// C ABI entry points (include/eup.h): handle life cycle, state transfer in the
+// reference's haloed layout, the time-step sequence and diagnostics.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/eup.h"
+#include "internal.h"
+
+using namespace eup;
+
+struct eup_handle {
+    eup_config cfg{};
+    Geo g{};
+    cudaStream_t stream = nullptr;
+    int prec = EUP_FP32;
+    size_t sbytes = 4, rbytes = 4;
+    int64_t Nq = 0;
+    void* lat[2] = {nullptr, nullptr};
+    void* ghost = nullptr;
+    int cur = 0;
+    uint32_t* bits = nullptr;
+    int wpr = 0;
+    int32_t* blist = nullptr;
+    int64_t nblist = 0;
+    double* partials = nullptr;
+    unsigned int* counter = nullptr;
+    double* series = nullptr;
+    int64_t cap = 0;
+    double* dscratch = nullptr;  // 64 doubles
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    int64_t itime = 0, series_first = 0;
+    bool has_state = false;
+    double scale = 1.0;
+    int variant = 0;
+    int64_t launches = 0;  // kernels launched by eup_step / eup_step_profiled
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(eup_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_err = msg;
+    return code;
+}
+
+int cuda_fail(eup_handle* h, cudaError_t e, const char* what) {
+    return fail(h, e == cudaErrorMemoryAllocation ? EUP_ERR_OOM : EUP_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define CK(h, call)                                      \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+bool face_flag_ok(int face, int f) {
+    switch (face) {
+        case EUP_FRONT: return f == 0 || f == 1 || f == 5;
+        case EUP_REAR: return f == 0 || f == 1 || f == 4;
+        case EUP_UP: return f == 0 || f == 1 || f == 2 || f == 3;
+        default: return f == 0 || f == 1 || f == 3;
+    }
+}
+
+template <typename S, typename R>
+Lat<S, R> make_lat(const eup_handle* h, int which) {
+    Lat<S, R> L;
+    char* base = static_cast<char*>(h->lat[which]);
+    for (int q = 0; q < Q; ++q) L.pop[q] = reinterpret_cast<S*>(base + (size_t)q * h->Nq * sizeof(S));
+    L.ghost = static_cast<R*>(h->ghost);
+    L.scale = (R)h->scale;
+    L.inv_scale = (R)(1.0 / h->scale);
+    return L;
+}
+
+template <typename R>
+Phys<R> make_phys(const eup_handle* h) {
+    // CODE/SRC/hencol.F90:30-39: svisc and u0 are real(mykind); omega from a
+    // double expression; fgrad = 4.0*u0*svisc/(5.0*real(n)*real(n)) in mykind.
+    Phys<R> ph;
+    const R sv = (R)h->cfg.svisc, u0 = (R)h->cfg.u0;
+    ph.omega = (R)(2.0 / (6.0 * (double)sv + 1.0));
+    ph.omega1 = R(1) - ph.omega;
+    ph.fgrad = R(4) * u0 * sv / (R(5) * (R)h->g.n * (R)h->g.n);
+    ph.u_inflow = (R)h->cfg.u_inflow;
+    ph.force = (R)((R)h->cfg.u00 / R(6));
+    return ph;
+}
+
+Mask make_mask(const eup_handle* h) { return Mask{h->bits, h->wpr}; }
+Reduce make_reduce(const eup_handle* h) { return Reduce{h->partials, h->counter, kReduceMaxBlocks}; }
+double* slot(const eup_handle* h, int64_t t) { return h->series + 3 * (t % h->cap); }
+
+template <typename S, typename R>
+void enqueue_drag_only(eup_handle* h) {
+    double* out = slot(h, h->itime);
+    if (h->nblist == 0) {
+        cudaMemsetAsync(out, 0, 3 * sizeof(double), h->stream);
+        return;
+    }
+    const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
+    launch_bounce_drag<S, R>(make_lat<S, R>(h, h->cur), h->g, make_mask(h), bc, h->blist, h->nblist, false,
+                             make_reduce(h), out, h->stream);
+}
+
+// Events bracketing the phases of each step when profiling: ev[4*s + p].
+struct PhaseEvents {
+    std::vector<cudaEvent_t> ev;
+    void mark(size_t idx, cudaStream_t st) {
+        if (idx < ev.size()) cudaEventRecord(ev[idx], st);
+    }
+};
+
+template <typename S, typename R>
+void enqueue_steps(eup_handle* h, int32_t nsteps, PhaseEvents* pe = nullptr) {
+    const Phys<R> ph = make_phys<R>(h);
+    const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
+    const Mask mk = make_mask(h);
+    const Reduce red = make_reduce(h);
+    for (int32_t s = 0; s < nsteps; ++s) {
+        const Lat<S, R> src = make_lat<S, R>(h, h->cur), dst = make_lat<S, R>(h, h->cur ^ 1);
+        if (pe) pe->mark(4 * (size_t)s + 0, h->stream);
+        // boundaries: bounce-back then halo planes (CODE/SRC/boundaries.F90:36-49,235-248)
+        if (h->nblist > 0) {
+            launch_bounce_drag<S, R>(src, h->g, mk, bc, h->blist, h->nblist, true, red, slot(h, h->itime),
+                                     h->stream);
+            h->launches += 1;
+        } else {
+            cudaMemsetAsync(slot(h, h->itime), 0, 3 * sizeof(double), h->stream);
+        }
+        if (pe) pe->mark(4 * (size_t)s + 1, h->stream);
+        h->launches += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
+        if (pe) pe->mark(4 * (size_t)s + 2, h->stream);
+        // propagation + collision (CODE/SRC/bgk3d.F90:133-138)
+        launch_stream_collide<S, R>(src, dst, h->g, ph, h->variant, h->stream);
+        h->launches += 1;
+        if (pe) pe->mark(4 * (size_t)s + 3, h->stream);
+        h->cur ^= 1;
+        h->itime += 1;
+    }
+    enqueue_drag_only<S, R>(h);
+    if (h->nblist > 0) h->launches += 1;
+}
+
+#define DISPATCH(h, FN, ...)                                                   \
+    do {                                                                       \
+        switch ((h)->prec) {                                                   \
+            case EUP_FP32: FN<float, float>(__VA_ARGS__); break;               \
+            case EUP_FP64: FN<double, double>(__VA_ARGS__); break;             \
+            case EUP_FP16_DEV: FN<__half, float>(__VA_ARGS__); break;          \
+            default: FN<__nv_bfloat16, float>(__VA_ARGS__); break;             \
+        }                                                                      \
+    } while (0)
+
+template <typename S, typename R, typename T>
+void enqueue_upload_q(eup_handle* h, int q) {
+    launch_scatter<S, R, T>(make_lat<S, R>(h, h->cur), h->g, q, static_cast<const T*>(h->staging), h->stream);
+}
+template <typename S, typename R, typename T>
+void enqueue_download_q(eup_handle* h, int q) {
+    launch_gather<S, R, T>(make_lat<S, R>(h, h->cur), h->g, q, static_cast<T*>(h->staging), h->stream);
+}
+template <typename S, typename R>
+void upload_q(eup_handle* h, int q, int eb) {
+    if (eb == 4) enqueue_upload_q<S, R, float>(h, q);
+    else enqueue_upload_q<S, R, double>(h, q);
+}
+template <typename S, typename R>
+void download_q(eup_handle* h, int q, int eb) {
+    if (eb == 4) enqueue_download_q<S, R, float>(h, q);
+    else enqueue_download_q<S, R, double>(h, q);
+}
+template <typename S, typename R>
+void monitor_dispatch(eup_handle* h) {
+    launch_monitor<S, R>(make_lat<S, R>(h, h->cur), h->g, make_mask(h), make_reduce(h), h->dscratch, h->stream);
+}
+template <typename S, typename R>
+void probes_dispatch(eup_handle* h, int npts, const int32_t* d_ijk, double* d_out) {
+    launch_probes<S, R>(make_lat<S, R>(h, h->cur), h->g, npts, d_ijk, d_out, h->stream);
+}
+
+int ensure_staging(eup_handle* h, size_t bytes) {
+    if (h->staging_bytes >= bytes) return EUP_OK;
+    if (h->staging) cudaFree(h->staging);
+    h->staging = nullptr;
+    h->staging_bytes = 0;
+    CK(h, cudaMalloc(&h->staging, bytes));
+    h->staging_bytes = bytes;
+    return EUP_OK;
+}
+
+int check_handle(eup_handle* h) {
+    if (!h) return fail(nullptr, EUP_ERR_INVALID_ARG, "null handle");
+    cudaError_t e = cudaSetDevice(h->cfg.device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+    return EUP_OK;
+}
+
+}  // namespace
+
+void eup_internal_set_error(const std::string& msg) { g_err = msg; }
+
+extern "C" {
+
+int32_t eup_abi_version(void) { return EUP_ABI_VERSION; }
+
+int32_t eup_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+const char* eup_last_error(const eup_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+int eup_create(const eup_config* cfg, eup_handle** out) {
+    if (!cfg || !out) return fail(nullptr, EUP_ERR_INVALID_ARG, "eup_create: null argument");
+    *out = nullptr;
+    if (cfg->lx < 1 || cfg->ly < 1 || cfg->lz < 1)
+        return fail(nullptr, EUP_ERR_INVALID_ARG, "eup_create: lattice sizes must be >= 1");
+    const int64_t N = (int64_t)cfg->lx * cfg->ly * cfg->lz;
+    if (N > 2147483647LL)
+        return fail(nullptr, EUP_ERR_UNSUPPORTED, "eup_create: more than 2^31-1 nodes on one GPU");
+    for (int f = 0; f < 6; ++f)
+        if (!face_flag_ok(f, cfg->bc[f]))
+            return fail(nullptr, EUP_ERR_UNSUPPORTED,
+                        "eup_create: boundary flag " + std::to_string(cfg->bc[f]) + " not defined for face " +
+                            std::to_string(f) + " (CODE/SRC/bcond.bc.F90 has no such block)");
+    if (cfg->precision < EUP_FP32 || cfg->precision > EUP_BF16_DEV)
+        return fail(nullptr, EUP_ERR_INVALID_ARG, "eup_create: unknown precision");
+    if (!(cfg->svisc > 0.0)) return fail(nullptr, EUP_ERR_INVALID_ARG, "eup_create: svisc must be > 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, EUP_ERR_NO_DEVICE, "eup_create: no CUDA device");
+    }
+    if (cfg->device < 0 || cfg->device >= ndev)
+        return fail(nullptr, EUP_ERR_INVALID_ARG, "eup_create: device ordinal out of range");
+
+    eup_handle* h = new eup_handle();
+    h->cfg = *cfg;
+    h->g.init(cfg->lx, cfg->ly, cfg->lz);
+    h->prec = cfg->precision;
+    h->sbytes = (h->prec == EUP_FP32) ? 4 : (h->prec == EUP_FP64) ? 8 : 2;
+    h->rbytes = (h->prec == EUP_FP64) ? 8 : 4;
+    h->scale = (h->prec == EUP_FP16_DEV || h->prec == EUP_BF16_DEV) ? (cfg->dev_scale > 0 ? cfg->dev_scale : 4096.0) : 1.0;
+    h->cap = cfg->series_capacity > 0 ? cfg->series_capacity : (int64_t)1 << 20;
+    h->Nq = (N + 127) / 128 * 128;
+    if (const char* v = std::getenv("EUP_STEP_VARIANT")) h->variant = std::atoi(v);
+
+    auto cleanup_fail = [&](int code) {
+        std::string m = h->err;
+        eup_destroy(h);
+        g_err = m;
+        return code;
+    };
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) return cleanup_fail(cuda_fail(h, e, "cudaSetDevice"));
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaStreamCreate"));
+    const size_t lat_bytes = (size_t)Q * h->Nq * h->sbytes;
+    for (int w = 0; w < 2; ++w) {
+        if ((e = cudaMalloc(&h->lat[w], lat_bytes)) != cudaSuccess)
+            return cleanup_fail(cuda_fail(h, e, "cudaMalloc(lattice)"));
+        cudaMemsetAsync(h->lat[w], 0, lat_bytes, h->stream);
+    }
+    const size_t ghost_bytes = (size_t)Q * h->g.G * h->rbytes;
+    if ((e = cudaMalloc(&h->ghost, ghost_bytes)) != cudaSuccess) return cleanup_fail(cuda_fail(h, e, "cudaMalloc(halo shell)"));
+    cudaMemsetAsync(h->ghost, 0, ghost_bytes, h->stream);
+    if ((e = cudaMalloc(&h->partials, sizeof(double) * kReduceMaxBlocks * kReduceWidth)) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMalloc(partials)"));
+    if ((e = cudaMalloc(&h->counter, sizeof(unsigned int))) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMalloc(counter)"));
+    cudaMemsetAsync(h->counter, 0, sizeof(unsigned int), h->stream);
+    if ((e = cudaMalloc(&h->series, sizeof(double) * 3 * h->cap)) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMalloc(force series)"));
+    cudaMemsetAsync(h->series, 0, sizeof(double) * 3 * h->cap, h->stream);
+    if ((e = cudaMalloc(&h->dscratch, sizeof(double) * 64)) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMalloc(scratch)"));
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cleanup_fail(cuda_fail(h, e, "create"));
+    *out = h;
+    return EUP_OK;
+}
+
+int eup_destroy(eup_handle* h) {
+    if (!h) return EUP_OK;
+    cudaSetDevice(h->cfg.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->partials, h->counter, h->series,
+                    h->dscratch, h->staging};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return EUP_OK;
+}
+
+int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!obs) return fail(h, EUP_ERR_INVALID_ARG, "eup_set_obstacles: null obs");
+    const Geo& g = h->g;
+    int64_t nsolid = 0;
+    for (int64_t t = 0; t < g.N; ++t) nsolid += (obs[t] == 1);
+    if (h->cfg.bc[EUP_FRONT] == EUP_BC_OUTFLOW) {
+        for (int64_t r = 0; r < (int64_t)g.m * g.n; ++r)
+            if (obs[r * g.l + (g.l - 1)] == 1)
+                return fail(h, EUP_ERR_UNSUPPORTED,
+                            "eup_set_obstacles: solid voxel on the outflow plane i=l; the reference's outflow "
+                            "there reads values whose order its bounce-back loop leaves undefined");
+    }
+    if (h->bits) { cudaFree(h->bits); h->bits = nullptr; }
+    if (h->blist) { cudaFree(h->blist); h->blist = nullptr; }
+    h->nblist = 0;
+    h->wpr = (g.l + 31) / 32;
+    if (nsolid > 0) {
+        int32_t* d_obs = nullptr;
+        uint8_t* d_flags = nullptr;
+        CK(h, cudaMalloc(&d_obs, sizeof(int32_t) * g.N));
+        CK(h, cudaMemcpyAsync(d_obs, obs, sizeof(int32_t) * g.N, cudaMemcpyHostToDevice, h->stream));
+        CK(h, cudaMalloc(&h->bits, sizeof(uint32_t) * (size_t)g.m * g.n * h->wpr));
+        launch_build_mask(d_obs, g, h->bits, h->wpr, h->stream);
+        CK(h, cudaMalloc(&d_flags, g.N));
+        launch_flag_boundary_solid(g, make_mask(h), d_flags, h->stream);
+        CK(h, cudaMalloc(&h->blist, sizeof(int32_t) * (size_t)(nsolid > 0 ? nsolid : 1)));
+        cudaError_t e;
+        const int64_t cnt = compact_flags(d_flags, g.N, h->blist, h->stream, &e);
+        cudaFree(d_flags);
+        cudaFree(d_obs);
+        if (e != cudaSuccess) return cuda_fail(h, e, "compact boundary solid list");
+        h->nblist = cnt;
+    }
+    if (h->has_state) DISPATCH(h, enqueue_drag_only, h);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
+int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, int64_t itime) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!pops || (elem_bytes != 4 && elem_bytes != 8))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_upload: pops must be 19 arrays of 4- or 8-byte reals");
+    for (int q = 0; q < Q; ++q)
+        if (!pops[q]) return fail(h, EUP_ERR_INVALID_ARG, "eup_upload: null population array");
+    const Geo& g = h->g;
+    const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * elem_bytes;
+    if ((rc = ensure_staging(h, bytes))) return rc;
+    for (int q = 0; q < Q; ++q) {
+        CK(h, cudaMemcpyAsync(h->staging, pops[q], bytes, cudaMemcpyHostToDevice, h->stream));
+        DISPATCH(h, upload_q, h, q, elem_bytes);
+    }
+    h->itime = itime;
+    h->series_first = itime;
+    h->has_state = true;
+    DISPATCH(h, enqueue_drag_only, h);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
+int eup_download(eup_handle* h, void* const pops[19], int32_t elem_bytes) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_download: no state uploaded");
+    if (!pops || (elem_bytes != 4 && elem_bytes != 8))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_download: pops must be 19 arrays of 4- or 8-byte reals");
+    for (int q = 0; q < Q; ++q)
+        if (!pops[q]) return fail(h, EUP_ERR_INVALID_ARG, "eup_download: null population array");
+    const Geo& g = h->g;
+    const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * elem_bytes;
+    if ((rc = ensure_staging(h, bytes))) return rc;
+    for (int q = 0; q < Q; ++q) {
+        DISPATCH(h, download_q, h, q, elem_bytes);
+        CK(h, cudaMemcpyAsync(pops[q], h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
+int eup_step(eup_handle* h, int32_t nsteps) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_step: no state uploaded");
+    if (nsteps < 0) return fail(h, EUP_ERR_INVALID_ARG, "eup_step: nsteps < 0");
+    if (nsteps == 0) return EUP_OK;
+    DISPATCH(h, enqueue_steps, h, nsteps);
+    CK(h, cudaGetLastError());
+    return EUP_OK;
+}
+
+int eup_step_profiled(eup_handle* h, int32_t nsteps, double ms[4]) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!ms) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_profiled: null ms");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_profiled: no state uploaded");
+    if (nsteps < 1) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_profiled: nsteps < 1");
+    PhaseEvents pe;
+    pe.ev.resize(4 * (size_t)nsteps + 1);
+    for (auto& e : pe.ev) CK(h, cudaEventCreate(&e));
+    DISPATCH(h, enqueue_steps, h, nsteps, &pe);
+    pe.mark(pe.ev.size() - 1, h->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) {
+        for (int32_t s = 0; s < nsteps; ++s)
+            for (int p = 0; p < 3; ++p) {
+                float t = 0.f;
+                cudaEventElapsedTime(&t, pe.ev[4 * (size_t)s + p], pe.ev[4 * (size_t)s + p + 1]);
+                ms[p] += t;
+            }
+        float tot = 0.f;
+        cudaEventElapsedTime(&tot, pe.ev[0], pe.ev.back());
+        ms[3] = tot;
+    }
+    for (auto& ev : pe.ev) cudaEventDestroy(ev);
+    if (e != cudaSuccess) return cuda_fail(h, e, "eup_step_profiled");
+    return EUP_OK;
+}
+
+int eup_synchronize(eup_handle* h) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
+int eup_get_launch_count(eup_handle* h, int64_t* launches) {
+    if (!h || !launches) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_launch_count: null argument");
+    *launches = h->launches;
+    return EUP_OK;
+}
+
+int eup_get_stream(eup_handle* h, void** stream) {
+    if (!h || !stream) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_stream: null argument");
+    *stream = (void*)h->stream;
+    return EUP_OK;
+}
+
+int eup_get_itime(eup_handle* h, int64_t* itime) {
+    if (!h || !itime) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_itime: null argument");
+    *itime = h->itime;
+    return EUP_OK;
+}
+
+int eup_get_forces(eup_handle* h, double fxyz[3]) { return eup_get_force_series(h, h ? h->itime : 0, 1, fxyz); }
+
+int eup_get_force_series(eup_handle* h, int64_t first_step, int32_t count, double* fxyz) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!fxyz || count < 0) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_force_series: bad argument");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_force_series: no state uploaded");
+    const int64_t lo = std::max(h->series_first, h->itime - h->cap + 1);
+    if (first_step < lo || first_step + count - 1 > h->itime)
+        return fail(h, EUP_ERR_INVALID_ARG,
+                    "eup_get_force_series: steps " + std::to_string(first_step) + ".." +
+                        std::to_string(first_step + count - 1) + " outside the recorded range " +
+                        std::to_string(lo) + ".." + std::to_string(h->itime));
+    CK(h, cudaStreamSynchronize(h->stream));
+    for (int32_t c = 0; c < count;) {
+        const int64_t t = first_step + c;
+        const int64_t pos = t % h->cap;
+        const int32_t run = (int32_t)std::min<int64_t>(count - c, h->cap - pos);
+        CK(h, cudaMemcpy(fxyz + 3 * (int64_t)c, h->series + 3 * pos, sizeof(double) * 3 * run, cudaMemcpyDeviceToHost));
+        c += run;
+    }
+    return EUP_OK;
+}
+
+int eup_get_cd_series(eup_handle* h, int64_t first_step, int32_t count, double* cd) {
+    if (!cd || count < 0) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_cd_series: bad argument");
+    if (h && !(h->cfg.cd_rho0 > 0 && h->cfg.cd_uref != 0 && h->cfg.cd_length > 0 && h->cfg.cd_span > 0))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_get_cd_series: drag normalisation not set in eup_config");
+    std::vector<double> f((size_t)3 * count);
+    int rc = eup_get_force_series(h, first_step, count, f.data());
+    if (rc) return rc;
+    const double den = 0.5 * h->cfg.cd_rho0 * h->cfg.cd_uref * h->cfg.cd_uref * h->cfg.cd_length * h->cfg.cd_span;
+    for (int32_t c = 0; c < count; ++c) cd[c] = f[3 * (size_t)c] / den;
+    return EUP_OK;
+}
+
+int eup_get_monitor(eup_handle* h, double out[5]) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!out) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_monitor: null out");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_monitor: no state uploaded");
+    DISPATCH(h, monitor_dispatch, h);
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(out, h->dscratch, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < 5; ++c)
+        if (!std::isfinite(out[c])) return fail(h, EUP_ERR_DIVERGED, "eup_get_monitor: non-finite FP64 sum (run diverged)");
+    return EUP_OK;
+}
+
+int eup_get_probes(eup_handle* h, int32_t npts, const int32_t* ijk, double* rho_u) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (npts < 0 || (npts > 0 && (!ijk || !rho_u))) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_probes: bad argument");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_probes: no state uploaded");
+    for (int32_t p = 0; p < npts; ++p)
+        if (!h->g.interior(ijk[3 * p], ijk[3 * p + 1], ijk[3 * p + 2]))
+            return fail(h, EUP_ERR_INVALID_ARG, "eup_get_probes: probe outside the interior");
+    if (npts == 0) return EUP_OK;
+    int32_t* d_ijk = nullptr;
+    double* d_out = nullptr;
+    CK(h, cudaMalloc(&d_ijk, sizeof(int32_t) * 3 * npts));
+    CK(h, cudaMalloc(&d_out, sizeof(double) * 4 * npts));
+    CK(h, cudaMemcpyAsync(d_ijk, ijk, sizeof(int32_t) * 3 * npts, cudaMemcpyHostToDevice, h->stream));
+    DISPATCH(h, probes_dispatch, h, npts, d_ijk, d_out);
+    cudaMemcpyAsync(rho_u, d_out, sizeof(double) * 4 * npts, cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_ijk);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return cuda_fail(h, e, "eup_get_probes");
+    return EUP_OK;
+}
+
+int eup_get_links(eup_handle* h, uint32_t* links) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!links) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_links: null out");
+    uint32_t* d = nullptr;
+    CK(h, cudaMalloc(&d, sizeof(uint32_t) * h->g.N));
+    launch_links(h->g, make_mask(h), d, h->stream);
+    cudaMemcpyAsync(links, d, sizeof(uint32_t) * h->g.N, cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(h, e, "eup_get_links");
+    return EUP_OK;
+}
+
+int eup_get_boundary_solid(eup_handle* h, int64_t* list, int64_t cap, int64_t* count) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!count || cap < 0 || (cap > 0 && !list)) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_boundary_solid: bad argument");
+    *count = h->nblist;
+    const int64_t n = std::min(cap, h->nblist);
+    if (n > 0) {
+        std::vector<int32_t> tmp((size_t)n);
+        CK(h, cudaMemcpy(tmp.data(), h->blist, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        for (int64_t t = 0; t < n; ++t) list[t] = tmp[(size_t)t];
+    }
+    return EUP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,517 @@
+// Boundary side of the time step: halo planes (CODE/SRC/bcond.bc.F90),
+// bounce-back on solid voxels with the momentum-exchange force
+// (CODE/SRC/bcond.obs.F90), the FP64 monitor (CODE/SRC/diagno.F90), probes
+// (CODE/SRC/probe_global.F90) and the host-layout scatter/gather used by
+// upload and download.  All of it is O(surface) or O(solid surface) work.
+#include "internal.h"
+
+namespace eup {
+
+namespace {
+
+// One thread per (a, b) pair of a face loop; a runs fastest.
+struct Range2 {
+    int a0, na, b0, nb;
+    __device__ __forceinline__ bool get(int& a, int& b) const {
+        const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= (int64_t)na * nb) return false;
+        a = a0 + (int)(t % na);
+        b = b0 + (int)(t / na);
+        return true;
+    }
+    unsigned blocks(int tpb) const {
+        const int64_t t = (int64_t)na * nb;
+        return (unsigned)((t + tpb - 1) / tpb);
+    }
+};
+
+constexpr int kTpb = 256;
+
+#define LD(q1, i, j, k) lat_load(L, g, (q1) - 1, (i), (j), (k))
+#define ST(q1, i, j, k, v) ghost_store(L, g, (q1) - 1, (i), (j), (k), (v))
+
+// ---- front wall, x = l+1 -----------------------------------------------------
+template <typename S, typename R>
+__global__ void k_front(Lat<S, R> L, Geo g, Range2 r, int flag) {
+    int j, k;
+    if (!r.get(j, k)) return;
+    const int l = g.l, l1 = g.l + 1, m = g.m;
+    if (flag == 0) {  // periodic, CODE/SRC/bcond.bc.F90:75-105 (SERIAL corner line :90)
+        if (j == 0) { ST(12, l1, 0, k, LD(12, 1, m, k)); return; }
+        for (int q = 10; q <= 14; ++q) ST(q, l1, j, k, LD(q, 1, j, k));
+    } else if (flag == 1) {  // no-slip, :108-124
+        ST(12, l1, j - 1, k, LD(1, l, j, k));
+        ST(13, l1, j, k - 1, LD(2, l, j, k));
+        ST(10, l1, j + 1, k, LD(3, l, j, k));
+        ST(11, l1, j, k + 1, LD(4, l, j, k));
+        ST(14, l1, j, k, LD(5, l, j, k));
+    } else {  // outflow, :127-169: equilibrium at rho=1 with the (un-normalised) momentum of x=l
+        R a[19];
+#pragma unroll
+        for (int q = 0; q < 18; ++q) a[q] = lat_load(L, g, q, l, j, k);
+        const R xj = a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13];
+        const R yj = a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17];
+        const R zj = a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15];
+        const R rf = R(3), qf = R(1.5), t3 = R(3), one = R(1);
+        const R cvsq = xj * xj + yj * yj + zj * zj;
+        const R cx10 = rf * (-xj - yj) + qf * (t3 * (xj + yj) * (xj + yj) - cvsq);
+        const R cx11 = rf * (-xj - zj) + qf * (t3 * (xj + zj) * (xj + zj) - cvsq);
+        const R cx12 = rf * (-xj + yj) + qf * (t3 * (xj - yj) * (xj - yj) - cvsq);
+        const R cx13 = rf * (-xj + zj) + qf * (t3 * (xj - zj) * (xj - zj) - cvsq);
+        const R cx14 = rf * (-xj) + qf * (t3 * (xj) * (xj) - cvsq);
+        const R p1 = Const<R>::p1(), p2 = Const<R>::p2();
+        ST(10, l1, j, k, p2 * (one + cx10));
+        ST(11, l1, j, k, p2 * (one + cx11));
+        ST(12, l1, j, k, p2 * (one + cx12));
+        ST(13, l1, j, k, p2 * (one + cx13));
+        ST(14, l1, j, k, p1 * (one + cx14));
+    }
+}
+
+// Outflow border fix, CODE/SRC/bcond.bc.F90:172-203: copies of the edge rows.
+template <typename S, typename R>
+__global__ void k_front_fix(Lat<S, R> L, Geo g, Range2 r) {
+    int t, side;
+    if (!r.get(t, side)) return;
+    const int l1 = g.l + 1, m = g.m, n = g.n;
+    if (side == 0 && t >= 1 && t <= m) {
+        for (int q = 10; q <= 14; ++q) ST(q, l1, t, 0, LD(q, l1, t, 1));
+        for (int q = 10; q <= 14; ++q) ST(q, l1, t, n + 1, LD(q, l1, t, n));
+    }
+    if (side == 1 && t >= 1 && t <= n) {
+        for (int q = 10; q <= 14; ++q) ST(q, l1, 0, t, LD(q, l1, 1, t));
+        for (int q = 10; q <= 14; ++q) ST(q, l1, m + 1, t, LD(q, l1, m, t));
+    }
+}
+
+// ---- rear wall, x = 0 ----------------------------------------------------------
+template <typename S, typename R>
+__global__ void k_rear(Lat<S, R> L, Geo g, Range2 r, int flag, R u_inflow) {
+    int j, k;
+    if (!r.get(j, k)) return;
+    const int l = g.l, m1 = g.m + 1;
+    if (flag == 0) {  // periodic, :210-238 (SERIAL corner line :223)
+        if (j == 0) { ST(1, 0, m1, k, LD(1, l, 1, k)); return; }
+        for (int q = 1; q <= 5; ++q) ST(q, 0, j, k, LD(q, l, j, k));
+    } else if (flag == 1) {  // no-slip, :241-257
+        ST(3, 0, j - 1, k, LD(10, 1, j, k));
+        ST(4, 0, j, k - 1, LD(11, 1, j, k));
+        ST(1, 0, j + 1, k, LD(12, 1, j, k));
+        ST(2, 0, j, k + 1, LD(13, 1, j, k));
+        ST(5, 0, j, k, LD(14, 1, j, k));
+    } else {  // inflow, uniform, :260-321
+        const R xj = u_inflow, yj = R(0), zj = R(0);
+        const R rf = R(3), qf = R(1.5), t3 = R(3), one = R(1);
+        const R cvsq = xj * xj + yj * yj + zj * zj;
+        const R cx01 = rf * (xj - yj) + qf * (t3 * (xj - yj) * (xj - yj) - cvsq);
+        const R cx02 = rf * (xj - zj) + qf * (t3 * (xj - zj) * (xj - zj) - cvsq);
+        const R cx03 = rf * (xj + yj) + qf * (t3 * (xj + yj) * (xj + yj) - cvsq);
+        const R cx04 = rf * (xj + zj) + qf * (t3 * (xj + zj) * (xj + zj) - cvsq);
+        const R cx05 = rf * (xj) + qf * (t3 * (xj) * (xj) - cvsq);
+        const R p1 = Const<R>::p1(), p2 = Const<R>::p2();
+        ST(1, 0, j, k, p2 * (one + cx01));
+        ST(2, 0, j, k, p2 * (one + cx02));
+        ST(3, 0, j, k, p2 * (one + cx03));
+        ST(4, 0, j, k, p2 * (one + cx04));
+        ST(5, 0, j, k, p1 * (one + cx05));
+    }
+}
+
+// ---- up wall, z = n+1 -------------------------------------------------------------
+template <typename S, typename R>
+__global__ void k_up(Lat<S, R> L, Geo g, Range2 r, int flag, R force) {
+    int i, j;
+    if (!r.get(i, j)) return;
+    const int n = g.n, n1 = g.n + 1;
+    if (flag == 0) {  // periodic, :385-409
+        ST(2, i, j, n1, LD(2, i, j, 1));
+        ST(9, i, j, n1, LD(9, i, j, 1));
+        ST(11, i, j, n1, LD(11, i, j, 1));
+        ST(15, i, j, n1, LD(15, i, j, 1));
+        ST(16, i, j, n1, LD(16, i, j, 1));
+    } else if (flag == 1 || flag == 2) {  // no-slip :412-428, lid :431-447
+        ST(15, i, j, n1, LD(6, i, j, n));
+        ST(2, i - 1, j, n1, flag == 2 ? LD(13, i, j, n) + force : LD(13, i, j, n));
+        ST(9, i, j - 1, n1, LD(18, i, j, n));
+        ST(11, i + 1, j, n1, flag == 2 ? LD(4, i, j, n) - force : LD(4, i, j, n));
+        ST(16, i, j + 1, n1, LD(7, i, j, n));
+    } else {  // free-slip over i = 0..l+1, j = 0..m+1, :450-468
+        ST(15, i, j, n1, LD(6, i, j, n));
+        ST(11, i, j, n1, LD(13, i, j, n));
+        ST(16, i, j, n1, LD(18, i, j, n));
+        ST(2, i, j, n1, LD(4, i, j, n));
+        ST(9, i, j, n1, LD(7, i, j, n));
+    }
+}
+
+// ---- down wall, z = 0 ---------------------------------------------------------------
+template <typename S, typename R>
+__global__ void k_down(Lat<S, R> L, Geo g, Range2 r, int flag) {
+    int i, j;
+    if (!r.get(i, j)) return;
+    const int n = g.n;
+    if (flag == 0) {  // periodic, :472-496
+        ST(4, i, j, 0, LD(4, i, j, n));
+        ST(6, i, j, 0, LD(6, i, j, n));
+        ST(7, i, j, 0, LD(7, i, j, n));
+        ST(13, i, j, 0, LD(13, i, j, n));
+        ST(18, i, j, 0, LD(18, i, j, n));
+    } else if (flag == 1) {  // no-slip, :499-515
+        ST(6, i, j, 0, LD(15, i, j, 1));
+        ST(4, i - 1, j, 0, LD(11, i, j, 1));
+        ST(7, i, j - 1, 0, LD(16, i, j, 1));
+        ST(13, i + 1, j, 0, LD(2, i, j, 1));
+        ST(18, i, j + 1, 0, LD(9, i, j, 1));
+    } else {  // free-slip, :518-530
+        ST(6, i, j, 0, LD(15, i, j, 1));
+        ST(13, i, j, 0, LD(11, i, j, 1));
+        ST(18, i, j, 0, LD(16, i, j, 1));
+        ST(4, i, j, 0, LD(2, i, j, 1));
+        ST(7, i, j, 0, LD(9, i, j, 1));
+    }
+}
+
+// ---- left wall, y = 0 ------------------------------------------------------------------
+template <typename S, typename R>
+__global__ void k_left(Lat<S, R> L, Geo g, Range2 r, int flag) {
+    int i, k;
+    if (!r.get(i, k)) return;
+    const int l = g.l, m = g.m;
+    if (flag == 0) {  // periodic, :535-560 (corner line :547)
+        if (i == 0) { ST(3, 0, 0, k, LD(3, l, m, k)); return; }
+        ST(3, i, 0, k, LD(3, i, m, k));
+        ST(7, i, 0, k, LD(7, i, m, k));
+        ST(8, i, 0, k, LD(8, i, m, k));
+        ST(9, i, 0, k, LD(9, i, m, k));
+        ST(12, i, 0, k, LD(12, i, m, k));
+    } else if (flag == 1) {  // no-slip, :563-579
+        ST(8, i, 0, k, LD(17, i, 1, k));
+        ST(12, i + 1, 0, k, LD(1, i, 1, k));
+        ST(3, i - 1, 0, k, LD(10, i, 1, k));
+        ST(7, i, 0, k - 1, LD(16, i, 1, k));
+        ST(9, i, 0, k + 1, LD(18, i, 1, k));
+    } else {  // free-slip, :582-594
+        ST(8, i, 0, k, LD(17, i, 1, k));
+        ST(3, i, 0, k, LD(1, i, 1, k));
+        ST(12, i, 0, k, LD(10, i, 1, k));
+        ST(9, i, 0, k, LD(16, i, 1, k));
+        ST(7, i, 0, k, LD(18, i, 1, k));
+    }
+}
+
+// ---- right wall, y = m+1 ------------------------------------------------------------------
+template <typename S, typename R>
+__global__ void k_right(Lat<S, R> L, Geo g, Range2 r, int flag) {
+    int i, k;
+    if (!r.get(i, k)) return;
+    const int m = g.m, m1 = g.m + 1, l1 = g.l + 1;
+    if (flag == 0) {  // periodic, :600-625 (corner line :612)
+        if (i == 0) { ST(10, l1, m1, k, LD(10, 1, 1, k)); return; }
+        ST(1, i, m1, k, LD(1, i, 1, k));
+        ST(10, i, m1, k, LD(10, i, 1, k));
+        ST(16, i, m1, k, LD(16, i, 1, k));
+        ST(17, i, m1, k, LD(17, i, 1, k));
+        ST(18, i, m1, k, LD(18, i, 1, k));
+    } else if (flag == 1) {  // no-slip, :628-644
+        ST(10, i + 1, m1, k, LD(3, i, m, k));
+        ST(16, i, m1, k + 1, LD(7, i, m, k));
+        ST(17, i, m1, k, LD(8, i, m, k));
+        ST(18, i, m1, k - 1, LD(9, i, m, k));
+        ST(1, i - 1, m1, k, LD(12, i, m, k));
+    } else {  // free-slip, :647-659
+        ST(1, i, m1, k, LD(3, i, m, k));
+        ST(18, i, m1, k, LD(7, i, m, k));
+        ST(17, i, m1, k, LD(8, i, m, k));
+        ST(16, i, m1, k, LD(9, i, m, k));
+        ST(10, i, m1, k, LD(12, i, m, k));
+    }
+}
+
+// Free-slip edge fixes, CODE/SRC/bcond.bc.F90:663-690.
+template <typename S, typename R>
+__global__ void k_edge_fix(Lat<S, R> L, Geo g, Range2 r, int fixes) {
+    int i, dummy;
+    if (!r.get(i, dummy)) return;
+    const int m = g.m, m1 = g.m + 1, n = g.n, n1 = g.n + 1;
+    if (fixes & 1) ST(9, i, 0, n1, LD(18, i, 1, n));
+    if (fixes & 2) ST(16, i, m1, n1, LD(7, i, m, n));
+    if (fixes & 4) ST(18, i, m1, 0, LD(9, i, m, 1));
+    if (fixes & 8) ST(7, i, 0, 0, LD(16, i, 1, 1));
+}
+
+#undef LD
+#undef ST
+
+// ---- block reduction into deterministic per-block partials ----------------------------
+template <int W>
+__device__ void block_reduce_store(double (&v)[W], const Reduce& red, double* out) {
+    __shared__ double sh[32][W];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+    if (lane == 0)
+        for (int c = 0; c < W; ++c) sh[warp][c] = v[c];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int c = 0; c < W; ++c) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += sh[w][c];
+            red.partials[(int64_t)blockIdx.x * W + c] = s;
+        }
+        __threadfence();
+        const unsigned done = atomicAdd(red.counter, 1u);
+        last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < W; ++c) {
+            double s = 0.0;
+            for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)red.partials)[(int64_t)b * W + c];
+            out[c] = s;
+        }
+        *red.counter = 0u;
+    }
+}
+
+// ---- bounce-back + momentum exchange ---------------------------------------------------
+//
+// For each solid voxel x touching fluid or halo and each moving q, the
+// reference sets a_q(x) = a_opp(q)(x + c_q) (CODE/SRC/bcond.obs.F90:56-73), so
+// that the next pull returns to the fluid node x + c_q its own post-collision
+// population.  Links whose neighbour is itself solid are skipped: their value
+// is only ever pulled into solid voxels.  The same reads give the force: the
+// population a_opp(q)(y) leaving fluid node y = x + c_q towards x transfers
+// 2 c_opp(q) a_opp(q)(y) = -2 c_q a_opp(q)(y); across a periodic axis y is the
+// wrapped node and its interior value is used.
+template <typename S, typename R>
+__global__ void k_bounce_drag(Lat<S, R> L, Geo g, Mask mk, int per_x, int per_y, int per_z,
+                              const int32_t* list, int64_t nlist, int do_bounce, Reduce red,
+                              double* force_out) {
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nlist;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t lin = list[t];
+        const int i = (int)(lin % g.l) + 1;
+        const int j = (int)((lin / g.l) % g.m) + 1;
+        const int k = (int)(lin / g.lm) + 1;
+#pragma unroll
+        for (int q = 0; q < 18; ++q) {
+            const int qo = opp_of(q);
+            const int ni = i + cx_of(q), nj = j + cy_of(q), nk = k + cz_of(q);
+            if (g.interior(ni, nj, nk)) {
+                if (mk.solid(g, ni, nj, nk)) continue;
+                const S raw = L.pop[qo][g.lin(ni, nj, nk)];
+                const double v = (double)Store<S, R>::load(raw, qo, L.inv_scale);
+                f[0] -= 2.0 * cx_of(q) * v;
+                f[1] -= 2.0 * cy_of(q) * v;
+                f[2] -= 2.0 * cz_of(q) * v;
+                if (do_bounce) L.pop[q][lin] = raw;
+            } else {
+                const R v = L.ghost[(int64_t)qo * g.G + g.gidx(ni, nj, nk)];
+                if (do_bounce) L.pop[q][lin] = Store<S, R>::store(v, q, L.scale);
+                int wi = ni, wj = nj, wk = nk;
+                if (per_x) wi = wi < 1 ? wi + g.l : (wi > g.l ? wi - g.l : wi);
+                if (per_y) wj = wj < 1 ? wj + g.m : (wj > g.m ? wj - g.m : wj);
+                if (per_z) wk = wk < 1 ? wk + g.n : (wk > g.n ? wk - g.n : wk);
+                if (g.interior(wi, wj, wk) && !mk.solid(g, wi, wj, wk)) {
+                    const double w = (double)lat_load(L, g, qo, wi, wj, wk);
+                    f[0] -= 2.0 * cx_of(q) * w;
+                    f[1] -= 2.0 * cy_of(q) * w;
+                    f[2] -= 2.0 * cz_of(q) * w;
+                }
+            }
+        }
+    }
+    block_reduce_store<3>(f, red, force_out);
+}
+
+// ---- FP64 monitor, CODE/SRC/diagno.F90:67-120 -------------------------------------------
+template <typename S, typename R>
+__global__ void k_monitor(Lat<S, R> L, Geo g, Mask mk, Reduce red, double* out) {
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.N;
+         lin += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(lin % g.l) + 1;
+        const int j = (int)((lin / g.l) % g.m) + 1;
+        const int k = (int)(lin / g.lm) + 1;
+        if (mk.solid(g, i, j, k)) {
+            s[0] += 1.0;
+            continue;
+        }
+        double a[19];
+#pragma unroll
+        for (int q = 0; q < 19; ++q) a[q] = (double)Store<S, R>::load(L.pop[q][lin], q, L.inv_scale);
+        double rho = 0.0;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) rho += a[q];
+        const double ri = 1.0 / rho;
+        const double xj = (a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13]) * ri;
+        const double yj = (a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17]) * ri;
+        const double zj = (a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15]) * ri;
+        s[0] += rho; s[1] += xj; s[2] += yj; s[3] += zj; s[4] += xj * xj + yj * yj + zj * zj;
+    }
+    block_reduce_store<5>(s, red, out);
+}
+
+template <typename S, typename R>
+__global__ void k_probes(Lat<S, R> L, Geo g, int npts, const int32_t* ijk, double* out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npts) return;
+    const int i = ijk[3 * p], j = ijk[3 * p + 1], k = ijk[3 * p + 2];
+    double a[19];
+    for (int q = 0; q < 19; ++q) a[q] = (double)lat_load(L, g, q, i, j, k);
+    double rho = 0.0;
+    for (int q = 0; q < 19; ++q) rho += a[q];
+    out[4 * p] = rho;
+    out[4 * p + 1] = (a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13]) / rho;
+    out[4 * p + 2] = (a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17]) / rho;
+    out[4 * p + 3] = (a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15]) / rho;
+}
+
+// ---- host layout <-> device layout ------------------------------------------------------
+template <typename S, typename R, typename T>
+__global__ void k_scatter(Lat<S, R> L, Geo g, int q, const T* src, int64_t total) {
+    const int64_t L2 = g.l + 2, M2 = g.m + 2;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % L2), j = (int)((idx / L2) % M2), k = (int)(idx / (L2 * M2));
+        const R v = (R)src[idx];
+        if (g.interior(i, j, k)) L.pop[q][g.lin(i, j, k)] = Store<S, R>::store(v, q, L.scale);
+        else L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)] = v;
+    }
+}
+
+template <typename S, typename R, typename T>
+__global__ void k_gather(Lat<S, R> L, Geo g, int q, T* dst, int64_t total) {
+    const int64_t L2 = g.l + 2, M2 = g.m + 2;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x)
+        dst[idx] = (T)lat_load(L, g, q, (int)(idx % L2), (int)((idx / L2) % M2), (int)(idx / (L2 * M2)));
+}
+
+unsigned grid_for(int64_t work, int tpb, unsigned cap = 148u * 16u) {
+    int64_t b = (work + tpb - 1) / tpb;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (unsigned)b;
+}
+
+}  // namespace
+
+template <typename S, typename R>
+int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& ph, cudaStream_t st) {
+    const int l = g.l, m = g.m, n = g.n;
+    int launches = 6;
+    // front
+    {
+        const int f = bc[0];
+        Range2 r = (f == 0) ? Range2{0, m + 1, 1, n} : Range2{1, m, 1, n};
+        k_front<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, f);
+        if (f == 5) {
+            Range2 rf{0, (m > n ? m : n) + 1, 0, 2};
+            k_front_fix<S, R><<<rf.blocks(kTpb), kTpb, 0, st>>>(L, g, rf);
+            ++launches;
+        }
+    }
+    // rear
+    {
+        const int f = bc[1];
+        Range2 r = (f == 0) ? Range2{0, m + 1, 1, n} : (f == 1) ? Range2{1, m, 1, n} : Range2{0, m + 2, 0, n + 2};
+        k_rear<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, f, ph.u_inflow);
+    }
+    // up
+    {
+        const int f = bc[4];
+        Range2 r = (f == 3) ? Range2{0, l + 2, 0, m + 2} : Range2{1, l, 1, m};
+        k_up<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, f, ph.force);
+    }
+    // down
+    {
+        Range2 r{1, l, 1, m};
+        k_down<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, bc[5]);
+    }
+    // left
+    {
+        const int f = bc[3];
+        Range2 r = (f == 0) ? Range2{0, l + 1, 1, n} : Range2{1, l, 1, n};
+        k_left<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, f);
+    }
+    // right
+    {
+        const int f = bc[2];
+        Range2 r = (f == 0) ? Range2{0, l + 1, 1, n} : Range2{1, l, 1, n};
+        k_right<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, f);
+    }
+    const int fixes = ((bc[3] == 3 && bc[4] == 3) ? 1 : 0) | ((bc[2] == 3 && bc[4] == 3) ? 2 : 0) |
+                      ((bc[2] == 3 && bc[5] == 3) ? 4 : 0) | ((bc[3] == 3 && bc[5] == 3) ? 8 : 0);
+    if (fixes) {
+        Range2 r{1, l, 0, 1};
+        k_edge_fix<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, fixes);
+        ++launches;
+    }
+    return launches;
+}
+
+template <typename S, typename R>
+void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const Mask& mk, const int bc[6],
+                        const int32_t* list, int64_t nlist, bool do_bounce, const Reduce& red,
+                        double* force_out, cudaStream_t st) {
+    const int per_x = (bc[0] == 0 && bc[1] == 0), per_y = (bc[2] == 0 && bc[3] == 0);
+    const int per_z = (bc[4] == 0 && bc[5] == 0);
+    const unsigned blocks = grid_for(nlist, kTpb, (unsigned)red.max_blocks);
+    k_bounce_drag<S, R><<<blocks, kTpb, 0, st>>>(L, g, mk, per_x, per_y, per_z, list, nlist,
+                                                 do_bounce ? 1 : 0, red, force_out);
+}
+
+template <typename S, typename R>
+void launch_monitor(const Lat<S, R>& L, const Geo& g, const Mask& mk, const Reduce& red, double* out,
+                    cudaStream_t st) {
+    const unsigned blocks = grid_for(g.N, kTpb, (unsigned)red.max_blocks);
+    k_monitor<S, R><<<blocks, kTpb, 0, st>>>(L, g, mk, red, out);
+}
+
+template <typename S, typename R>
+void launch_probes(const Lat<S, R>& L, const Geo& g, int npts, const int32_t* ijk, double* out,
+                   cudaStream_t st) {
+    k_probes<S, R><<<(npts + 127) / 128, 128, 0, st>>>(L, g, npts, ijk, out);
+}
+
+template <typename S, typename R, typename T>
+void launch_scatter(const Lat<S, R>& L, const Geo& g, int q, const T* staging, cudaStream_t st) {
+    const int64_t total = (int64_t)(g.l + 2) * (g.m + 2) * (g.n + 2);
+    k_scatter<S, R, T><<<grid_for(total, kTpb), kTpb, 0, st>>>(L, g, q, staging, total);
+}
+
+template <typename S, typename R, typename T>
+void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStream_t st) {
+    const int64_t total = (int64_t)(g.l + 2) * (g.m + 2) * (g.n + 2);
+    k_gather<S, R, T><<<grid_for(total, kTpb), kTpb, 0, st>>>(L, g, q, staging, total);
+}
+
+#define EUP_INST(S, R)                                                                                 \
+    template int launch_bc<S, R>(const Lat<S, R>&, const Geo&, const int*, const Phys<R>&, cudaStream_t); \
+    template void launch_bounce_drag<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const int*,      \
+                                           const int32_t*, int64_t, bool, const Reduce&, double*,      \
+                                           cudaStream_t);                                              \
+    template void launch_monitor<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const Reduce&,       \
+                                       double*, cudaStream_t);                                         \
+    template void launch_probes<S, R>(const Lat<S, R>&, const Geo&, int, const int32_t*, double*,      \
+                                      cudaStream_t);                                                   \
+    template void launch_scatter<S, R, float>(const Lat<S, R>&, const Geo&, int, const float*,         \
+                                              cudaStream_t);                                           \
+    template void launch_scatter<S, R, double>(const Lat<S, R>&, const Geo&, int, const double*,       \
+                                               cudaStream_t);                                          \
+    template void launch_gather<S, R, float>(const Lat<S, R>&, const Geo&, int, float*, cudaStream_t); \
+    template void launch_gather<S, R, double>(const Lat<S, R>&, const Geo&, int, double*, cudaStream_t);
+
+EUP_INST(float, float)
+EUP_INST(double, double)
+EUP_INST(__half, float)
+EUP_INST(__nv_bfloat16, float)
+
+}  // namespace eup

@@ -1,0 +1,246 @@
+// Device-side building blocks of the D3Q19 BGK step: lattice constants,
+// population storage formats, the halo shell and the collision.
+//
+// Population q (0-based) is the reference's a(q+1); velocities follow
+// CODE/SRC/bgk3d.F90:30-49 and the streaming offsets of CODE/SRC/movef.F90:48-65.
+// All kernels of this library are compiled with --fmad=false: every float or
+// double operation rounds on its own, in the evaluation order of the
+// reference's Fortran, so the FP32 and FP64 paths reproduce a serial IEEE
+// build of the reference bit for bit.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace eup {
+
+constexpr int Q = 19;
+
+// c_q, q = 0..18 (reference a01..a19)
+__host__ __device__ constexpr int cx_of(int q) {
+    return (q <= 4) ? 1 : (q >= 9 && q <= 13) ? -1 : 0;
+}
+__host__ __device__ constexpr int cy_of(int q) {
+    return (q == 2 || q == 6 || q == 7 || q == 8 || q == 11) ? 1
+           : (q == 0 || q == 9 || q == 15 || q == 16 || q == 17) ? -1
+                                                                  : 0;
+}
+__host__ __device__ constexpr int cz_of(int q) {
+    return (q == 3 || q == 5 || q == 6 || q == 12 || q == 17) ? 1
+           : (q == 1 || q == 8 || q == 10 || q == 14 || q == 15) ? -1
+                                                                  : 0;
+}
+// opposite direction: 1<->12, 2<->13, 3<->10, 4<->11, 5<->14, 6<->15, 7<->16, 8<->17, 9<->18
+__host__ __device__ constexpr int opp_of(int q) {
+    return (q == 18) ? 18 : (q <= 1) ? q + 11 : (q <= 3) ? q + 7 : (q <= 8) ? q + 9
+           : (q <= 10) ? q - 7 : (q <= 12) ? q - 11 : q - 9;
+}
+// weight class: 0 -> p0 (rest), 1 -> p1 (axis), 2 -> p2 (diagonal)
+__host__ __device__ constexpr int wclass_of(int q) {
+    return (q == 18) ? 0 : (q == 4 || q == 5 || q == 7 || q == 13 || q == 14 || q == 16) ? 1 : 2;
+}
+
+template <typename R> struct Const;
+template <> struct Const<float> {
+    // CODE/SRC/storage.F90:54-81,194-205: computed wide, rounded to mykind
+    static __device__ __forceinline__ float p0() { return (float)(1.0 / 3.0); }
+    static __device__ __forceinline__ float p1() { return (float)(1.0 / 18.0); }
+    static __device__ __forceinline__ float p2() { return (float)(1.0 / 36.0); }
+};
+template <> struct Const<double> {
+    static __device__ __forceinline__ double p0() { return 1.0 / 3.0; }
+    static __device__ __forceinline__ double p1() { return 1.0 / 18.0; }
+    static __device__ __forceinline__ double p2() { return 1.0 / 36.0; }
+};
+
+template <typename R>
+__device__ __forceinline__ R weight(int q) {
+    const int c = wclass_of(q);
+    return c == 0 ? Const<R>::p0() : (c == 1 ? Const<R>::p1() : Const<R>::p2());
+}
+
+// ---------------------------------------------------------------------------
+// Storage formats.  S is what lives in HBM, R the arithmetic type.
+//   float/double : the population itself;
+//   __half/bf16  : (f_q - w_q) * scale, scale a power of two.
+// ---------------------------------------------------------------------------
+template <typename S, typename R> struct Store;
+
+template <> struct Store<float, float> {
+    static __device__ __forceinline__ float load(float s, int, float) { return s; }
+    static __device__ __forceinline__ float store(float f, int, float) { return f; }
+};
+template <> struct Store<double, double> {
+    static __device__ __forceinline__ double load(double s, int, double) { return s; }
+    static __device__ __forceinline__ double store(double f, int, double) { return f; }
+};
+template <> struct Store<__half, float> {
+    static __device__ __forceinline__ float load(__half s, int q, float inv_scale) {
+        return weight<float>(q) + __half2float(s) * inv_scale;
+    }
+    static __device__ __forceinline__ __half store(float f, int q, float scale) {
+        return __float2half_rn((f - weight<float>(q)) * scale);
+    }
+};
+template <> struct Store<__nv_bfloat16, float> {
+    static __device__ __forceinline__ float load(__nv_bfloat16 s, int q, float inv_scale) {
+        return weight<float>(q) + __bfloat162float(s) * inv_scale;
+    }
+    static __device__ __forceinline__ __nv_bfloat16 store(float f, int q, float scale) {
+        return __float2bfloat16_rn((f - weight<float>(q)) * scale);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Lattice geometry and the persistent halo shell.
+//
+// Interior node (i,j,k), 1-based, lives at lin = (i-1) + l*((j-1) + m*(k-1))
+// of each population array.  Halo nodes (any coordinate 0 or l+1/m+1/n+1)
+// live in one shell per population with a single owner per node: the x
+// planes own their full (m+2)*(n+2) extent, the y planes i = 1..l and
+// k = 0..n+1, the z planes i = 1..l, j = 1..m.  The shell plays the role of
+// the halo of the reference's single array a (CODE/SRC/alloca.F90:94-132):
+// it persists across steps, so halo values that the reference never rewrites
+// keep their initial values here too.
+// ---------------------------------------------------------------------------
+struct Geo {
+    int l, m, n;
+    int64_t lm;      // l*m
+    int64_t N;       // l*m*n
+    int64_t sx, sy, sz;         // face sizes
+    int64_t ox0, oxl, oy0, oym, oz0, ozn, G;
+
+    __host__ __device__ void init(int l_, int m_, int n_) {
+        l = l_; m = m_; n = n_;
+        lm = (int64_t)l * m;
+        N = lm * n;
+        sx = (int64_t)(m + 2) * (n + 2);
+        sy = (int64_t)l * (n + 2);
+        sz = (int64_t)l * m;
+        ox0 = 0; oxl = sx; oy0 = 2 * sx; oym = oy0 + sy; oz0 = oym + sy; ozn = oz0 + sz;
+        G = ozn + sz;
+    }
+    __host__ __device__ __forceinline__ bool interior(int i, int j, int k) const {
+        return i >= 1 && i <= l && j >= 1 && j <= m && k >= 1 && k <= n;
+    }
+    __host__ __device__ __forceinline__ int64_t lin(int i, int j, int k) const {
+        return (int64_t)(i - 1) + (int64_t)l * ((int64_t)(j - 1) + (int64_t)m * (k - 1));
+    }
+    // (i,j,k) must be a halo node
+    __host__ __device__ __forceinline__ int64_t gidx(int i, int j, int k) const {
+        if (i == 0) return ox0 + (int64_t)k * (m + 2) + j;
+        if (i == l + 1) return oxl + (int64_t)k * (m + 2) + j;
+        if (j == 0) return oy0 + (int64_t)k * l + (i - 1);
+        if (j == m + 1) return oym + (int64_t)k * l + (i - 1);
+        if (k == 0) return oz0 + (int64_t)(j - 1) * l + (i - 1);
+        return ozn + (int64_t)(j - 1) * l + (i - 1);
+    }
+};
+
+// Pointers of one lattice (19 population arrays) plus the halo shell.
+template <typename S, typename R>
+struct Lat {
+    S* pop[Q];
+    R* ghost;       // ghost[q*G + gidx]
+    R scale, inv_scale;
+};
+
+template <typename S, typename R>
+__device__ __forceinline__ R lat_load(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k) {
+    if (g.interior(i, j, k)) return Store<S, R>::load(L.pop[q][g.lin(i, j, k)], q, L.inv_scale);
+    return L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)];
+}
+template <typename S, typename R>
+__device__ __forceinline__ void ghost_store(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k, R v) {
+    L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)] = v;
+}
+
+// ---------------------------------------------------------------------------
+// BGK collision of one node, CODE/SRC/col.F90:127-229, same operation order.
+// x[0..17] are the streamed populations b01..b18, x[18] is a19; on return x
+// holds a01..a19 after collision.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void collide(R* x, R omega, R omega1, R fgrad) {
+    const R uno = R(1), tre = R(3), qf = R(1.5), rf = R(3), zero = R(0);
+    const R p0 = Const<R>::p0(), p1 = Const<R>::p1(), p2 = Const<R>::p2();
+    const R drho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] +
+                   x[11] + x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18];
+    const R drhoinv = uno / drho;
+    R dvx = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * drhoinv;
+    R dvy = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * drhoinv;
+    R dvz = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * drhoinv;
+    const R dvx2 = dvx * dvx, dvy2 = dvy * dvy, dvz2 = dvz * dvz;
+    const R dvsq = dvx2 + dvy2 + dvz2;
+    R dvxpy = dvx + dvy;
+    const R dqxpy = uno + qf * (tre * dvxpy * dvxpy - dvsq);
+    R dvxmy = dvx - dvy;
+    const R dqxmy = uno + qf * (tre * dvxmy * dvxmy - dvsq);
+    R dvxpz = dvx + dvz;
+    const R dqxpz = uno + qf * (tre * dvxpz * dvxpz - dvsq);
+    R dvxmz = dvx - dvz;
+    const R dqxmz = uno + qf * (tre * dvxmz * dvxmz - dvsq);
+    R dvypz = dvy + dvz;
+    const R dqypz = uno + qf * (tre * dvypz * dvypz - dvsq);
+    R dvymz = dvy - dvz;
+    const R dqymz = uno + qf * (tre * dvymz * dvymz - dvsq);
+    const R dqx = uno + qf * (tre * dvx2 - dvsq);
+    const R dqy = uno + qf * (tre * dvy2 - dvsq);
+    const R dqz = uno + qf * (tre * dvz2 - dvsq);
+    dvx = rf * dvx; dvy = rf * dvy; dvz = rf * dvz;
+    dvxpy = rf * dvxpy; dvxmy = rf * dvxmy; dvxpz = rf * dvxpz;
+    dvxmz = rf * dvxmz; dvypz = rf * dvypz; dvymz = rf * dvymz;
+    const R drp1 = drho * p1;
+    const R drp2 = drho * p2;
+    const R forcex = fgrad * drho, forcey = zero, forcez = zero;  // FORCING_X (default)
+
+    const R de01 = drp2 * (dvxmy + dqxmy);
+    const R de02 = drp2 * (dvxmz + dqxmz);
+    const R de03 = drp2 * (dvxpy + dqxpy);
+    const R de04 = drp2 * (dvxpz + dqxpz);
+    const R de05 = drp1 * (dvx + dqx);
+    const R de06 = drp1 * (dvz + dqz);
+    const R de07 = drp2 * (dvypz + dqypz);
+    const R de08 = drp1 * (dvy + dqy);
+    const R de09 = drp2 * (dvymz + dqymz);
+    const R de10 = drp2 * (-dvxpy + dqxpy);
+    const R de11 = drp2 * (-dvxpz + dqxpz);
+    const R de12 = drp2 * (-dvxmy + dqxmy);
+    const R de13 = drp2 * (-dvxmz + dqxmz);
+    const R de14 = drp1 * (-dvx + dqx);
+    const R de15 = drp1 * (-dvz + dqz);
+    const R de16 = drp2 * (-dvypz + dqypz);
+    const R de17 = drp1 * (-dvy + dqy);
+    const R de18 = drp2 * (-dvymz + dqymz);
+    const R de19 = drho * p0 * (uno - qf * dvsq);
+
+    x[0] = omega1 * x[0] + (omega * de01 + forcex - forcey);
+    x[1] = omega1 * x[1] + (omega * de02 + forcex - forcez);
+    x[2] = omega1 * x[2] + (omega * de03 + forcex + forcey);
+    x[3] = omega1 * x[3] + (omega * de04 + forcex + forcez);
+    x[4] = omega1 * x[4] + (omega * de05 + forcex);
+    x[5] = omega1 * x[5] + (omega * de06 + forcez);
+    x[6] = omega1 * x[6] + (omega * de07 + forcey + forcez);
+    x[7] = omega1 * x[7] + (omega * de08 + forcey);
+    x[8] = omega1 * x[8] + (omega * de09 + forcey - forcez);
+    x[9] = omega1 * x[9] + (omega * de10 - forcex - forcey);
+    x[10] = omega1 * x[10] + (omega * de11 - forcex - forcez);
+    x[11] = omega1 * x[11] + (omega * de12 - forcex + forcey);
+    x[12] = omega1 * x[12] + (omega * de13 - forcex + forcez);
+    x[13] = omega1 * x[13] + (omega * de14 - forcex);
+    x[14] = omega1 * x[14] + (omega * de15 - forcez);
+    x[15] = omega1 * x[15] + (omega * de16 - forcey - forcez);
+    x[16] = omega1 * x[16] + (omega * de17 - forcey);
+    x[17] = omega1 * x[17] + (omega * de18 - forcey + forcez);
+    x[18] = omega1 * x[18] + (omega * de19);
+}
+
+// Physical constants of one run, rounded to the arithmetic type the way
+// CODE/SRC/hencol.F90:30-39 rounds them to mykind.
+template <typename R>
+struct Phys {
+    R omega, omega1, fgrad, u_inflow, force;
+};
+
+}  // namespace eup

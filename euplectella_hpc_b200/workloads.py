@@ -1,0 +1,79 @@
+"""Synthetic workloads: lattice, geometry, boundary flags and physics of the
+named configurations.  There are no shipped geometry files for these sizes
+(the reference's production obstacles are unshipped ~1 GB .dat files), so each
+geometry is voxelised from a seed-parameterised analytic description and the
+initial state is a seeded equilibrium injected the way the reference restarts
+from restore.*.bin.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import (FREESLIP, FP32, INFLOW, OUTFLOW, PERIODIC, Config, geometry_cylinder_z,
+               geometry_reticular_shell, init_equilibrium)
+
+U_IN = 0.05          # inlet velocity of every configuration
+PERTURBATION = 1e-4  # amplitude of the seeded initial velocity perturbation
+
+
+def svisc_for(re: float, u: float, d: float) -> float:
+    """Kinematic viscosity for Reynolds number re = u d / nu."""
+    return u * d / re
+
+
+@dataclasses.dataclass
+class Workload:
+    name: str
+    cfg: Config
+    obs: np.ndarray
+    steps: int
+    seed: int
+    probes: list = dataclasses.field(default_factory=list)
+    cavity: np.ndarray | None = None  # boolean mask (n, m, l) of the body cavity
+
+    def initial_state(self, dtype=np.float32) -> np.ndarray:
+        c = self.cfg
+        return init_equilibrium(c.lx, c.ly, c.lz, U_IN, PERTURBATION, self.seed, dtype)
+
+    @property
+    def nodes(self) -> int:
+        return self.cfg.lx * self.cfg.ly * self.cfg.lz
+
+
+def cylinder_channel(lx=256, ly=128, lz=64, d=20.0, xc=64.0, yc=64.0, re=100.0, steps=2000, seed=1234,
+                     precision=FP32) -> Workload:
+    """Channel with a solid circular cylinder, axis along z: inlet u=0.05 at x=0,
+    zero-gradient (equilibrium) outlet, free-slip y, periodic z (256x128x64, D=20, Re=100)."""
+    nu = svisc_for(re, U_IN, d)
+    cfg = Config(lx, ly, lz, bc=(OUTFLOW, INFLOW, FREESLIP, FREESLIP, PERIODIC, PERIODIC), svisc=nu,
+                 u_inflow=U_IN, precision=precision, cd_rho0=1.0, cd_uref=U_IN, cd_length=d, cd_span=float(lz))
+    obs = geometry_cylinder_z(lx, ly, lz, xc, yc, 0.5 * d)
+    probes = [(int(xc + 2 * d), int(yc), lz // 2), (int(xc + 4 * d), int(yc + d // 2), lz // 2)]
+    return Workload("cylinder_256x128x64_re100", cfg, obs, steps, seed, probes)
+
+
+def reticular_shell_channel(lx=768, ly=384, lz=384, outer_d=96.0, length=256.0, strut_d=4.0, pitch=16.0,
+                            re=2000.0, steps=20000, seed=2024, precision=FP32) -> Workload:
+    """Channel 768x384x384 with a reticular cylindrical shell (outer D 96, length 256,
+    axis x, struts d=4 at pitch 16 plus diagonals in alternate cells), inlet 0.05,
+    free-slip y and z (the reference's FREESLIP preset, CODE/SRC/build.bcond.F90:286-315),
+    Re 2000 on the shell diameter."""
+    nu = svisc_for(re, U_IN, outer_d)
+    x0 = lx / 4.0
+    yc = zc = (ly + 1) / 2.0
+    area = math.pi * outer_d * outer_d / 4.0  # frontal disc
+    cfg = Config(lx, ly, lz, bc=(OUTFLOW, INFLOW, FREESLIP, FREESLIP, FREESLIP, FREESLIP), svisc=nu,
+                 u_inflow=U_IN, precision=precision, cd_rho0=1.0, cd_uref=U_IN, cd_length=outer_d,
+                 cd_span=area / outer_d)
+    obs = geometry_reticular_shell(lx, ly, lz, x0, length, yc, zc, outer_d, strut_d, pitch, seed)
+    yi, zi = int(round(yc)), int(round(zc))
+    probes = [(int(x0 - 32), yi, zi), (int(x0 + length / 2), yi, zi), (int(x0 + length + 64), yi, zi)]
+    # cavity: inside the strut centreline radius minus a strut radius, within the shell's x span
+    k, j, i = np.meshgrid(np.arange(1, lz + 1), np.arange(1, ly + 1), np.arange(1, lx + 1), indexing="ij",
+                          sparse=True)
+    rin = 0.5 * outer_d - strut_d
+    cavity = ((j - yc) ** 2 + (k - zc) ** 2 < rin * rin) & (i >= x0) & (i <= x0 + length)
+    return Workload("reticular_shell_768x384x384_re2000", cfg, obs, steps, seed, probes, cavity)

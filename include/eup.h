@@ -1,0 +1,243 @@
+/*
+ * eup.h -- C ABI of the B200 (sm_100a) D3Q19 BGK lattice-Boltzmann time step.
+ *
+ * Drop-in for the time-step loop of giacomofalcucci/Euplectella_HPC
+ * (CODE/SRC/bgk3d.F90:114-152).  The reference's Fortran driver keeps its
+ * input files, its arrays a01..a19(0:l+1,0:m+1,0:n+1) and its output layout;
+ * a `bind(c)` interface (fortran/eup_mod.F90) calls these entry points in
+ * place of boundaries/propagation/collision.  Plain pointers and sizes only;
+ * every entry point returns an eup_status (0 = success) and never aborts,
+ * exits or throws.
+ *
+ * Conventions shared with the reference:
+ *  - population q = 1..19 is the reference's aQQ; arrays passed as `pops[19]`
+ *    are indexed q-1 and velocity q is the table of CODE/SRC/bgk3d.F90:30-49;
+ *  - every population array is haloed, Fortran order (i fastest), extent
+ *    (l+2)*(m+2)*(n+2) elements, element type float (4 bytes, the reference's
+ *    default mykind) or double (8 bytes, -DDOUBLE_P);
+ *  - `obs` is obs(1:l,1:m,1:n), int32, Fortran order, value 1 = solid;
+ *  - boundary flags use the reference codes of CODE/SRC/build.bcond.F90:11-17.
+ *
+ * Threading: one host thread per handle (the reference runs one MPI rank per
+ * GPU, MPI_THREAD_SINGLE).  Calls on one handle are serialised.  eup_step is
+ * asynchronous on the handle's stream; entry points that return data
+ * synchronise.  Host arrays belong to the caller and are never retained.
+ */
+#ifndef EUP_H
+#define EUP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EUP_ABI_VERSION 1
+
+typedef enum eup_status {
+    EUP_OK = 0,
+    EUP_ERR_INVALID_ARG = 1,    /* bad pointer, size, flag or call order */
+    EUP_ERR_CUDA = 2,           /* a CUDA runtime call failed; text in eup_last_error */
+    EUP_ERR_OOM = 3,            /* device or pinned-host allocation failed */
+    EUP_ERR_DIVERGED = 4,       /* a monitored FP64 sum is not finite */
+    EUP_ERR_UNSUPPORTED = 5,    /* valid in the reference but not offered here (text says why) */
+    EUP_ERR_IO = 6,             /* file missing, short or malformed */
+    EUP_ERR_NO_DEVICE = 7       /* no usable CUDA device */
+} eup_status;
+
+/* Boundary flag codes (CODE/SRC/build.bcond.F90:11-17). */
+enum {
+    EUP_BC_PERIODIC = 0,
+    EUP_BC_NOSLIP = 1,
+    EUP_BC_LID = 2,       /* up face only */
+    EUP_BC_FREESLIP = 3,  /* up/down/left/right */
+    EUP_BC_INFLOW = 4,    /* rear face only */
+    EUP_BC_OUTFLOW = 5    /* front face only */
+};
+
+/* Face order of eup_config.bc (reference names front/rear/right/left/up/down). */
+enum { EUP_FRONT = 0, EUP_REAR = 1, EUP_RIGHT = 2, EUP_LEFT = 3, EUP_UP = 4, EUP_DOWN = 5 };
+
+/* Population storage in device memory. */
+typedef enum eup_precision {
+    EUP_FP32 = 0,       /* float storage and arithmetic (the reference's default) */
+    EUP_FP64 = 1,       /* double storage and arithmetic (-DDOUBLE_P) */
+    EUP_FP16_DEV = 2,   /* half storage of (f_q - w_q)*scale, float arithmetic */
+    EUP_BF16_DEV = 3    /* bfloat16 storage of (f_q - w_q)*scale, float arithmetic */
+} eup_precision;
+
+typedef struct eup_config {
+    int32_t lx, ly, lz;     /* lattice nodes (one GPU: l=lx, m=ly, n=lz) */
+    int32_t bc[6];          /* reference flag per face, order EUP_FRONT..EUP_DOWN */
+    double svisc;           /* kinematic viscosity; omega = 2/(6 svisc+1) as in CODE/SRC/hencol.F90:30 */
+    double u0;              /* body-force scale; fgrad = 4 u0 svisc/(5 lz^2), CODE/SRC/hencol.F90:37 (0 with an inlet) */
+    double u_inflow;        /* inlet velocity of EUP_BC_INFLOW, CODE/SRC/bcond.bc.F90:262 */
+    double u00;             /* lid velocity scale, force = u00/6, CODE/SRC/bcond.bc.F90:50-56 */
+    int32_t precision;      /* eup_precision */
+    int32_t device;         /* CUDA device ordinal */
+    double dev_scale;       /* scale of the 16-bit deviation storage; 0 selects 4096 */
+    /* drag coefficient normalisation C_d = F_x / (0.5 rho0 u_ref^2 length span) */
+    double cd_rho0, cd_uref, cd_length, cd_span;
+    int64_t series_capacity;  /* force history entries kept on the device; 0 selects 1<<20 */
+} eup_config;
+
+typedef struct eup_handle eup_handle;
+
+/* ---- life cycle --------------------------------------------------------- */
+
+/* Library ABI version (EUP_ABI_VERSION). */
+int32_t eup_abi_version(void);
+
+/* Number of usable CUDA devices, 0 when none (never fails). */
+int32_t eup_device_count(void);
+
+/* Creates a solver on cfg->device and allocates both population lattices, the
+ * halo shell and the diagnostic buffers.  Replaces the set-up half of
+ * CODE/SRC/initialize.F90:22-158 (build_bcond, alloca, hencol). */
+int eup_create(const eup_config* cfg, eup_handle** out);
+
+/* Frees every device resource of the handle; h may be NULL. */
+int eup_destroy(eup_handle* h);
+
+/* Text of the last failure on h (h == NULL: last failure of eup_create or of
+ * a handle-less call on this thread).  Valid until the next call. */
+const char* eup_last_error(const eup_handle* h);
+
+/* ---- state ---------------------------------------------------------------- */
+
+/* Installs the solid mask obs(1:l,1:m,1:n) (1 = solid): builds the bit-packed
+ * mask, the list of solid voxels adjacent to fluid or halo, and the bounding
+ * box.  Replaces CODE/SRC/build.obs.F90:33-194 as consumed by
+ * CODE/SRC/bcond.obs.F90:47-77.  Solid voxels on the outflow plane i = l are
+ * rejected (EUP_ERR_UNSUPPORTED): there the reference's result depends on the
+ * iteration order of its bounce-back loop. */
+int eup_set_obstacles(eup_handle* h, const int32_t* obs);
+
+/* Copies the 19 haloed host arrays (elem_bytes 4 or 8) into device storage:
+ * interior nodes into the lattice (converted to the storage precision), halo
+ * nodes into the persistent halo shell.  Replaces the host-to-device copy of
+ * CODE/SRC/bgk3d.F90:113 / CODE/SRC/initialize.F90:164-175; also the
+ * restart path (CODE/SRC/restore_raw.F90:43-63).  Sets the step counter. */
+int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, int64_t itime);
+
+/* Copies the current state back into 19 haloed host arrays: the interior from
+ * the lattice, the halo from the halo shell, exactly what the reference's
+ * arrays hold after a step.  Replaces the device-to-host copies of
+ * CODE/SRC/diagnostic.F90:47-58,110-120,163-174 and CODE/SRC/bgk3d.F90:153. */
+int eup_download(eup_handle* h, void* const pops[19], int32_t elem_bytes);
+
+/* ---- time step ------------------------------------------------------------ */
+
+/* Advances nsteps time steps of CODE/SRC/bgk3d.F90:128-138: bounce-back on
+ * solid voxels (CODE/SRC/bcond.obs.F90), halo planes in the reference's order
+ * (CODE/SRC/bcond.bc.F90), then one fused pull stream-collide kernel
+ * (CODE/SRC/movef.F90 + CODE/SRC/col.F90).  The momentum-exchange force of
+ * every state reached is recorded in FP64.  Asynchronous. */
+int eup_step(eup_handle* h, int32_t nsteps);
+
+/* Same work as eup_step, with CUDA events on the handle's stream around each
+ * phase; adds to ms[0..2] the device milliseconds spent in bounce-back + drag,
+ * halo planes and stream-collide over the nsteps, and sets ms[3] to the
+ * elapsed device time of the whole call.  Synchronises.  Replaces the phase
+ * timers of CODE/SRC/boundaries.F90, propagation.F90 and collision.F90
+ * (time_obs, time_bc, time_move, time_coll of CODE/SRC/finalize.F90:58-124). */
+int eup_step_profiled(eup_handle* h, int32_t nsteps, double ms[4]);
+
+/* Waits for all work queued on the handle; reports deferred CUDA errors. */
+int eup_synchronize(eup_handle* h);
+
+/* The handle's CUDA stream (a cudaStream_t), so callers can order their own
+ * device work, events or copies with the solver's. */
+int eup_get_stream(eup_handle* h, void** stream);
+
+/* Number of CUDA kernels the time-step entry points have launched on this
+ * handle so far (bounce-back/drag, halo planes, stream-collide). */
+int eup_get_launch_count(eup_handle* h, int64_t* launches);
+
+/* Current step counter (itime of the state held on the device). */
+int eup_get_itime(eup_handle* h, int64_t* itime);
+
+/* ---- diagnostics ---------------------------------------------------------- */
+
+/* Momentum-exchange force on the solid for the current state, FP64:
+ * F = sum over fluid nodes x and directions q with solid neighbour x + c_q
+ * (wrapped across periodic axes) of 2 c_q f_q(x), post-collision.  No
+ * reference counterpart (the reference's drag is CODE/SRC/drag.F90:33-79). */
+int eup_get_forces(eup_handle* h, double fxyz[3]);
+
+/* Force history: entries for steps first_step .. first_step+count-1 (step t =
+ * the state after t time steps), 3 doubles each.  Steps older than the ring
+ * capacity or not yet reached are EUP_ERR_INVALID_ARG. */
+int eup_get_force_series(eup_handle* h, int64_t first_step, int32_t count, double* fxyz);
+
+/* Drag coefficient history C_d(t) = F_x/(0.5 cd_rho0 cd_uref^2 cd_length cd_span). */
+int eup_get_cd_series(eup_handle* h, int64_t first_step, int32_t count, double* cd);
+
+/* Global sums of CODE/SRC/diagno.F90:67-120 in FP64 over the interior, solid
+ * voxels counted as rho = 1, u = 0: out = {sum rho, sum ux, sum uy, sum uz,
+ * sum u^2}.  EUP_ERR_DIVERGED when any sum is not finite. */
+int eup_get_monitor(eup_handle* h, double out[5]);
+
+/* rho, ux, uy, uz (FP64) at npts interior nodes (1-based i,j,k triples), as
+ * CODE/SRC/probe_global.F90:58-77 computes them. */
+int eup_get_probes(eup_handle* h, int32_t npts, const int32_t* ijk, double* rho_u);
+
+/* Link classification per interior node (Fortran order): bit q-1 set when the
+ * node is fluid and x - c_q is an interior solid voxel (its pull is served by
+ * bounce-back); bit 31 marks a solid voxel. */
+int eup_get_links(eup_handle* h, uint32_t* links);
+
+/* Interior linear indices (i-1 + l*(j-1 + m*(k-1))) of the solid voxels that
+ * touch fluid or halo, ascending.  *count receives the total; at most cap
+ * entries are written. */
+int eup_get_boundary_solid(eup_handle* h, int64_t* list, int64_t cap, int64_t* count);
+
+/* ---- host utilities (no GPU) ---------------------------------------------- */
+
+/* Reads obs.RRRR.TTTTTTTT.bin (CODE/SRC/build.obs.F90:147-177): Fortran
+ * unformatted sequential, record 1 = nobs, then nobs records of (i,j,k).
+ * Fills obs(1:l,1:m,1:n) with 0/1; *nobs receives the count. */
+int eup_read_obs_file(const char* path, int32_t l, int32_t m, int32_t n, int32_t* obs,
+                      int64_t* nobs);
+
+/* Writes obs in the same format (CODE/SRC/build.obs.F90:506-541). */
+int eup_write_obs_file(const char* path, int32_t l, int32_t m, int32_t n, const int32_t* obs);
+
+/* Reads restore.XX.YY.ZZ.bin / save.*.bin (CODE/SRC/restore_raw.F90:43-63,
+ * CODE/SRC/save_raw.F90:54-74): record 1 = itime, then 19 records of the
+ * haloed arrays. */
+int eup_read_raw_state(const char* path, int32_t l, int32_t m, int32_t n, int32_t elem_bytes,
+                       void* const pops[19], int64_t* itime);
+
+/* Writes the same format (CODE/SRC/save_raw.F90:54-74). */
+int eup_write_raw_state(const char* path, int32_t l, int32_t m, int32_t n, int32_t elem_bytes,
+                        const void* const pops[19], int64_t itime);
+
+/* Equilibrium state of CODE/SRC/init.F90:194-232 with rho = 1 and
+ * u = (u_in + amp*xi_x, amp*xi_y, amp*xi_z), xi uniform in [-1,1) from
+ * splitmix64(seed + 3 L + c) (L haloed linear index, c the component), halos
+ * included.  The synthetic workloads inject it through eup_upload the way the
+ * reference restarts from restore.*.bin. */
+int eup_init_equilibrium(int32_t l, int32_t m, int32_t n, double u_in, double amp, uint64_t seed,
+                         int32_t elem_bytes, void* const pops[19]);
+
+/* ---- synthetic geometries (no GPU) ---------------------------------------- */
+
+/* Solid circular cylinder with axis along z: node (i,j,k) is solid when
+ * (i-xc)^2 + (j-yc)^2 <= r^2 (1-based node coordinates). */
+int eup_geometry_cylinder_z(int32_t l, int32_t m, int32_t n, double xc, double yc, double r,
+                            int32_t* obs);
+
+/* Reticular cylindrical shell with its axis along x (Euplectella-like
+ * lattice): cylindrical struts of diameter strut_d on the shell of outer
+ * diameter outer_d, a square grid of pitch `pitch` (longitudinal struts and
+ * rings) plus both diagonals in alternate cells; the shell spans x0..x0+length
+ * and is centred at (yc, zc).  seed sets the angular phase of the grid. */
+int eup_geometry_reticular_shell(int32_t l, int32_t m, int32_t n, double x0, double length,
+                                 double yc, double zc, double outer_d, double strut_d,
+                                 double pitch, uint64_t seed, int32_t* obs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EUP_H */

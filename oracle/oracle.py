@@ -1,0 +1,186 @@
+"""ctypes harness for the CPU ORACLE (test infrastructure only).
+
+The oracle (oracle/orc.c, oracle/orc_impl.h) is a plain-C restatement of the
+reference's serial D3Q19 BGK step; it is the checker for the CUDA path and the
+CPU baseline leg of the benchmark.  Nothing in the product package imports
+this module.  PARITY STATUS: parity unpinned (the reference has no tests or
+golden vectors and cannot be compiled here).
+
+Arrays follow the reference layout: populations as one numpy array of shape
+(19, n+2, m+2, l+2) -- C order with the last axis fastest, i.e. the Fortran
+arrays a01..a19(0:l+1, 0:m+1, 0:n+1) of CODE/SRC/alloca.F90:94-132 stacked.
+`obs` has shape (n, m, l), 1 = solid.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liborc.so")
+
+FRONT, REAR, RIGHT, LEFT, UP, DOWN = range(6)
+PERIODIC, NOSLIP, LID, FREESLIP, INFLOW, OUTFLOW = range(6)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("l", ctypes.c_int32), ("m", ctypes.c_int32), ("n", ctypes.c_int32),
+        ("bc", ctypes.c_int32 * 6),
+        ("svisc", ctypes.c_double), ("u0", ctypes.c_double),
+        ("u_inflow", ctypes.c_double), ("u00", ctypes.c_double),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle library in place (make -C oracle)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        PP = ctypes.POINTER(ctypes.c_void_p)
+        for pfx in ("f", "d"):
+            getattr(L, f"orc_{pfx}_run").argtypes = [ctypes.POINTER(Params), PP, PP, ctypes.c_void_p, ctypes.c_int32]
+            getattr(L, f"orc_{pfx}_run").restype = ctypes.c_int
+            for nm in ("bcond_obs",):
+                getattr(L, f"orc_{pfx}_{nm}").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_void_p]
+            getattr(L, f"orc_{pfx}_bcond_bc").argtypes = [ctypes.POINTER(Params), PP]
+            getattr(L, f"orc_{pfx}_movef").argtypes = [ctypes.POINTER(Params), PP, PP]
+            getattr(L, f"orc_{pfx}_col").argtypes = [ctypes.POINTER(Params), PP, PP]
+            getattr(L, f"orc_{pfx}_init_perturbed").argtypes = [
+                ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                ctypes.c_uint64, PP]
+            getattr(L, f"orc_{pfx}_mem_force").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_void_p, ctypes.c_void_p]
+            getattr(L, f"orc_{pfx}_monitor").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_void_p, ctypes.c_void_p]
+            getattr(L, f"orc_{pfx}_macro").argtypes = [ctypes.POINTER(Params), PP] + [ctypes.c_void_p] * 4
+            getattr(L, f"orc_{pfx}_constants").argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_links.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_boundary_solid.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_boundary_solid.restype = ctypes.c_int64
+        L.orc_splitmix64.argtypes = [ctypes.c_uint64]
+        L.orc_splitmix64.restype = ctypes.c_uint64
+        L.orc_nthreads.restype = ctypes.c_int32
+        _lib = L
+    return _lib
+
+
+def params(l, m, n, bc, svisc, u0=0.0, u_inflow=0.0, u00=0.0) -> Params:
+    p = Params()
+    p.l, p.m, p.n = l, m, n
+    for f in range(6):
+        p.bc[f] = int(bc[f])
+    p.svisc, p.u0, p.u_inflow, p.u00 = float(svisc), float(u0), float(u_inflow), float(u00)
+    return p
+
+
+def _pfx(arr: np.ndarray) -> str:
+    if arr.dtype == np.float32:
+        return "f"
+    if arr.dtype == np.float64:
+        return "d"
+    raise TypeError(f"populations must be float32 or float64, got {arr.dtype}")
+
+
+def _ptrs(arr: np.ndarray):
+    assert arr.flags["C_CONTIGUOUS"] and arr.shape[0] == 19
+    return (ctypes.c_void_p * 19)(*[arr[q].ctypes.data for q in range(19)])
+
+
+def _obs_ptr(obs):
+    if obs is None:
+        return None
+    assert obs.dtype == np.int32 and obs.flags["C_CONTIGUOUS"]
+    return obs.ctypes.data
+
+
+def new_state(l, m, n, dtype=np.float32) -> np.ndarray:
+    # CODE/SRC/alloca.F90:134-172 fills fresh arrays with huge(); every value read
+    # by the step is overwritten by init or restore before use.
+    return np.full((19, n + 2, m + 2, l + 2), 3.0e38 if dtype == np.float32 else 1.0e300, dtype=dtype)
+
+
+def init_perturbed(l, m, n, u_in, amp, seed, dtype=np.float32) -> np.ndarray:
+    a = new_state(l, m, n, dtype)
+    getattr(lib(), f"orc_{_pfx(a)}_init_perturbed")(l, m, n, u_in, amp, seed, _ptrs(a))
+    return a
+
+
+def run(p: Params, a: np.ndarray, obs: np.ndarray | None, nsteps: int, b: np.ndarray | None = None) -> np.ndarray:
+    """Advance `a` in place by nsteps reference time steps; returns the scratch b."""
+    if b is None:
+        b = np.zeros_like(a)
+    rc = getattr(lib(), f"orc_{_pfx(a)}_run")(ctypes.byref(p), _ptrs(a), _ptrs(b), _obs_ptr(obs), nsteps)
+    assert rc == 0
+    return b
+
+
+def bcond_obs(p, a, obs):
+    getattr(lib(), f"orc_{_pfx(a)}_bcond_obs")(ctypes.byref(p), _ptrs(a), _obs_ptr(obs))
+
+
+def bcond_bc(p, a):
+    getattr(lib(), f"orc_{_pfx(a)}_bcond_bc")(ctypes.byref(p), _ptrs(a))
+
+
+def movef(p, a, b):
+    getattr(lib(), f"orc_{_pfx(a)}_movef")(ctypes.byref(p), _ptrs(a), _ptrs(b))
+
+
+def col(p, a, b):
+    getattr(lib(), f"orc_{_pfx(a)}_col")(ctypes.byref(p), _ptrs(a), _ptrs(b))
+
+
+def constants(p, dtype=np.float32):
+    o = np.zeros(1, dtype=dtype)
+    f = np.zeros(1, dtype=dtype)
+    getattr(lib(), f"orc_{'f' if dtype == np.float32 else 'd'}_constants")(ctypes.byref(p), o.ctypes.data, f.ctypes.data)
+    return o[0], f[0]
+
+
+def mem_force(p, a, obs) -> np.ndarray:
+    out = np.zeros(3, dtype=np.float64)
+    getattr(lib(), f"orc_{_pfx(a)}_mem_force")(ctypes.byref(p), _ptrs(a), _obs_ptr(obs), out.ctypes.data)
+    return out
+
+
+def monitor(p, a, obs) -> np.ndarray:
+    out = np.zeros(5, dtype=np.float64)
+    getattr(lib(), f"orc_{_pfx(a)}_monitor")(ctypes.byref(p), _ptrs(a), _obs_ptr(obs), out.ctypes.data)
+    return out
+
+
+def macro(p, a):
+    shp = (p.n, p.m, p.l)
+    rho, ux, uy, uz = (np.zeros(shp, dtype=np.float64) for _ in range(4))
+    getattr(lib(), f"orc_{_pfx(a)}_macro")(ctypes.byref(p), _ptrs(a), rho.ctypes.data, ux.ctypes.data,
+                                           uy.ctypes.data, uz.ctypes.data)
+    return rho, ux, uy, uz
+
+
+def links(p, obs) -> np.ndarray:
+    out = np.zeros((p.n, p.m, p.l), dtype=np.uint32)
+    lib().orc_links(ctypes.byref(p), _obs_ptr(obs), out.ctypes.data)
+    return out
+
+
+def boundary_solid(p, obs) -> np.ndarray:
+    cnt = lib().orc_boundary_solid(ctypes.byref(p), _obs_ptr(obs), None)
+    out = np.zeros(max(cnt, 1), dtype=np.int64)
+    lib().orc_boundary_solid(ctypes.byref(p), _obs_ptr(obs), out.ctypes.data)
+    return out[:cnt]
+
+
+def nthreads() -> int:
+    return int(lib().orc_nthreads())

@@ -1,0 +1,197 @@
+"""GPU parity: the sm_100a step, called through the C ABI, against the CPU
+oracle on the same seeded inputs.
+
+FP32 and FP64 are compared bit for bit on every value the reference's fluid
+can observe: the full haloed arrays (interior and halo) except interior solid
+voxels, whose values in the reference depend on the iteration order of its
+racy bounce-back loop and are never read by a fluid node.  Forces and monitor
+sums are FP64 reductions whose summation order differs (relative 1e-12).
+"""
+import numpy as np
+import pytest
+
+from conftest import fluid_mask_haloed
+
+pytestmark = pytest.mark.gpu
+
+# (name, (lx,ly,lz), bc, svisc, u0, u_inflow, u00, obstacle builder)
+def _cyl(l, m, n):
+    k, j, i = np.meshgrid(np.arange(1, n + 1), np.arange(1, m + 1), np.arange(1, l + 1), indexing="ij")
+    return (((i - l / 3) ** 2 + (j - m / 2) ** 2) <= (m / 6) ** 2).astype(np.int32)
+
+
+def _block(l, m, n):
+    obs = np.zeros((n, m, l), np.int32)
+    obs[n // 3:2 * n // 3 + 1, m // 3:2 * m // 3 + 1, l // 3:l // 3 + 3] = 1
+    return obs
+
+
+def _wall_touch(l, m, n):
+    # obstacle touching the y = 1 and z = 1, z = n faces (periodic / free-slip planes)
+    obs = np.zeros((n, m, l), np.int32)
+    obs[:, 0:3, l // 3:l // 3 + 2] = 1
+    obs[0, m // 2, l // 2] = 1
+    return obs
+
+
+CASES = [
+    ("cylinder_inout_freeslipY_periodicZ", (24, 16, 8), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
+    ("shell_freeslip_all", (28, 14, 12), (5, 4, 3, 3, 3, 3), 0.0024, 0.0, 0.05, 0.0, _block),
+    ("closed_noslip_box", (16, 12, 10), (1, 1, 1, 1, 1, 1), 0.02, 0.0, 0.0, 0.0, _block),
+    ("lid_driven", (16, 12, 10), (1, 1, 1, 1, 2, 1), 0.02, 0.0, 0.0, 0.1, None),
+    ("periodic_x_body_force", (20, 12, 10), (0, 0, 3, 3, 1, 1), 0.05, 0.05, 0.0, 0.0, _block),
+    ("all_periodic", (12, 10, 8), (0, 0, 0, 0, 0, 0), 0.01, 0.0, 0.0, 0.0, _block),
+    ("obstacle_on_faces", (24, 12, 10), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _wall_touch),
+    ("noslip_y_periodic_z_inflow", (20, 10, 9), (5, 4, 1, 1, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
+    ("freeslip_z_periodic_y", (20, 10, 9), (5, 4, 0, 0, 3, 3), 0.01, 0.0, 0.05, 0.0, _cyl),
+]
+
+
+def _run_pair(eup, orc, case, dtype, steps, precision):
+    name, (l, m, n), bc, svisc, u0, uin, u00, builder = case
+    obs = builder(l, m, n) if builder else np.zeros((n, m, l), np.int32)
+    a = eup.init_equilibrium(l, m, n, max(uin, 0.02), 1e-3, 4321, dtype)
+    p = orc.params(l, m, n, bc, svisc=svisc, u0=u0, u_inflow=uin, u00=u00)
+    cfg = eup.Config(l, m, n, bc=bc, svisc=svisc, u0=u0, u_inflow=uin, u00=u00, precision=precision)
+    with eup.Solver(cfg) as s:
+        s.set_obstacles(obs)
+        s.upload(a)
+        s.step(steps)
+        got = s.download(dtype)
+        f_gpu = s.forces()
+        mon_gpu = s.monitor()
+        series = s.force_series(0, steps + 1)
+    ref = a.copy()
+    orc.run(p, ref, obs, steps)
+    return obs, p, got, ref, f_gpu, mon_gpu, series
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_step_bit_exact(eup, orc, require_gpu, case, prec):
+    dtype, precision = (np.float32, eup.FP32) if prec == "fp32" else (np.float64, eup.FP64)
+    obs, p, got, ref, f_gpu, mon_gpu, _ = _run_pair(eup, orc, case, dtype, 25, precision)
+    keep = fluid_mask_haloed(obs)
+    for q in range(19):
+        bad = (got[q] != ref[q]) & keep
+        assert not bad.any(), f"population {q + 1}: {bad.sum()} mismatches, first at {np.argwhere(bad)[0]}"
+    f_ref = orc.mem_force(p, ref, obs)
+    np.testing.assert_allclose(f_gpu, f_ref, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(mon_gpu, orc.monitor(p, ref, obs), rtol=1e-12, atol=1e-10)
+
+
+def test_force_series_every_step(eup, orc, require_gpu):
+    case = CASES[0]
+    name, (l, m, n), bc, svisc, u0, uin, u00, builder = case
+    obs = builder(l, m, n)
+    a = eup.init_equilibrium(l, m, n, uin, 1e-3, 99, np.float32)
+    p = orc.params(l, m, n, bc, svisc=svisc, u_inflow=uin)
+    cfg = eup.Config(l, m, n, bc=bc, svisc=svisc, u_inflow=uin, cd_uref=uin, cd_length=m / 3, cd_span=n)
+    ref = a.copy()
+    expect = [orc.mem_force(p, ref, obs)]
+    for _ in range(12):
+        orc.run(p, ref, obs, 1)
+        expect.append(orc.mem_force(p, ref, obs))
+    with eup.Solver(cfg) as s:
+        s.set_obstacles(obs)
+        s.upload(a)
+        for chunk in (1, 4, 7):
+            s.step(chunk)
+        assert s.itime == 12
+        series = s.force_series(0, 13)
+        cd = s.cd_series(0, 13)
+    np.testing.assert_allclose(series, np.array(expect), rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(cd, series[:, 0] / (0.5 * uin * uin * (m / 3) * n), rtol=1e-15)
+
+
+def test_links_and_boundary_list_match_oracle(eup, orc, require_gpu):
+    for case in CASES:
+        name, (l, m, n), bc, *_rest, builder = case
+        if builder is None:
+            continue
+        obs = builder(l, m, n)
+        p = orc.params(l, m, n, bc, svisc=0.01)
+        with eup.Solver(eup.Config(l, m, n, bc=bc)) as s:
+            s.set_obstacles(obs)
+            assert np.array_equal(s.links(), orc.links(p, obs)), name
+            assert np.array_equal(s.boundary_solid(), orc.boundary_solid(p, obs)), name
+
+
+def test_upload_download_round_trip(eup, require_gpu):
+    l, m, n = 20, 9, 7
+    for dt, prec in ((np.float32, eup.FP32), (np.float64, eup.FP64)):
+        a = eup.init_equilibrium(l, m, n, 0.05, 1e-3, 5, dt)
+        with eup.Solver(eup.Config(l, m, n, precision=prec)) as s:
+            s.upload(a, itime=17)
+            assert s.itime == 17
+            assert np.array_equal(s.download(dt), a)
+
+
+def test_probes_match_oracle(eup, orc, require_gpu):
+    case = CASES[0]
+    name, (l, m, n), bc, svisc, u0, uin, u00, builder = case
+    obs = builder(l, m, n)
+    a = eup.init_equilibrium(l, m, n, uin, 1e-3, 7, np.float32)
+    p = orc.params(l, m, n, bc, svisc=svisc, u_inflow=uin)
+    pts = [(1, 1, 1), (l, m, n), (l // 2, 3, 4), (20, 15, 2)]
+    with eup.Solver(eup.Config(l, m, n, bc=bc, svisc=svisc, u_inflow=uin)) as s:
+        s.set_obstacles(obs)
+        s.upload(a)
+        s.step(9)
+        got = s.probes(pts)
+    orc.run(p, a, obs, 9)
+    rho, ux, uy, uz = orc.macro(p, a)
+    for t, (i, j, k) in enumerate(pts):
+        assert np.array_equal(got[t], [rho[k - 1, j - 1, i - 1], ux[k - 1, j - 1, i - 1],
+                                       uy[k - 1, j - 1, i - 1], uz[k - 1, j - 1, i - 1]])
+
+
+def test_error_paths(eup, require_gpu):
+    with eup.Solver(eup.Config(12, 8, 6)) as s:
+        with pytest.raises(eup.EupError) as e:
+            s.step(1)
+        assert e.value.code == 1
+        obs = np.zeros((6, 8, 12), np.int32)
+        obs[2, 3, 11] = 1  # on the outflow plane i = l
+        with pytest.raises(eup.EupError) as e:
+            s.set_obstacles(obs)
+        assert e.value.code == 5
+        with pytest.raises(eup.EupError):
+            s.probes([(0, 1, 1)])
+        s.upload(eup.init_equilibrium(12, 8, 6, 0.05, 0, 1))
+        with pytest.raises(eup.EupError):
+            s.force_series(0, 5)
+
+
+@pytest.mark.parametrize("prec", ["fp16", "bf16"])
+def test_deviation_storage_against_fp64(eup, require_gpu, prec):
+    """16-bit storage of (f - w)*scale with FP32 arithmetic, measured against the
+    FP64 run of the same kernel: velocity relative L2 and drag."""
+    l, m, n = 96, 48, 16
+    obs = eup.geometry_cylinder_z(l, m, n, 24, 24.5, 5)
+    cfg = dict(bc=(5, 4, 3, 3, 0, 0), svisc=0.05 * 10 / 100, u_inflow=0.05)
+    a64 = eup.init_equilibrium(l, m, n, 0.05, 1e-4, 1234, np.float64)
+    res = {}
+    for name, pr in (("fp64", eup.FP64), (prec, eup.FP16_DEV if prec == "fp16" else eup.BF16_DEV)):
+        with eup.Solver(eup.Config(l, m, n, precision=pr, **cfg)) as s:
+            s.set_obstacles(obs)
+            s.upload(a64)
+            s.step(400)
+            res[name] = (s.download(np.float64), s.force_series(300, 101))
+    ref, f_ref = res["fp64"]
+    got, f_got = res[prec]
+
+    def vel(x):
+        c = x[:, 1:-1, 1:-1, 1:-1]
+        rho = c.sum(0)
+        cx = np.array([1, 1, 1, 1, 1, 0, 0, 0, 0, -1, -1, -1, -1, -1, 0, 0, 0, 0, 0])
+        cy = np.array([-1, 0, 1, 0, 0, 0, 1, 1, 1, -1, 0, 1, 0, 0, 0, -1, -1, -1, 0])
+        return np.stack([np.tensordot(cx, c, 1) / rho, np.tensordot(cy, c, 1) / rho])
+
+    fluid = obs == 0
+    v_ref, v_got = vel(ref)[:, fluid], vel(got)[:, fluid]
+    rel_l2 = np.linalg.norm(v_got - v_ref) / np.linalg.norm(v_ref)
+    cd_err = abs(f_got[:, 0].mean() - f_ref[:, 0].mean()) / abs(f_ref[:, 0].mean())
+    tol_l2, tol_cd = (1e-3, 5e-3) if prec == "fp16" else (2e-2, 5e-2)
+    assert rel_l2 < tol_l2, rel_l2
+    assert cd_err < tol_cd, cd_err
