@@ -22,6 +22,9 @@ struct eup_handle {
     int64_t Nq = 0;
     void* lat[2] = {nullptr, nullptr};
     void* ghost = nullptr;
+    void* xface = nullptr;        // x = 1 / x = l columns, [2][18][m*n] arithmetic type
+    int64_t* d_itime = nullptr;   // device copy of the step counter (series slot of the drag)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one time step, source lattice 0 or 1
     int cur = 0;
     uint32_t* bits = nullptr;
     int wpr = 0;
@@ -37,8 +40,9 @@ struct eup_handle {
     int64_t itime = 0, series_first = 0;
     bool has_state = false;
     double scale = 1.0;
-    int variant = 0;
+    int variant = 0;  // EUP_STEP_VARIANT: bit 0 scalar stream-collide, bit 1 no CUDA graphs
     int64_t launches = 0;  // kernels launched by eup_step / eup_step_profiled
+    int launches_per_step = 0;
     std::string err;
 };
 
@@ -78,6 +82,7 @@ Lat<S, R> make_lat(const eup_handle* h, int which) {
     char* base = static_cast<char*>(h->lat[which]);
     for (int q = 0; q < Q; ++q) L.pop[q] = reinterpret_cast<S*>(base + (size_t)q * h->Nq * sizeof(S));
     L.ghost = static_cast<R*>(h->ghost);
+    L.xface = static_cast<R*>(h->xface);
     L.scale = (R)h->scale;
     L.inv_scale = (R)(1.0 / h->scale);
     return L;
@@ -99,18 +104,12 @@ Phys<R> make_phys(const eup_handle* h) {
 
 Mask make_mask(const eup_handle* h) { return Mask{h->bits, h->wpr}; }
 Reduce make_reduce(const eup_handle* h) { return Reduce{h->partials, h->counter, kReduceMaxBlocks}; }
-double* slot(const eup_handle* h, int64_t t) { return h->series + 3 * (t % h->cap); }
 
 template <typename S, typename R>
 void enqueue_drag_only(eup_handle* h) {
-    double* out = slot(h, h->itime);
-    if (h->nblist == 0) {
-        cudaMemsetAsync(out, 0, 3 * sizeof(double), h->stream);
-        return;
-    }
     const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
     launch_bounce_drag<S, R>(make_lat<S, R>(h, h->cur), h->g, make_mask(h), bc, h->blist, h->nblist, false,
-                             make_reduce(h), out, h->stream);
+                             make_reduce(h), h->series, h->cap, h->d_itime, false, h->stream);
 }
 
 // Events bracketing the phases of each step when profiling: ev[4*s + p].
@@ -121,35 +120,80 @@ struct PhaseEvents {
     }
 };
 
+// One time step from lattice `src_idx`: bounce-back + drag (advances the device
+// step counter), halo planes in the reference's order, stream-collide.
+// Returns the number of kernels launched.
 template <typename S, typename R>
-void enqueue_steps(eup_handle* h, int32_t nsteps, PhaseEvents* pe = nullptr) {
+int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
     const Phys<R> ph = make_phys<R>(h);
     const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
-    const Mask mk = make_mask(h);
-    const Reduce red = make_reduce(h);
-    for (int32_t s = 0; s < nsteps; ++s) {
-        const Lat<S, R> src = make_lat<S, R>(h, h->cur), dst = make_lat<S, R>(h, h->cur ^ 1);
-        if (pe) pe->mark(4 * (size_t)s + 0, h->stream);
-        // boundaries: bounce-back then halo planes (CODE/SRC/boundaries.F90:36-49,235-248)
-        if (h->nblist > 0) {
-            launch_bounce_drag<S, R>(src, h->g, mk, bc, h->blist, h->nblist, true, red, slot(h, h->itime),
-                                     h->stream);
-            h->launches += 1;
-        } else {
-            cudaMemsetAsync(slot(h, h->itime), 0, 3 * sizeof(double), h->stream);
+    const Lat<S, R> src = make_lat<S, R>(h, src_idx), dst = make_lat<S, R>(h, src_idx ^ 1);
+    int n = 0;
+    if (pe) pe->mark(4 * s + 0, h->stream);
+    // boundaries: bounce-back then halo planes (CODE/SRC/boundaries.F90:36-49,235-248)
+    launch_bounce_drag<S, R>(src, h->g, make_mask(h), bc, h->blist, h->nblist, true, make_reduce(h), h->series,
+                             h->cap, h->d_itime, true, h->stream);
+    n += 1;
+    if (pe) pe->mark(4 * s + 1, h->stream);
+    n += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
+    if (pe) pe->mark(4 * s + 2, h->stream);
+    // propagation + collision (CODE/SRC/bgk3d.F90:133-138)
+    launch_stream_collide<S, R>(src, dst, h->g, ph, h->variant, h->stream);
+    n += 1;
+    if (pe) pe->mark(4 * s + 3, h->stream);
+    return n;
+}
+
+template <typename S, typename R>
+cudaError_t capture_graphs(eup_handle* h, int* per_step) {
+    for (int p = 0; p < 2; ++p) {
+        if (h->graph[p]) continue;
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        *per_step = enqueue_one_step<S, R>(h, p, nullptr, 0);
+        e = cudaStreamEndCapture(h->stream, &graph);
+        if (e != cudaSuccess) return e;
+        e = cudaGraphInstantiate(&h->graph[p], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void drop_graphs(eup_handle* h) {
+    for (auto& g : h->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
         }
-        if (pe) pe->mark(4 * (size_t)s + 1, h->stream);
-        h->launches += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
-        if (pe) pe->mark(4 * (size_t)s + 2, h->stream);
-        // propagation + collision (CODE/SRC/bgk3d.F90:133-138)
-        launch_stream_collide<S, R>(src, dst, h->g, ph, h->variant, h->stream);
-        h->launches += 1;
-        if (pe) pe->mark(4 * (size_t)s + 3, h->stream);
-        h->cur ^= 1;
-        h->itime += 1;
+}
+
+template <typename S, typename R>
+cudaError_t enqueue_steps(eup_handle* h, int32_t nsteps, PhaseEvents* pe = nullptr) {
+    if (pe || (h->variant & 2)) {  // profiled, or graphs disabled (EUP_STEP_VARIANT bit 1)
+        for (int32_t s = 0; s < nsteps; ++s) {
+            h->launches += enqueue_one_step<S, R>(h, h->cur, pe, (size_t)s);
+            h->cur ^= 1;
+            h->itime += 1;
+        }
+    } else {
+        int per_step = 0;
+        cudaError_t e = capture_graphs<S, R>(h, &per_step);
+        if (e != cudaSuccess) return e;
+        if (per_step == 0) per_step = h->launches_per_step;
+        h->launches_per_step = per_step;
+        for (int32_t s = 0; s < nsteps; ++s) {
+            e = cudaGraphLaunch(h->graph[h->cur], h->stream);
+            if (e != cudaSuccess) return e;
+            h->launches += per_step;
+            h->cur ^= 1;
+            h->itime += 1;
+        }
     }
     enqueue_drag_only<S, R>(h);
-    if (h->nblist > 0) h->launches += 1;
+    h->launches += 1;
+    return cudaSuccess;
 }
 
 #define DISPATCH(h, FN, ...)                                                   \
@@ -161,6 +205,21 @@ void enqueue_steps(eup_handle* h, int32_t nsteps, PhaseEvents* pe = nullptr) {
             default: FN<__nv_bfloat16, float>(__VA_ARGS__); break;             \
         }                                                                      \
     } while (0)
+
+#define DISPATCH_RET(h, OUT, FN, ...)                                          \
+    do {                                                                       \
+        switch ((h)->prec) {                                                   \
+            case EUP_FP32: OUT = FN<float, float>(__VA_ARGS__); break;         \
+            case EUP_FP64: OUT = FN<double, double>(__VA_ARGS__); break;       \
+            case EUP_FP16_DEV: OUT = FN<__half, float>(__VA_ARGS__); break;    \
+            default: OUT = FN<__nv_bfloat16, float>(__VA_ARGS__); break;       \
+        }                                                                      \
+    } while (0)
+
+template <typename S, typename R>
+void fill_xface_dispatch(eup_handle* h) {
+    launch_fill_xface<S, R>(make_lat<S, R>(h, h->cur), h->g, h->stream);
+}
 
 template <typename S, typename R, typename T>
 void enqueue_upload_q(eup_handle* h, int q) {
@@ -289,6 +348,13 @@ int eup_create(const eup_config* cfg, eup_handle** out) {
     cudaMemsetAsync(h->series, 0, sizeof(double) * 3 * h->cap, h->stream);
     if ((e = cudaMalloc(&h->dscratch, sizeof(double) * 64)) != cudaSuccess)
         return cleanup_fail(cuda_fail(h, e, "cudaMalloc(scratch)"));
+    const size_t xface_bytes = (size_t)2 * 18 * h->g.m * h->g.n * h->rbytes;
+    if ((e = cudaMalloc(&h->xface, xface_bytes)) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMalloc(x-face copy)"));
+    cudaMemsetAsync(h->xface, 0, xface_bytes, h->stream);
+    if ((e = cudaMalloc(&h->d_itime, sizeof(int64_t))) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMalloc(step counter)"));
+    cudaMemsetAsync(h->d_itime, 0, sizeof(int64_t), h->stream);
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cleanup_fail(cuda_fail(h, e, "create"));
     *out = h;
     return EUP_OK;
@@ -298,8 +364,9 @@ int eup_destroy(eup_handle* h) {
     if (!h) return EUP_OK;
     cudaSetDevice(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graphs(h);
     void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->partials, h->counter, h->series,
-                    h->dscratch, h->staging};
+                    h->dscratch, h->staging, h->xface, h->d_itime};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -321,6 +388,8 @@ int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
                             "eup_set_obstacles: solid voxel on the outflow plane i=l; the reference's outflow "
                             "there reads values whose order its bounce-back loop leaves undefined");
     }
+    CK(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);  // the captured steps hold the old mask and list pointers
     if (h->bits) { cudaFree(h->bits); h->bits = nullptr; }
     if (h->blist) { cudaFree(h->blist); h->blist = nullptr; }
     h->nblist = 0;
@@ -362,6 +431,8 @@ int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, in
         CK(h, cudaMemcpyAsync(h->staging, pops[q], bytes, cudaMemcpyHostToDevice, h->stream));
         DISPATCH(h, upload_q, h, q, elem_bytes);
     }
+    CK(h, cudaMemcpyAsync(h->d_itime, &itime, sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+    DISPATCH(h, fill_xface_dispatch, h);
     h->itime = itime;
     h->series_first = itime;
     h->has_state = true;
@@ -397,7 +468,9 @@ int eup_step(eup_handle* h, int32_t nsteps) {
     if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_step: no state uploaded");
     if (nsteps < 0) return fail(h, EUP_ERR_INVALID_ARG, "eup_step: nsteps < 0");
     if (nsteps == 0) return EUP_OK;
-    DISPATCH(h, enqueue_steps, h, nsteps);
+    cudaError_t e = cudaSuccess;
+    DISPATCH_RET(h, e, enqueue_steps, h, nsteps);
+    if (e != cudaSuccess) return cuda_fail(h, e, "eup_step");
     CK(h, cudaGetLastError());
     return EUP_OK;
 }
@@ -411,9 +484,10 @@ int eup_step_profiled(eup_handle* h, int32_t nsteps, double ms[4]) {
     PhaseEvents pe;
     pe.ev.resize(4 * (size_t)nsteps + 1);
     for (auto& e : pe.ev) CK(h, cudaEventCreate(&e));
-    DISPATCH(h, enqueue_steps, h, nsteps, &pe);
+    cudaError_t e = cudaSuccess;
+    DISPATCH_RET(h, e, enqueue_steps, h, nsteps, &pe);
     pe.mark(pe.ev.size() - 1, h->stream);
-    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e == cudaSuccess) {
         for (int32_t s = 0; s < nsteps; ++s)

@@ -39,11 +39,16 @@ template <typename S, typename R>
 int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& ph, cudaStream_t st);
 
 // Bounce-back on solid voxels touching fluid/halo (CODE/SRC/bcond.obs.F90) and the
-// FP64 momentum-exchange force of the state it reads, written to force_out[3].
+// FP64 momentum-exchange force of the state it reads, written to
+// series[3*(*d_itime % cap)]; with `advance` the device step counter is incremented.
 template <typename S, typename R>
 void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const Mask& mk, const int bc[6],
                         const int32_t* list, int64_t nlist, bool do_bounce, const Reduce& red,
-                        double* force_out, cudaStream_t st);
+                        double* series, int64_t cap, int64_t* d_itime, bool advance, cudaStream_t st);
+
+// x-face copy of the current lattice (needed once after an upload).
+template <typename S, typename R>
+void launch_fill_xface(const Lat<S, R>& L, const Geo& g, cudaStream_t st);
 
 // Fused pull stream + collide (CODE/SRC/movef.F90 + CODE/SRC/col.F90): src -> dst.
 template <typename S, typename R>

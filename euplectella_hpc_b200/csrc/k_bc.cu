@@ -27,7 +27,12 @@ struct Range2 {
 
 constexpr int kTpb = 256;
 
-#define LD(q1, i, j, k) lat_load(L, g, (q1) - 1, (i), (j), (k))
+// Loads inside the halo kernels go through bc_load: interior nodes of the
+// x = 1 and x = l columns come from the compact x-face copy written by the
+// stream-collide kernel (coalesced in j), other interior nodes from the
+// lattice, halo nodes from the shell.  Every kernel issues all of a thread's
+// loads before its first store (stores to the shell may alias the loads).
+#define LD(q1, i, j, k) bc_load(L, g, (q1) - 1, (i), (j), (k))
 #define ST(q1, i, j, k, v) ghost_store(L, g, (q1) - 1, (i), (j), (k), (v))
 
 // ---- front wall, x = l+1 -----------------------------------------------------
@@ -37,18 +42,23 @@ __global__ void k_front(Lat<S, R> L, Geo g, Range2 r, int flag) {
     if (!r.get(j, k)) return;
     const int l = g.l, l1 = g.l + 1, m = g.m;
     if (flag == 0) {  // periodic, CODE/SRC/bcond.bc.F90:75-105 (SERIAL corner line :90)
-        if (j == 0) { ST(12, l1, 0, k, LD(12, 1, m, k)); return; }
-        for (int q = 10; q <= 14; ++q) ST(q, l1, j, k, LD(q, 1, j, k));
-    } else if (flag == 1) {  // no-slip, :108-124
-        ST(12, l1, j - 1, k, LD(1, l, j, k));
-        ST(13, l1, j, k - 1, LD(2, l, j, k));
-        ST(10, l1, j + 1, k, LD(3, l, j, k));
-        ST(11, l1, j, k + 1, LD(4, l, j, k));
-        ST(14, l1, j, k, LD(5, l, j, k));
-    } else {  // outflow, :127-169: equilibrium at rho=1 with the (un-normalised) momentum of x=l
-        R a[19];
+        if (j == 0) { const R v = LD(12, 1, m, k); ST(12, l1, 0, k, v); return; }
+        R v[5];
 #pragma unroll
-        for (int q = 0; q < 18; ++q) a[q] = lat_load(L, g, q, l, j, k);
+        for (int q = 10; q <= 14; ++q) v[q - 10] = LD(q, 1, j, k);
+#pragma unroll
+        for (int q = 10; q <= 14; ++q) ST(q, l1, j, k, v[q - 10]);
+    } else if (flag == 1) {  // no-slip, :108-124
+        const R v1 = LD(1, l, j, k), v2 = LD(2, l, j, k), v3 = LD(3, l, j, k), v4 = LD(4, l, j, k), v5 = LD(5, l, j, k);
+        ST(12, l1, j - 1, k, v1);
+        ST(13, l1, j, k - 1, v2);
+        ST(10, l1, j + 1, k, v3);
+        ST(11, l1, j, k + 1, v4);
+        ST(14, l1, j, k, v5);
+    } else {  // outflow, :127-169: equilibrium at rho=1 with the (un-normalised) momentum of x=l
+        R a[18];
+#pragma unroll
+        for (int q = 0; q < 18; ++q) a[q] = bc_load(L, g, q, l, j, k);
         const R xj = a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13];
         const R yj = a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17];
         const R zj = a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15];
@@ -74,13 +84,18 @@ __global__ void k_front_fix(Lat<S, R> L, Geo g, Range2 r) {
     int t, side;
     if (!r.get(t, side)) return;
     const int l1 = g.l + 1, m = g.m, n = g.n;
+    R lo[5], hi[5];
     if (side == 0 && t >= 1 && t <= m) {
-        for (int q = 10; q <= 14; ++q) ST(q, l1, t, 0, LD(q, l1, t, 1));
-        for (int q = 10; q <= 14; ++q) ST(q, l1, t, n + 1, LD(q, l1, t, n));
+#pragma unroll
+        for (int q = 10; q <= 14; ++q) { lo[q - 10] = LD(q, l1, t, 1); hi[q - 10] = LD(q, l1, t, n); }
+#pragma unroll
+        for (int q = 10; q <= 14; ++q) { ST(q, l1, t, 0, lo[q - 10]); ST(q, l1, t, n + 1, hi[q - 10]); }
     }
     if (side == 1 && t >= 1 && t <= n) {
-        for (int q = 10; q <= 14; ++q) ST(q, l1, 0, t, LD(q, l1, 1, t));
-        for (int q = 10; q <= 14; ++q) ST(q, l1, m + 1, t, LD(q, l1, m, t));
+#pragma unroll
+        for (int q = 10; q <= 14; ++q) { lo[q - 10] = LD(q, l1, 1, t); hi[q - 10] = LD(q, l1, m, t); }
+#pragma unroll
+        for (int q = 10; q <= 14; ++q) { ST(q, l1, 0, t, lo[q - 10]); ST(q, l1, m + 1, t, hi[q - 10]); }
     }
 }
 
@@ -91,14 +106,20 @@ __global__ void k_rear(Lat<S, R> L, Geo g, Range2 r, int flag, R u_inflow) {
     if (!r.get(j, k)) return;
     const int l = g.l, m1 = g.m + 1;
     if (flag == 0) {  // periodic, :210-238 (SERIAL corner line :223)
-        if (j == 0) { ST(1, 0, m1, k, LD(1, l, 1, k)); return; }
-        for (int q = 1; q <= 5; ++q) ST(q, 0, j, k, LD(q, l, j, k));
+        if (j == 0) { const R v = LD(1, l, 1, k); ST(1, 0, m1, k, v); return; }
+        R v[5];
+#pragma unroll
+        for (int q = 1; q <= 5; ++q) v[q - 1] = LD(q, l, j, k);
+#pragma unroll
+        for (int q = 1; q <= 5; ++q) ST(q, 0, j, k, v[q - 1]);
     } else if (flag == 1) {  // no-slip, :241-257
-        ST(3, 0, j - 1, k, LD(10, 1, j, k));
-        ST(4, 0, j, k - 1, LD(11, 1, j, k));
-        ST(1, 0, j + 1, k, LD(12, 1, j, k));
-        ST(2, 0, j, k + 1, LD(13, 1, j, k));
-        ST(5, 0, j, k, LD(14, 1, j, k));
+        const R v10 = LD(10, 1, j, k), v11 = LD(11, 1, j, k), v12 = LD(12, 1, j, k), v13 = LD(13, 1, j, k),
+                v14 = LD(14, 1, j, k);
+        ST(3, 0, j - 1, k, v10);
+        ST(4, 0, j, k - 1, v11);
+        ST(1, 0, j + 1, k, v12);
+        ST(2, 0, j, k + 1, v13);
+        ST(5, 0, j, k, v14);
     } else {  // inflow, uniform, :260-321
         const R xj = u_inflow, yj = R(0), zj = R(0);
         const R rf = R(3), qf = R(1.5), t3 = R(3), one = R(1);
@@ -124,23 +145,29 @@ __global__ void k_up(Lat<S, R> L, Geo g, Range2 r, int flag, R force) {
     if (!r.get(i, j)) return;
     const int n = g.n, n1 = g.n + 1;
     if (flag == 0) {  // periodic, :385-409
-        ST(2, i, j, n1, LD(2, i, j, 1));
-        ST(9, i, j, n1, LD(9, i, j, 1));
-        ST(11, i, j, n1, LD(11, i, j, 1));
-        ST(15, i, j, n1, LD(15, i, j, 1));
-        ST(16, i, j, n1, LD(16, i, j, 1));
+        const R v2 = LD(2, i, j, 1), v9 = LD(9, i, j, 1), v11 = LD(11, i, j, 1), v15 = LD(15, i, j, 1),
+                v16 = LD(16, i, j, 1);
+        ST(2, i, j, n1, v2);
+        ST(9, i, j, n1, v9);
+        ST(11, i, j, n1, v11);
+        ST(15, i, j, n1, v15);
+        ST(16, i, j, n1, v16);
     } else if (flag == 1 || flag == 2) {  // no-slip :412-428, lid :431-447
-        ST(15, i, j, n1, LD(6, i, j, n));
-        ST(2, i - 1, j, n1, flag == 2 ? LD(13, i, j, n) + force : LD(13, i, j, n));
-        ST(9, i, j - 1, n1, LD(18, i, j, n));
-        ST(11, i + 1, j, n1, flag == 2 ? LD(4, i, j, n) - force : LD(4, i, j, n));
-        ST(16, i, j + 1, n1, LD(7, i, j, n));
+        const R v6 = LD(6, i, j, n), v13 = LD(13, i, j, n), v18 = LD(18, i, j, n), v4 = LD(4, i, j, n),
+                v7 = LD(7, i, j, n);
+        ST(15, i, j, n1, v6);
+        ST(2, i - 1, j, n1, flag == 2 ? v13 + force : v13);
+        ST(9, i, j - 1, n1, v18);
+        ST(11, i + 1, j, n1, flag == 2 ? v4 - force : v4);
+        ST(16, i, j + 1, n1, v7);
     } else {  // free-slip over i = 0..l+1, j = 0..m+1, :450-468
-        ST(15, i, j, n1, LD(6, i, j, n));
-        ST(11, i, j, n1, LD(13, i, j, n));
-        ST(16, i, j, n1, LD(18, i, j, n));
-        ST(2, i, j, n1, LD(4, i, j, n));
-        ST(9, i, j, n1, LD(7, i, j, n));
+        const R v6 = LD(6, i, j, n), v13 = LD(13, i, j, n), v18 = LD(18, i, j, n), v4 = LD(4, i, j, n),
+                v7 = LD(7, i, j, n);
+        ST(15, i, j, n1, v6);
+        ST(11, i, j, n1, v13);
+        ST(16, i, j, n1, v18);
+        ST(2, i, j, n1, v4);
+        ST(9, i, j, n1, v7);
     }
 }
 
@@ -151,23 +178,29 @@ __global__ void k_down(Lat<S, R> L, Geo g, Range2 r, int flag) {
     if (!r.get(i, j)) return;
     const int n = g.n;
     if (flag == 0) {  // periodic, :472-496
-        ST(4, i, j, 0, LD(4, i, j, n));
-        ST(6, i, j, 0, LD(6, i, j, n));
-        ST(7, i, j, 0, LD(7, i, j, n));
-        ST(13, i, j, 0, LD(13, i, j, n));
-        ST(18, i, j, 0, LD(18, i, j, n));
+        const R v4 = LD(4, i, j, n), v6 = LD(6, i, j, n), v7 = LD(7, i, j, n), v13 = LD(13, i, j, n),
+                v18 = LD(18, i, j, n);
+        ST(4, i, j, 0, v4);
+        ST(6, i, j, 0, v6);
+        ST(7, i, j, 0, v7);
+        ST(13, i, j, 0, v13);
+        ST(18, i, j, 0, v18);
     } else if (flag == 1) {  // no-slip, :499-515
-        ST(6, i, j, 0, LD(15, i, j, 1));
-        ST(4, i - 1, j, 0, LD(11, i, j, 1));
-        ST(7, i, j - 1, 0, LD(16, i, j, 1));
-        ST(13, i + 1, j, 0, LD(2, i, j, 1));
-        ST(18, i, j + 1, 0, LD(9, i, j, 1));
+        const R v15 = LD(15, i, j, 1), v11 = LD(11, i, j, 1), v16 = LD(16, i, j, 1), v2 = LD(2, i, j, 1),
+                v9 = LD(9, i, j, 1);
+        ST(6, i, j, 0, v15);
+        ST(4, i - 1, j, 0, v11);
+        ST(7, i, j - 1, 0, v16);
+        ST(13, i + 1, j, 0, v2);
+        ST(18, i, j + 1, 0, v9);
     } else {  // free-slip, :518-530
-        ST(6, i, j, 0, LD(15, i, j, 1));
-        ST(13, i, j, 0, LD(11, i, j, 1));
-        ST(18, i, j, 0, LD(16, i, j, 1));
-        ST(4, i, j, 0, LD(2, i, j, 1));
-        ST(7, i, j, 0, LD(9, i, j, 1));
+        const R v15 = LD(15, i, j, 1), v11 = LD(11, i, j, 1), v16 = LD(16, i, j, 1), v2 = LD(2, i, j, 1),
+                v9 = LD(9, i, j, 1);
+        ST(6, i, j, 0, v15);
+        ST(13, i, j, 0, v11);
+        ST(18, i, j, 0, v16);
+        ST(4, i, j, 0, v2);
+        ST(7, i, j, 0, v9);
     }
 }
 
@@ -178,24 +211,30 @@ __global__ void k_left(Lat<S, R> L, Geo g, Range2 r, int flag) {
     if (!r.get(i, k)) return;
     const int l = g.l, m = g.m;
     if (flag == 0) {  // periodic, :535-560 (corner line :547)
-        if (i == 0) { ST(3, 0, 0, k, LD(3, l, m, k)); return; }
-        ST(3, i, 0, k, LD(3, i, m, k));
-        ST(7, i, 0, k, LD(7, i, m, k));
-        ST(8, i, 0, k, LD(8, i, m, k));
-        ST(9, i, 0, k, LD(9, i, m, k));
-        ST(12, i, 0, k, LD(12, i, m, k));
+        if (i == 0) { const R v = LD(3, l, m, k); ST(3, 0, 0, k, v); return; }
+        const R v3 = LD(3, i, m, k), v7 = LD(7, i, m, k), v8 = LD(8, i, m, k), v9 = LD(9, i, m, k),
+                v12 = LD(12, i, m, k);
+        ST(3, i, 0, k, v3);
+        ST(7, i, 0, k, v7);
+        ST(8, i, 0, k, v8);
+        ST(9, i, 0, k, v9);
+        ST(12, i, 0, k, v12);
     } else if (flag == 1) {  // no-slip, :563-579
-        ST(8, i, 0, k, LD(17, i, 1, k));
-        ST(12, i + 1, 0, k, LD(1, i, 1, k));
-        ST(3, i - 1, 0, k, LD(10, i, 1, k));
-        ST(7, i, 0, k - 1, LD(16, i, 1, k));
-        ST(9, i, 0, k + 1, LD(18, i, 1, k));
+        const R v17 = LD(17, i, 1, k), v1 = LD(1, i, 1, k), v10 = LD(10, i, 1, k), v16 = LD(16, i, 1, k),
+                v18 = LD(18, i, 1, k);
+        ST(8, i, 0, k, v17);
+        ST(12, i + 1, 0, k, v1);
+        ST(3, i - 1, 0, k, v10);
+        ST(7, i, 0, k - 1, v16);
+        ST(9, i, 0, k + 1, v18);
     } else {  // free-slip, :582-594
-        ST(8, i, 0, k, LD(17, i, 1, k));
-        ST(3, i, 0, k, LD(1, i, 1, k));
-        ST(12, i, 0, k, LD(10, i, 1, k));
-        ST(9, i, 0, k, LD(16, i, 1, k));
-        ST(7, i, 0, k, LD(18, i, 1, k));
+        const R v17 = LD(17, i, 1, k), v1 = LD(1, i, 1, k), v10 = LD(10, i, 1, k), v16 = LD(16, i, 1, k),
+                v18 = LD(18, i, 1, k);
+        ST(8, i, 0, k, v17);
+        ST(3, i, 0, k, v1);
+        ST(12, i, 0, k, v10);
+        ST(9, i, 0, k, v16);
+        ST(7, i, 0, k, v18);
     }
 }
 
@@ -206,24 +245,30 @@ __global__ void k_right(Lat<S, R> L, Geo g, Range2 r, int flag) {
     if (!r.get(i, k)) return;
     const int m = g.m, m1 = g.m + 1, l1 = g.l + 1;
     if (flag == 0) {  // periodic, :600-625 (corner line :612)
-        if (i == 0) { ST(10, l1, m1, k, LD(10, 1, 1, k)); return; }
-        ST(1, i, m1, k, LD(1, i, 1, k));
-        ST(10, i, m1, k, LD(10, i, 1, k));
-        ST(16, i, m1, k, LD(16, i, 1, k));
-        ST(17, i, m1, k, LD(17, i, 1, k));
-        ST(18, i, m1, k, LD(18, i, 1, k));
+        if (i == 0) { const R v = LD(10, 1, 1, k); ST(10, l1, m1, k, v); return; }
+        const R v1 = LD(1, i, 1, k), v10 = LD(10, i, 1, k), v16 = LD(16, i, 1, k), v17 = LD(17, i, 1, k),
+                v18 = LD(18, i, 1, k);
+        ST(1, i, m1, k, v1);
+        ST(10, i, m1, k, v10);
+        ST(16, i, m1, k, v16);
+        ST(17, i, m1, k, v17);
+        ST(18, i, m1, k, v18);
     } else if (flag == 1) {  // no-slip, :628-644
-        ST(10, i + 1, m1, k, LD(3, i, m, k));
-        ST(16, i, m1, k + 1, LD(7, i, m, k));
-        ST(17, i, m1, k, LD(8, i, m, k));
-        ST(18, i, m1, k - 1, LD(9, i, m, k));
-        ST(1, i - 1, m1, k, LD(12, i, m, k));
+        const R v3 = LD(3, i, m, k), v7 = LD(7, i, m, k), v8 = LD(8, i, m, k), v9 = LD(9, i, m, k),
+                v12 = LD(12, i, m, k);
+        ST(10, i + 1, m1, k, v3);
+        ST(16, i, m1, k + 1, v7);
+        ST(17, i, m1, k, v8);
+        ST(18, i, m1, k - 1, v9);
+        ST(1, i - 1, m1, k, v12);
     } else {  // free-slip, :647-659
-        ST(1, i, m1, k, LD(3, i, m, k));
-        ST(18, i, m1, k, LD(7, i, m, k));
-        ST(17, i, m1, k, LD(8, i, m, k));
-        ST(16, i, m1, k, LD(9, i, m, k));
-        ST(10, i, m1, k, LD(12, i, m, k));
+        const R v3 = LD(3, i, m, k), v7 = LD(7, i, m, k), v8 = LD(8, i, m, k), v9 = LD(9, i, m, k),
+                v12 = LD(12, i, m, k);
+        ST(1, i, m1, k, v3);
+        ST(18, i, m1, k, v7);
+        ST(17, i, m1, k, v8);
+        ST(16, i, m1, k, v9);
+        ST(10, i, m1, k, v12);
     }
 }
 
@@ -233,10 +278,14 @@ __global__ void k_edge_fix(Lat<S, R> L, Geo g, Range2 r, int fixes) {
     int i, dummy;
     if (!r.get(i, dummy)) return;
     const int m = g.m, m1 = g.m + 1, n = g.n, n1 = g.n + 1;
-    if (fixes & 1) ST(9, i, 0, n1, LD(18, i, 1, n));
-    if (fixes & 2) ST(16, i, m1, n1, LD(7, i, m, n));
-    if (fixes & 4) ST(18, i, m1, 0, LD(9, i, m, 1));
-    if (fixes & 8) ST(7, i, 0, 0, LD(16, i, 1, 1));
+    const R v1 = (fixes & 1) ? LD(18, i, 1, n) : R(0);
+    const R v2 = (fixes & 2) ? LD(7, i, m, n) : R(0);
+    const R v3 = (fixes & 4) ? LD(9, i, m, 1) : R(0);
+    const R v4 = (fixes & 8) ? LD(16, i, 1, 1) : R(0);
+    if (fixes & 1) ST(9, i, 0, n1, v1);
+    if (fixes & 2) ST(16, i, m1, n1, v2);
+    if (fixes & 4) ST(18, i, m1, 0, v3);
+    if (fixes & 8) ST(7, i, 0, 0, v4);
 }
 
 #undef LD
@@ -244,7 +293,8 @@ __global__ void k_edge_fix(Lat<S, R> L, Geo g, Range2 r, int fixes) {
 
 // ---- block reduction into deterministic per-block partials ----------------------------
 template <int W>
-__device__ void block_reduce_store(double (&v)[W], const Reduce& red, double* out) {
+__device__ void block_reduce_store(double (&v)[W], const Reduce& red, double* out, double* series = nullptr,
+                                   int64_t cap = 0, int64_t* d_itime = nullptr, int advance = 0) {
     __shared__ double sh[32][W];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -269,10 +319,16 @@ __device__ void block_reduce_store(double (&v)[W], const Reduce& red, double* ou
     if (!last) return;
     __threadfence();
     if (threadIdx.x == 0) {
+        double* dst = out;
+        if (series) {
+            const int64_t t = *(volatile int64_t*)d_itime;
+            dst = series + W * (t % cap);
+            if (advance) *d_itime = t + 1;
+        }
         for (int c = 0; c < W; ++c) {
             double s = 0.0;
             for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)red.partials)[(int64_t)b * W + c];
-            out[c] = s;
+            dst[c] = s;
         }
         *red.counter = 0u;
     }
@@ -287,11 +343,13 @@ __device__ void block_reduce_store(double (&v)[W], const Reduce& red, double* ou
 // is only ever pulled into solid voxels.  The same reads give the force: the
 // population a_opp(q)(y) leaving fluid node y = x + c_q towards x transfers
 // 2 c_opp(q) a_opp(q)(y) = -2 c_q a_opp(q)(y); across a periodic axis y is the
-// wrapped node and its interior value is used.
+// wrapped node and its interior value is used.  The force of the state read
+// goes to series[itime % cap], itime read from device memory; with `advance`
+// the last block then increments the device step counter.
 template <typename S, typename R>
 __global__ void k_bounce_drag(Lat<S, R> L, Geo g, Mask mk, int per_x, int per_y, int per_z,
                               const int32_t* list, int64_t nlist, int do_bounce, Reduce red,
-                              double* force_out) {
+                              double* series, int64_t cap, int64_t* d_itime, int advance) {
     double f[3] = {0.0, 0.0, 0.0};
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nlist;
          t += (int64_t)gridDim.x * blockDim.x) {
@@ -299,21 +357,30 @@ __global__ void k_bounce_drag(Lat<S, R> L, Geo g, Mask mk, int per_x, int per_y,
         const int i = (int)(lin % g.l) + 1;
         const int j = (int)((lin / g.l) % g.m) + 1;
         const int k = (int)(lin / g.lm) + 1;
+        S raw[18];
+        R val[18];
+        bool wr[18];
 #pragma unroll
         for (int q = 0; q < 18; ++q) {
             const int qo = opp_of(q);
             const int ni = i + cx_of(q), nj = j + cy_of(q), nk = k + cz_of(q);
+            wr[q] = false;
+            val[q] = R(0);
+            raw[q] = S();
             if (g.interior(ni, nj, nk)) {
                 if (mk.solid(g, ni, nj, nk)) continue;
-                const S raw = L.pop[qo][g.lin(ni, nj, nk)];
-                const double v = (double)Store<S, R>::load(raw, qo, L.inv_scale);
+                raw[q] = L.pop[qo][g.lin(ni, nj, nk)];
+                val[q] = Store<S, R>::load(raw[q], qo, L.inv_scale);
+                wr[q] = true;
+                const double v = (double)val[q];
                 f[0] -= 2.0 * cx_of(q) * v;
                 f[1] -= 2.0 * cy_of(q) * v;
                 f[2] -= 2.0 * cz_of(q) * v;
-                if (do_bounce) L.pop[q][lin] = raw;
             } else {
                 const R v = L.ghost[(int64_t)qo * g.G + g.gidx(ni, nj, nk)];
-                if (do_bounce) L.pop[q][lin] = Store<S, R>::store(v, q, L.scale);
+                raw[q] = Store<S, R>::store(v, q, L.scale);
+                val[q] = Store<S, R>::load(raw[q], q, L.inv_scale);
+                wr[q] = true;
                 int wi = ni, wj = nj, wk = nk;
                 if (per_x) wi = wi < 1 ? wi + g.l : (wi > g.l ? wi - g.l : wi);
                 if (per_y) wj = wj < 1 ? wj + g.m : (wj > g.m ? wj - g.m : wj);
@@ -326,8 +393,21 @@ __global__ void k_bounce_drag(Lat<S, R> L, Geo g, Mask mk, int per_x, int per_y,
                 }
             }
         }
+        if (do_bounce) {
+#pragma unroll
+            for (int q = 0; q < 18; ++q)
+                if (wr[q]) L.pop[q][lin] = raw[q];
+            if (i == 1 || i == g.l) {
+#pragma unroll
+                for (int q = 0; q < 18; ++q) {
+                    if (!wr[q]) continue;
+                    if (i == 1) L.xface[xface_idx(g, 0, q, j, k)] = val[q];
+                    if (i == g.l) L.xface[xface_idx(g, 1, q, j, k)] = val[q];
+                }
+            }
+        }
     }
-    block_reduce_store<3>(f, red, force_out);
+    block_reduce_store<3>(f, red, nullptr, series, cap, d_itime, advance);
 }
 
 // ---- FP64 monitor, CODE/SRC/diagno.F90:67-120 -------------------------------------------
@@ -392,6 +472,19 @@ __global__ void k_gather(Lat<S, R> L, Geo g, int q, T* dst, int64_t total) {
     for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (int64_t)gridDim.x * blockDim.x)
         dst[idx] = (T)lat_load(L, g, q, (int)(idx % L2), (int)((idx / L2) % M2), (int)(idx / (L2 * M2)));
+}
+
+// x-face copy of the current lattice (after an upload): one thread per (j,k).
+template <typename S, typename R>
+__global__ void k_fill_xface(Lat<S, R> L, Geo g) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)g.m * g.n) return;
+    const int j = (int)(t % g.m) + 1, k = (int)(t / g.m) + 1;
+#pragma unroll
+    for (int q = 0; q < 18; ++q) {
+        L.xface[xface_idx(g, 0, q, j, k)] = lat_load(L, g, q, 1, j, k);
+        L.xface[xface_idx(g, 1, q, j, k)] = lat_load(L, g, q, g.l, j, k);
+    }
 }
 
 unsigned grid_for(int64_t work, int tpb, unsigned cap = 148u * 16u) {
@@ -460,12 +553,18 @@ int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& 
 template <typename S, typename R>
 void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const Mask& mk, const int bc[6],
                         const int32_t* list, int64_t nlist, bool do_bounce, const Reduce& red,
-                        double* force_out, cudaStream_t st) {
+                        double* series, int64_t cap, int64_t* d_itime, bool advance, cudaStream_t st) {
     const int per_x = (bc[0] == 0 && bc[1] == 0), per_y = (bc[2] == 0 && bc[3] == 0);
     const int per_z = (bc[4] == 0 && bc[5] == 0);
     const unsigned blocks = grid_for(nlist, kTpb, (unsigned)red.max_blocks);
-    k_bounce_drag<S, R><<<blocks, kTpb, 0, st>>>(L, g, mk, per_x, per_y, per_z, list, nlist,
-                                                 do_bounce ? 1 : 0, red, force_out);
+    k_bounce_drag<S, R><<<blocks, kTpb, 0, st>>>(L, g, mk, per_x, per_y, per_z, list, nlist, do_bounce ? 1 : 0,
+                                                 red, series, cap, d_itime, advance ? 1 : 0);
+}
+
+template <typename S, typename R>
+void launch_fill_xface(const Lat<S, R>& L, const Geo& g, cudaStream_t st) {
+    const int64_t work = (int64_t)g.m * g.n;
+    k_fill_xface<S, R><<<(unsigned)((work + kTpb - 1) / kTpb), kTpb, 0, st>>>(L, g);
 }
 
 template <typename S, typename R>
@@ -497,7 +596,8 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
     template int launch_bc<S, R>(const Lat<S, R>&, const Geo&, const int*, const Phys<R>&, cudaStream_t); \
     template void launch_bounce_drag<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const int*,      \
                                            const int32_t*, int64_t, bool, const Reduce&, double*,      \
-                                           cudaStream_t);                                              \
+                                           int64_t, int64_t*, bool, cudaStream_t);                     \
+    template void launch_fill_xface<S, R>(const Lat<S, R>&, const Geo&, cudaStream_t);                 \
     template void launch_monitor<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const Reduce&,       \
                                        double*, cudaStream_t);                                         \
     template void launch_probes<S, R>(const Lat<S, R>&, const Geo&, int, const int32_t*, double*,      \

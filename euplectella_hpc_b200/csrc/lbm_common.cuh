@@ -138,11 +138,18 @@ struct Geo {
     }
 };
 
-// Pointers of one lattice (19 population arrays) plus the halo shell.
+// Pointers of one lattice (19 population arrays) plus the halo shell and the
+// x-face copy.  The x-face copy holds, for the interior columns x = 1 (side 0)
+// and x = l (side 1), the 18 moving populations exactly as a load from the
+// lattice returns them, laid out xface[(side*18 + q)*m*n + (j-1) + (k-1)*m].
+// The stream-collide kernel writes it for the state it produces and the
+// bounce-back kernel keeps it in step, so that halo kernels read these
+// columns coalesced in j instead of with a stride of l elements.
 template <typename S, typename R>
 struct Lat {
     S* pop[Q];
     R* ghost;       // ghost[q*G + gidx]
+    R* xface;       // [2][18][m*n]
     R scale, inv_scale;
 };
 
@@ -150,6 +157,24 @@ template <typename S, typename R>
 __device__ __forceinline__ R lat_load(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k) {
     if (g.interior(i, j, k)) return Store<S, R>::load(L.pop[q][g.lin(i, j, k)], q, L.inv_scale);
     return L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)];
+}
+
+__host__ __device__ __forceinline__ int64_t xface_idx(const Geo& g, int side, int q, int j, int k) {
+    return (int64_t)(side * 18 + q) * ((int64_t)g.m * g.n) + (j - 1) + (int64_t)(k - 1) * g.m;
+}
+
+// Load used by the halo kernels: x-face columns from the x-face copy.
+template <typename S, typename R>
+__device__ __forceinline__ R bc_load(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k) {
+    if (q < 18 && (i == 1 || i == g.l) && j >= 1 && j <= g.m && k >= 1 && k <= g.n)
+        return L.xface[xface_idx(g, i == 1 ? 0 : 1, q, j, k)];
+    return lat_load(L, g, q, i, j, k);
+}
+
+// Value a later lattice load returns for an arithmetic value v of population q.
+template <typename S, typename R>
+__device__ __forceinline__ R stored_value(R v, int q, R scale, R inv_scale) {
+    return Store<S, R>::load(Store<S, R>::store(v, q, scale), q, inv_scale);
 }
 template <typename S, typename R>
 __device__ __forceinline__ void ghost_store(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k, R v) {

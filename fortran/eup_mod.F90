@@ -1,0 +1,103 @@
+! =====================================================================
+!     eup_mod -- iso_c_binding interface to the B200 D3Q19 BGK step
+!
+!     Declares the C ABI of include/eup.h for the Fortran driver of
+!     Euplectella_HPC (CODE/SRC/bgk3d.F90).  With this module the driver
+!     keeps its namelist, its arrays a01..a19(0:l+1,0:m+1,0:n+1) and all of
+!     its output routines; only the calls of the time loop change (see
+!     INTEGRATION.md for the patch of bgk3d.F90, initialize.F90 and
+!     diagnostic.F90).  Same pattern as the reference's own C interop in
+!     CODE/SRC/get_mem_mod.F90:1-10.
+! =====================================================================
+      module eup_mod
+      use iso_c_binding
+      implicit none
+
+      integer(c_int), parameter :: EUP_OK = 0
+      integer(c_int), parameter :: EUP_FP32 = 0, EUP_FP64 = 1
+      integer(c_int), parameter :: EUP_FP16_DEV = 2, EUP_BF16_DEV = 3
+
+      type, bind(c) :: eup_config
+         integer(c_int32_t) :: lx, ly, lz
+         integer(c_int32_t) :: bc(6)        ! front, rear, right, left, up, down
+         real(c_double)     :: svisc, u0, u_inflow, u00
+         integer(c_int32_t) :: precision, device
+         real(c_double)     :: dev_scale
+         real(c_double)     :: cd_rho0, cd_uref, cd_length, cd_span
+         integer(c_int64_t) :: series_capacity
+      end type eup_config
+
+      interface
+         integer(c_int) function eup_create(cfg, h) bind(c, name="eup_create")
+            import :: c_int, c_ptr, eup_config
+            type(eup_config), intent(in) :: cfg
+            type(c_ptr), intent(out)     :: h
+         end function
+
+         integer(c_int) function eup_destroy(h) bind(c, name="eup_destroy")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+         end function
+
+         integer(c_int) function eup_set_obstacles(h, obs) bind(c, name="eup_set_obstacles")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            type(c_ptr), value :: obs             ! c_loc(obs(1,1,1))
+         end function
+
+         integer(c_int) function eup_upload(h, pops, elem_bytes, itime) bind(c, name="eup_upload")
+            import :: c_int, c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value          :: h
+            type(c_ptr), intent(in)     :: pops(19)    ! c_loc(a01(0,0,0)) ... c_loc(a19(0,0,0))
+            integer(c_int32_t), value   :: elem_bytes  ! 4 (sp) or 8 (-DDOUBLE_P)
+            integer(c_int64_t), value   :: itime
+         end function
+
+         integer(c_int) function eup_download(h, pops, elem_bytes) bind(c, name="eup_download")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value          :: h
+            type(c_ptr), intent(in)     :: pops(19)
+            integer(c_int32_t), value   :: elem_bytes
+         end function
+
+         integer(c_int) function eup_step(h, nsteps) bind(c, name="eup_step")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: nsteps
+         end function
+
+         integer(c_int) function eup_get_forces(h, fxyz) bind(c, name="eup_get_forces")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value    :: h
+            real(c_double)        :: fxyz(3)
+         end function
+
+         integer(c_int) function eup_get_cd_series(h, first, cnt, cd) bind(c, name="eup_get_cd_series")
+            import :: c_int, c_ptr, c_int64_t, c_int32_t, c_double
+            type(c_ptr), value        :: h
+            integer(c_int64_t), value :: first
+            integer(c_int32_t), value :: cnt
+            real(c_double)            :: cd(*)
+         end function
+
+         integer(c_int) function eup_get_monitor(h, sums) bind(c, name="eup_get_monitor")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double)     :: sums(5)
+         end function
+
+         type(c_ptr) function eup_last_error(h) bind(c, name="eup_last_error")
+            import :: c_ptr
+            type(c_ptr), value :: h
+         end function
+
+         integer(c_int) function eup_read_obs_file(path, l, m, n, obs, nobs) bind(c, name="eup_read_obs_file")
+            import :: c_int, c_char, c_int32_t, c_ptr, c_int64_t
+            character(kind=c_char), intent(in) :: path(*)
+            integer(c_int32_t), value :: l, m, n
+            type(c_ptr), value        :: obs
+            integer(c_int64_t)        :: nobs
+         end function
+      end interface
+
+      end module eup_mod

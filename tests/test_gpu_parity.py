@@ -44,6 +44,10 @@ CASES = [
     ("obstacle_on_faces", (24, 12, 10), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _wall_touch),
     ("noslip_y_periodic_z_inflow", (20, 10, 9), (5, 4, 1, 1, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
     ("freeslip_z_periodic_y", (20, 10, 9), (5, 4, 0, 0, 3, 3), 0.01, 0.0, 0.05, 0.0, _cyl),
+    # l a multiple of 128: the vectorised stream-collide kernel (16-byte rows) runs
+    ("vec_cylinder", (128, 24, 10), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
+    ("vec_freeslip_all", (128, 18, 14), (5, 4, 3, 3, 3, 3), 0.0024, 0.0, 0.05, 0.0, _block),
+    ("vec_periodic_x_body_force", (128, 12, 10), (0, 0, 3, 3, 1, 1), 0.05, 0.05, 0.0, 0.0, _wall_touch),
 ]
 
 
@@ -195,3 +199,39 @@ def test_deviation_storage_against_fp64(eup, require_gpu, prec):
     tol_l2, tol_cd = (1e-3, 5e-3) if prec == "fp16" else (2e-2, 5e-2)
     assert rel_l2 < tol_l2, rel_l2
     assert cd_err < tol_cd, cd_err
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16", "bf16"])
+def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
+    """Vectorised vs one-node-per-thread stream-collide, CUDA graphs vs plain
+    launches: all four paths give the same bits in every storage format."""
+    l, m, n = 256, 20, 12
+    code = {"fp32": eup.FP32, "fp64": eup.FP64, "fp16": eup.FP16_DEV, "bf16": eup.BF16_DEV}[prec]
+    dt = np.float64 if prec == "fp64" else np.float32
+    obs = _cyl(l, m, n)
+    a = eup.init_equilibrium(l, m, n, 0.05, 1e-3, 77, dt)
+    cfg = eup.Config(l, m, n, bc=(5, 4, 3, 3, 0, 0), svisc=0.01, u_inflow=0.05, precision=code)
+    res = []
+    for var in ("0", "1", "2", "3"):
+        monkeypatch.setenv("EUP_STEP_VARIANT", var)
+        with eup.Solver(cfg) as s:
+            s.set_obstacles(obs)
+            s.upload(a)
+            s.step(7)
+            s.step(5)
+            res.append((s.download(dt), s.force_series(0, 13)))
+    for got, f in res[1:]:
+        assert np.array_equal(got, res[0][0])
+        assert np.array_equal(f, res[0][1])
+
+
+def test_launch_count(eup, require_gpu):
+    l, m, n = 128, 12, 10
+    obs = _block(l, m, n)
+    with eup.Solver(eup.Config(l, m, n, bc=(5, 4, 3, 3, 3, 3), svisc=0.01, u_inflow=0.05)) as s:
+        s.set_obstacles(obs)
+        s.upload(eup.init_equilibrium(l, m, n, 0.05, 0, 1))
+        s.step(4)
+        # per step: bounce-back/drag, front, front border fix, rear, up, down, left, right,
+        # free-slip edge fixes, stream-collide = 10; plus one drag of the final state
+        assert s.launches == 4 * 10 + 1
