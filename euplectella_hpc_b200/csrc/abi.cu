@@ -29,6 +29,7 @@ struct eup_handle {
     uint32_t* bits = nullptr;
     int wpr = 0;
     int32_t* blist = nullptr;
+    uint64_t* blinks = nullptr;   // neighbour classification of each boundary-solid voxel
     int64_t nblist = 0;
     double* partials = nullptr;
     unsigned int* counter = nullptr;
@@ -40,7 +41,7 @@ struct eup_handle {
     int64_t itime = 0, series_first = 0;
     bool has_state = false;
     double scale = 1.0;
-    int variant = 0;  // EUP_STEP_VARIANT: bit 0 scalar stream-collide, bit 1 no CUDA graphs
+    int variant = 0;  // EUP_STEP_VARIANT: bit 0/2 16/8-byte vector stream-collide, bit 1 no CUDA graphs
     int64_t launches = 0;  // kernels launched by eup_step / eup_step_profiled
     int launches_per_step = 0;
     std::string err;
@@ -108,7 +109,7 @@ Reduce make_reduce(const eup_handle* h) { return Reduce{h->partials, h->counter,
 template <typename S, typename R>
 void enqueue_drag_only(eup_handle* h) {
     const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
-    launch_bounce_drag<S, R>(make_lat<S, R>(h, h->cur), h->g, make_mask(h), bc, h->blist, h->nblist, false,
+    launch_bounce_drag<S, R>(make_lat<S, R>(h, h->cur), h->g, bc, h->blist, h->blinks, h->nblist, false,
                              make_reduce(h), h->series, h->cap, h->d_itime, false, h->stream);
 }
 
@@ -131,7 +132,7 @@ int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
     int n = 0;
     if (pe) pe->mark(4 * s + 0, h->stream);
     // boundaries: bounce-back then halo planes (CODE/SRC/boundaries.F90:36-49,235-248)
-    launch_bounce_drag<S, R>(src, h->g, make_mask(h), bc, h->blist, h->nblist, true, make_reduce(h), h->series,
+    launch_bounce_drag<S, R>(src, h->g, bc, h->blist, h->blinks, h->nblist, true, make_reduce(h), h->series,
                              h->cap, h->d_itime, true, h->stream);
     n += 1;
     if (pe) pe->mark(4 * s + 1, h->stream);
@@ -365,8 +366,8 @@ int eup_destroy(eup_handle* h) {
     cudaSetDevice(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
-    void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->partials, h->counter, h->series,
-                    h->dscratch, h->staging, h->xface, h->d_itime};
+    void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->blinks, h->partials, h->counter,
+                    h->series, h->dscratch, h->staging, h->xface, h->d_itime};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -392,6 +393,7 @@ int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
     drop_graphs(h);  // the captured steps hold the old mask and list pointers
     if (h->bits) { cudaFree(h->bits); h->bits = nullptr; }
     if (h->blist) { cudaFree(h->blist); h->blist = nullptr; }
+    if (h->blinks) { cudaFree(h->blinks); h->blinks = nullptr; }
     h->nblist = 0;
     h->wpr = (g.l + 31) / 32;
     if (nsolid > 0) {
@@ -410,6 +412,9 @@ int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
         cudaFree(d_obs);
         if (e != cudaSuccess) return cuda_fail(h, e, "compact boundary solid list");
         h->nblist = cnt;
+        CK(h, cudaMalloc(&h->blinks, sizeof(uint64_t) * (size_t)(cnt > 0 ? cnt : 1)));
+        const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
+        launch_bsolid_links(g, make_mask(h), bc, h->blist, cnt, h->blinks, h->stream);
     }
     if (h->has_state) DISPATCH(h, enqueue_drag_only, h);
     CK(h, cudaGetLastError());

@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+#include <vector>
+
 #include "lbm_common.cuh"
 
 namespace eup {
@@ -33,6 +36,66 @@ struct Reduce {
 constexpr int kReduceMaxBlocks = 4096;
 constexpr int kReduceWidth = 8;
 
+// ---- block reduction into deterministic per-block partials ----------------------------
+template <int W>
+__device__ __forceinline__ void block_reduce_store(double (&v)[W], const Reduce& red, double* out, double* series = nullptr,
+                                   int64_t cap = 0, int64_t* d_itime = nullptr, int advance = 0,
+                                   int slot_offset = 0) {
+    __shared__ double sh[32][W];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+    if (lane == 0)
+        for (int c = 0; c < W; ++c) sh[warp][c] = v[c];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int c = 0; c < W; ++c) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += sh[w][c];
+            red.partials[(int64_t)blockIdx.x * W + c] = s;
+        }
+        __threadfence();
+        const unsigned done = atomicAdd(red.counter, 1u);
+        last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the last block adds the partials: thread t takes blocks t, t+blockDim, ...
+    // (independent loads, fixed assignment), then the same fixed tree as above
+    double s[W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) s[c] = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < W; ++c) s[c] += __ldcg(red.partials + (int64_t)b * W + c);
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+        for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_down_sync(0xffffffffu, s[c], o);
+    __syncthreads();
+    if (lane == 0)
+        for (int c = 0; c < W; ++c) sh[warp][c] = s[c];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double* dst = out;
+        if (series) {
+            const int64_t t = *(volatile int64_t*)d_itime;
+            dst = series + W * ((t + slot_offset) % cap);
+            if (advance) *d_itime = t + 1;
+        }
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int c = 0; c < W; ++c) {
+            double tot = 0.0;
+            for (int w = 0; w < nw; ++w) tot += sh[w][c];
+            dst[c] = tot;
+        }
+        *red.counter = 0u;
+    }
+}
+
 // Halo-plane operations of CODE/SRC/bcond.bc.F90, launched in the reference's order;
 // returns the number of kernels launched.
 template <typename S, typename R>
@@ -41,10 +104,11 @@ int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& 
 // Bounce-back on solid voxels touching fluid/halo (CODE/SRC/bcond.obs.F90) and the
 // FP64 momentum-exchange force of the state it reads, written to
 // series[3*(*d_itime % cap)]; with `advance` the device step counter is incremented.
+// links[t] classifies the 18 neighbours of list[t] (see launch_bsolid_links).
 template <typename S, typename R>
-void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const Mask& mk, const int bc[6],
-                        const int32_t* list, int64_t nlist, bool do_bounce, const Reduce& red,
-                        double* series, int64_t cap, int64_t* d_itime, bool advance, cudaStream_t st);
+void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const int bc[6], const int32_t* list,
+                        const uint64_t* links, int64_t nlist, bool do_bounce, const Reduce& red, double* series,
+                        int64_t cap, int64_t* d_itime, bool advance, cudaStream_t st);
 
 // x-face copy of the current lattice (needed once after an upload).
 template <typename S, typename R>
@@ -75,7 +139,49 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
 void launch_build_mask(const int32_t* obs, const Geo& g, uint32_t* bits, int wpr, cudaStream_t st);
 void launch_flag_boundary_solid(const Geo& g, const Mask& mk, uint8_t* flags, cudaStream_t st);
 void launch_links(const Geo& g, const Mask& mk, uint32_t* links, cudaStream_t st);
+// Neighbour classification of each boundary-solid voxel: bit q (0..17) neighbour
+// x + c_q is interior fluid, bit 18+q it is a halo node, bit 36+q that halo node
+// wraps across a periodic axis onto interior fluid.
+void launch_bsolid_links(const Geo& g, const Mask& mk, const int bc[6], const int32_t* list, int64_t n,
+                         uint64_t* links, cudaStream_t st);
 // Ordered compaction of flagged linear indices; returns the count (synchronous).
 int64_t compact_flags(const uint8_t* flags, int64_t n, int32_t* out, cudaStream_t st, cudaError_t* err);
+
+// ---- partial bounce-back and its adjoint (k_adjoint.cu) -------------------------
+// Where the adjoint of each halo value goes, derived on the host by running the
+// reference's halo blocks on symbols.  copy_*: halo slots holding a copy of an
+// interior population, grouped by source key q*N + lin (CSR: copy_start).
+// out_*: halo slots holding an outflow equilibrium, grouped by the x = l node
+// (j-1) + (k-1)*m they are computed from, with the population produced.
+struct HaloAdjointTables {
+    std::vector<int64_t> copy_key;
+    std::vector<int32_t> copy_start;
+    std::vector<int64_t> copy_slot;
+    std::vector<int32_t> out_jk;
+    std::vector<int32_t> out_start;
+    std::vector<int64_t> out_slot;
+    std::vector<int8_t> out_q;
+};
+struct HaloAdjointDevice {
+    const int64_t* copy_key = nullptr;
+    const int32_t* copy_start = nullptr;
+    const int64_t* copy_slot = nullptr;
+    int64_t ncopy = 0;
+    const int32_t* out_jk = nullptr;
+    const int32_t* out_start = nullptr;
+    const int64_t* out_slot = nullptr;
+    const int8_t* out_q = nullptr;
+    int64_t nout = 0;
+};
+// Returns EUP_OK or EUP_ERR_UNSUPPORTED (err says why).
+int build_halo_adjoint_tables(const Geo& g, const int bc[6], HaloAdjointTables* out, std::string* err);
+
+template <typename R>
+void launch_pbb_step(const Lat<R, R>& src, const Lat<R, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
+                     const Reduce& red, double* series, int64_t cap, int64_t* d_itime, cudaStream_t st);
+template <typename R>
+void launch_pbb_adjoint(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
+                        const Lat<R, R>& lam_out, R* gmu, double* grad, R gamma, const HaloAdjointDevice& t,
+                        cudaStream_t st);
 
 }  // namespace eup

@@ -291,49 +291,6 @@ __global__ void k_edge_fix(Lat<S, R> L, Geo g, Range2 r, int fixes) {
 #undef LD
 #undef ST
 
-// ---- block reduction into deterministic per-block partials ----------------------------
-template <int W>
-__device__ void block_reduce_store(double (&v)[W], const Reduce& red, double* out, double* series = nullptr,
-                                   int64_t cap = 0, int64_t* d_itime = nullptr, int advance = 0) {
-    __shared__ double sh[32][W];
-    __shared__ bool last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int c = 0; c < W; ++c)
-        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
-    if (lane == 0)
-        for (int c = 0; c < W; ++c) sh[warp][c] = v[c];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-        for (int c = 0; c < W; ++c) {
-            double s = 0.0;
-            for (int w = 0; w < nw; ++w) s += sh[w][c];
-            red.partials[(int64_t)blockIdx.x * W + c] = s;
-        }
-        __threadfence();
-        const unsigned done = atomicAdd(red.counter, 1u);
-        last = (done == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    if (threadIdx.x == 0) {
-        double* dst = out;
-        if (series) {
-            const int64_t t = *(volatile int64_t*)d_itime;
-            dst = series + W * (t % cap);
-            if (advance) *d_itime = t + 1;
-        }
-        for (int c = 0; c < W; ++c) {
-            double s = 0.0;
-            for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)red.partials)[(int64_t)b * W + c];
-            dst[c] = s;
-        }
-        *red.counter = 0u;
-    }
-}
-
 // ---- bounce-back + momentum exchange ---------------------------------------------------
 //
 // For each solid voxel x touching fluid or halo and each moving q, the
@@ -347,60 +304,68 @@ __device__ void block_reduce_store(double (&v)[W], const Reduce& red, double* ou
 // goes to series[itime % cap], itime read from device memory; with `advance`
 // the last block then increments the device step counter.
 template <typename S, typename R>
-__global__ void k_bounce_drag(Lat<S, R> L, Geo g, Mask mk, int per_x, int per_y, int per_z,
-                              const int32_t* list, int64_t nlist, int do_bounce, Reduce red,
-                              double* series, int64_t cap, int64_t* d_itime, int advance) {
+__global__ void k_bounce_drag(Lat<S, R> L, Geo g, int per_x, int per_y, int per_z, const int32_t* list,
+                              const uint64_t* links, int64_t nlist, int do_bounce, Reduce red, double* series,
+                              int64_t cap, int64_t* d_itime, int advance) {
     double f[3] = {0.0, 0.0, 0.0};
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nlist;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t lin = list[t];
-        const int i = (int)(lin % g.l) + 1;
-        const int j = (int)((lin / g.l) % g.m) + 1;
-        const int k = (int)(lin / g.lm) + 1;
+        const int32_t lin = list[t];
+        const uint64_t w = links[t];
+        const uint32_t fl = (uint32_t)(w & 0x3FFFFu);          // neighbour x + c_q is interior fluid
+        const uint32_t gh = (uint32_t)((w >> 18) & 0x3FFFFu);  // neighbour is a halo node
+        const uint32_t wf = (uint32_t)((w >> 36) & 0x3FFFFu);  // halo neighbour wraps onto interior fluid
+        const int i = lin % g.l + 1;
+        const int jk = lin / g.l;
+        const int j = jk % g.m + 1, k = jk / g.m + 1;
         S raw[18];
         R val[18];
-        bool wr[18];
+        // all loads first: interior fluid neighbours from the lattice, halo ones from the shell
 #pragma unroll
         for (int q = 0; q < 18; ++q) {
             const int qo = opp_of(q);
-            const int ni = i + cx_of(q), nj = j + cy_of(q), nk = k + cz_of(q);
-            wr[q] = false;
-            val[q] = R(0);
             raw[q] = S();
-            if (g.interior(ni, nj, nk)) {
-                if (mk.solid(g, ni, nj, nk)) continue;
-                raw[q] = L.pop[qo][g.lin(ni, nj, nk)];
-                val[q] = Store<S, R>::load(raw[q], qo, L.inv_scale);
-                wr[q] = true;
+            if ((fl >> q) & 1u) {
+                raw[q] = L.pop[qo][(int64_t)lin + cx_of(q) + (int64_t)cy_of(q) * g.l + (int64_t)cz_of(q) * g.lm];
+            } else if ((gh >> q) & 1u) {
+                const R v = L.ghost[(int64_t)qo * g.G + g.gidx(i + cx_of(q), j + cy_of(q), k + cz_of(q))];
+                raw[q] = Store<S, R>::store(v, q, L.scale);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 18; ++q) {
+            val[q] = ((fl >> q) & 1u) ? Store<S, R>::load(raw[q], opp_of(q), L.inv_scale)
+                                      : Store<S, R>::load(raw[q], q, L.inv_scale);
+            if ((fl >> q) & 1u) {
                 const double v = (double)val[q];
                 f[0] -= 2.0 * cx_of(q) * v;
                 f[1] -= 2.0 * cy_of(q) * v;
                 f[2] -= 2.0 * cz_of(q) * v;
-            } else {
-                const R v = L.ghost[(int64_t)qo * g.G + g.gidx(ni, nj, nk)];
-                raw[q] = Store<S, R>::store(v, q, L.scale);
-                val[q] = Store<S, R>::load(raw[q], q, L.inv_scale);
-                wr[q] = true;
-                int wi = ni, wj = nj, wk = nk;
+            }
+        }
+        if (wf) {  // links across a periodic axis: force from the wrapped fluid node
+#pragma unroll
+            for (int q = 0; q < 18; ++q) {
+                if (!((wf >> q) & 1u)) continue;
+                int wi = i + cx_of(q), wj = j + cy_of(q), wk = k + cz_of(q);
                 if (per_x) wi = wi < 1 ? wi + g.l : (wi > g.l ? wi - g.l : wi);
                 if (per_y) wj = wj < 1 ? wj + g.m : (wj > g.m ? wj - g.m : wj);
                 if (per_z) wk = wk < 1 ? wk + g.n : (wk > g.n ? wk - g.n : wk);
-                if (g.interior(wi, wj, wk) && !mk.solid(g, wi, wj, wk)) {
-                    const double w = (double)lat_load(L, g, qo, wi, wj, wk);
-                    f[0] -= 2.0 * cx_of(q) * w;
-                    f[1] -= 2.0 * cy_of(q) * w;
-                    f[2] -= 2.0 * cz_of(q) * w;
-                }
+                const double v = (double)lat_load(L, g, opp_of(q), wi, wj, wk);
+                f[0] -= 2.0 * cx_of(q) * v;
+                f[1] -= 2.0 * cy_of(q) * v;
+                f[2] -= 2.0 * cz_of(q) * v;
             }
         }
         if (do_bounce) {
+            const uint32_t wr = fl | gh;
 #pragma unroll
             for (int q = 0; q < 18; ++q)
-                if (wr[q]) L.pop[q][lin] = raw[q];
+                if ((wr >> q) & 1u) L.pop[q][lin] = raw[q];
             if (i == 1 || i == g.l) {
 #pragma unroll
                 for (int q = 0; q < 18; ++q) {
-                    if (!wr[q]) continue;
+                    if (!((wr >> q) & 1u)) continue;
                     if (i == 1) L.xface[xface_idx(g, 0, q, j, k)] = val[q];
                     if (i == g.l) L.xface[xface_idx(g, 1, q, j, k)] = val[q];
                 }
@@ -551,13 +516,13 @@ int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& 
 }
 
 template <typename S, typename R>
-void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const Mask& mk, const int bc[6],
-                        const int32_t* list, int64_t nlist, bool do_bounce, const Reduce& red,
-                        double* series, int64_t cap, int64_t* d_itime, bool advance, cudaStream_t st) {
+void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const int bc[6], const int32_t* list,
+                        const uint64_t* links, int64_t nlist, bool do_bounce, const Reduce& red, double* series,
+                        int64_t cap, int64_t* d_itime, bool advance, cudaStream_t st) {
     const int per_x = (bc[0] == 0 && bc[1] == 0), per_y = (bc[2] == 0 && bc[3] == 0);
     const int per_z = (bc[4] == 0 && bc[5] == 0);
     const unsigned blocks = grid_for(nlist, kTpb, (unsigned)red.max_blocks);
-    k_bounce_drag<S, R><<<blocks, kTpb, 0, st>>>(L, g, mk, per_x, per_y, per_z, list, nlist, do_bounce ? 1 : 0,
+    k_bounce_drag<S, R><<<blocks, kTpb, 0, st>>>(L, g, per_x, per_y, per_z, list, links, nlist, do_bounce ? 1 : 0,
                                                  red, series, cap, d_itime, advance ? 1 : 0);
 }
 
@@ -594,8 +559,8 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
 
 #define EUP_INST(S, R)                                                                                 \
     template int launch_bc<S, R>(const Lat<S, R>&, const Geo&, const int*, const Phys<R>&, cudaStream_t); \
-    template void launch_bounce_drag<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const int*,      \
-                                           const int32_t*, int64_t, bool, const Reduce&, double*,      \
+    template void launch_bounce_drag<S, R>(const Lat<S, R>&, const Geo&, const int*, const int32_t*,   \
+                                           const uint64_t*, int64_t, bool, const Reduce&, double*,     \
                                            int64_t, int64_t*, bool, cudaStream_t);                     \
     template void launch_fill_xface<S, R>(const Lat<S, R>&, const Geo&, cudaStream_t);                 \
     template void launch_monitor<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const Reduce&,       \

@@ -55,6 +55,29 @@ __global__ void k_links(Geo g, Mask mk, uint32_t* links) {
     links[lin] = w;
 }
 
+__global__ void k_bsolid_links(Geo g, Mask mk, int per_x, int per_y, int per_z, const int32_t* list, int64_t n,
+                               uint64_t* links) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int64_t lin = list[t];
+    const int i = (int)(lin % g.l) + 1, j = (int)((lin / g.l) % g.m) + 1, k = (int)(lin / g.lm) + 1;
+    uint64_t w = 0;
+    for (int q = 0; q < 18; ++q) {
+        const int ni = i + cx_of(q), nj = j + cy_of(q), nk = k + cz_of(q);
+        if (g.interior(ni, nj, nk)) {
+            if (!mk.solid(g, ni, nj, nk)) w |= 1ull << q;
+        } else {
+            w |= 1ull << (18 + q);
+            int wi = ni, wj = nj, wk = nk;
+            if (per_x) wi = wi < 1 ? wi + g.l : (wi > g.l ? wi - g.l : wi);
+            if (per_y) wj = wj < 1 ? wj + g.m : (wj > g.m ? wj - g.m : wj);
+            if (per_z) wk = wk < 1 ? wk + g.n : (wk > g.n ? wk - g.n : wk);
+            if (g.interior(wi, wj, wk) && !mk.solid(g, wi, wj, wk)) w |= 1ull << (36 + q);
+        }
+    }
+    links[t] = w;
+}
+
 unsigned blocks_for(int64_t n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
 
 }  // namespace
@@ -66,6 +89,14 @@ void launch_build_mask(const int32_t* obs, const Geo& g, uint32_t* bits, int wpr
 
 void launch_flag_boundary_solid(const Geo& g, const Mask& mk, uint8_t* flags, cudaStream_t st) {
     k_flag_boundary_solid<<<blocks_for(g.N, 256), 256, 0, st>>>(g, mk, flags);
+}
+
+void launch_bsolid_links(const Geo& g, const Mask& mk, const int bc[6], const int32_t* list, int64_t n,
+                         uint64_t* links, cudaStream_t st) {
+    if (n <= 0) return;
+    const int per_x = (bc[0] == 0 && bc[1] == 0), per_y = (bc[2] == 0 && bc[3] == 0);
+    const int per_z = (bc[4] == 0 && bc[5] == 0);
+    k_bsolid_links<<<blocks_for(n, 256), 256, 0, st>>>(g, mk, per_x, per_y, per_z, list, n, links);
 }
 
 void launch_links(const Geo& g, const Mask& mk, uint32_t* links, cudaStream_t st) {

@@ -11,9 +11,38 @@ namespace eup {
 
 namespace {
 
+// What the kernels compute with: the population f itself (FP32/FP64 storage,
+// reference arithmetic), or the scaled deviation D = (f - w)*S (16-bit
+// storage, collide_dev).  Values from the halo shell are always f.
+template <typename S, typename R>
+struct KOps {
+    static constexpr bool dev = DevStore<S>::value;
+    static __device__ __forceinline__ R val(S raw, int q, const Lat<S, R>& L) {
+        if constexpr (dev) return DevStore<S>::to_f(raw);
+        else return Store<S, R>::load(raw, q, L.inv_scale);
+    }
+    static __device__ __forceinline__ R from_shell(R f, int q, const Lat<S, R>& L) {
+        if constexpr (dev) return (f - weight<R>(q)) * L.scale;
+        else return f;
+    }
+    static __device__ __forceinline__ R pull(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k) {
+        if (g.interior(i, j, k)) return val(L.pop[q][g.lin(i, j, k)], q, L);
+        return from_shell(L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)], q, L);
+    }
+    static __device__ __forceinline__ void collide_node(R* x, const Phys<R>& ph, const Lat<S, R>& L) {
+        if constexpr (dev) collide_dev(x, ph.omega, ph.omega1, ph.fgrad, L.scale, L.inv_scale);
+        else collide<R>(x, ph.omega, ph.omega1, ph.fgrad);
+    }
+    static __device__ __forceinline__ S store(R v, int q, const Lat<S, R>& L) {
+        if constexpr (dev) return DevStore<S>::from_f(v);
+        else return Store<S, R>::store(v, q, L.scale);
+    }
+};
+
 // One thread per node; grid (ceil(l/bx), m, n).
 template <typename S, typename R>
 __global__ void __launch_bounds__(128) k_stream_collide_scalar(Lat<S, R> src, Lat<S, R> dst, Geo g, Phys<R> ph) {
+    using K = KOps<S, R>;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y + 1;
     const int k = blockIdx.z + 1;
@@ -25,20 +54,24 @@ __global__ void __launch_bounds__(128) k_stream_collide_scalar(Lat<S, R> src, La
 #pragma unroll
         for (int q = 0; q < 18; ++q) {
             const int64_t s = lin - cx_of(q) - (int64_t)cy_of(q) * g.l - (int64_t)cz_of(q) * g.lm;
-            x[q] = Store<S, R>::load(src.pop[q][s], q, src.inv_scale);
+            x[q] = K::val(src.pop[q][s], q, src);
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < 18; ++q) x[q] = lat_load(src, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
+        for (int q = 0; q < 18; ++q) x[q] = K::pull(src, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
     }
-    x[18] = Store<S, R>::load(src.pop[18][lin], 18, src.inv_scale);
-    collide<R>(x, ph.omega, ph.omega1, ph.fgrad);
+    x[18] = K::val(src.pop[18][lin], 18, src);
+    K::collide_node(x, ph, src);
+    S out[19];
 #pragma unroll
-    for (int q = 0; q < 19; ++q) dst.pop[q][lin] = Store<S, R>::store(x[q], q, dst.scale);
+    for (int q = 0; q < 19; ++q) {
+        out[q] = K::store(x[q], q, dst);
+        dst.pop[q][lin] = out[q];
+    }
     if (i == 1 || i == g.l) {
 #pragma unroll
         for (int q = 0; q < 18; ++q) {
-            const R v = stored_value<S, R>(x[q], q, dst.scale, dst.inv_scale);
+            const R v = Store<S, R>::load(out[q], q, dst.inv_scale);
             if (i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = v;
             if (i == g.l) dst.xface[xface_idx(g, 1, q, j, k)] = v;
         }
@@ -80,6 +113,7 @@ __device__ __forceinline__ void st_pack(S* ptr, const Pack<S, VW>& p) {
 
 template <typename S, typename R, int VW>
 __global__ void __launch_bounds__(256) k_stream_collide_vec(Lat<S, R> src, Lat<S, R> dst, Geo g, Phys<R> ph) {
+    using K = KOps<S, R>;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;  // vector index within the row
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z + 1;
@@ -93,23 +127,42 @@ __global__ void __launch_bounds__(256) k_stream_collide_vec(Lat<S, R> src, Lat<S
     Pack<S, VW> in[19];
     R edge[19];  // x-neighbour element for cx = +1 (left) and cx = -1 (right) populations
     if (!face) {
+        // 1) every vector load of the node group first, so all 19 are in flight together
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const int cy = (q == 18) ? 0 : cy_of(q), cz = (q == 18) ? 0 : cz_of(q);
+            ld_pack<S, VW>(in[q], src.pop[q] + row - (int64_t)cy * g.l - (int64_t)cz * g.lm + (int64_t)t * VW);
+        }
+        // 2) the edge elements this lane cannot get from a neighbour lane: predicated
+        //    loads from the row (lanes 0/31) or from the x halo (row ends)
+        const bool lo_row = (t == 0), hi_row = (t == nvec - 1);
+        const bool lo_glob = (lane == 0) && !lo_row, hi_glob = (lane == 31) && !hi_row;
 #pragma unroll
         for (int q = 0; q < 18; ++q) {
+            if (cx_of(q) == 0) continue;
             const S* rp = src.pop[q] + row - (int64_t)cy_of(q) * g.l - (int64_t)cz_of(q) * g.lm;
-            ld_pack<S, VW>(in[q], rp + (int64_t)t * VW);
+            R e = R(0);
             if (cx_of(q) == 1) {
-                R e = __shfl_up_sync(0xffffffffu, Store<S, R>::load(in[q].s[VW - 1], q, src.inv_scale), 1);
-                if (t == 0) e = src.ghost[(int64_t)q * g.G + g.gidx(0, j - cy_of(q), k - cz_of(q))];
-                else if (lane == 0) e = Store<S, R>::load(rp[(int64_t)t * VW - 1], q, src.inv_scale);
-                edge[q] = e;
+                if (lo_glob) e = K::val(__ldg(rp + (int64_t)t * VW - 1), q, src);
+                if (lo_row) e = K::from_shell(src.ghost[(int64_t)q * g.G + g.gidx(0, j - cy_of(q), k - cz_of(q))], q, src);
+            } else {
+                if (hi_glob) e = K::val(__ldg(rp + (int64_t)t * VW + VW), q, src);
+                if (hi_row)
+                    e = K::from_shell(src.ghost[(int64_t)q * g.G + g.gidx(g.l + 1, j - cy_of(q), k - cz_of(q))], q, src);
+            }
+            edge[q] = e;
+        }
+        // 3) neighbour-lane elements by shuffle
+#pragma unroll
+        for (int q = 0; q < 18; ++q) {
+            if (cx_of(q) == 1) {
+                const R e = __shfl_up_sync(0xffffffffu, K::val(in[q].s[VW - 1], q, src), 1);
+                if (!lo_glob && !lo_row) edge[q] = e;
             } else if (cx_of(q) == -1) {
-                R e = __shfl_down_sync(0xffffffffu, Store<S, R>::load(in[q].s[0], q, src.inv_scale), 1);
-                if (t == nvec - 1) e = src.ghost[(int64_t)q * g.G + g.gidx(g.l + 1, j - cy_of(q), k - cz_of(q))];
-                else if (lane == 31) e = Store<S, R>::load(rp[(int64_t)t * VW + VW], q, src.inv_scale);
-                edge[q] = e;
+                const R e = __shfl_down_sync(0xffffffffu, K::val(in[q].s[0], q, src), 1);
+                if (!hi_glob && !hi_row) edge[q] = e;
             }
         }
-        ld_pack<S, VW>(in[18], src.pop[18] + row + (int64_t)t * VW);
     }
 
     Pack<S, VW> out[19];
@@ -120,19 +173,19 @@ __global__ void __launch_bounds__(256) k_stream_collide_vec(Lat<S, R> src, Lat<S
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
                 const int c = (q == 18) ? 0 : cx_of(q);
-                if (c == 0) x[q] = Store<S, R>::load(in[q].s[e], q, src.inv_scale);
-                else if (c == 1) x[q] = (e == 0) ? edge[q] : Store<S, R>::load(in[q].s[e - 1], q, src.inv_scale);
-                else x[q] = (e == VW - 1) ? edge[q] : Store<S, R>::load(in[q].s[e + 1], q, src.inv_scale);
+                if (c == 0) x[q] = K::val(in[q].s[e], q, src);
+                else if (c == 1) x[q] = (e == 0) ? edge[q] : K::val(in[q].s[e - 1], q, src);
+                else x[q] = (e == VW - 1) ? edge[q] : K::val(in[q].s[e + 1], q, src);
             }
         } else {
             const int i = i0 + e;
 #pragma unroll
-            for (int q = 0; q < 18; ++q) x[q] = lat_load(src, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
-            x[18] = Store<S, R>::load(src.pop[18][row + i - 1], 18, src.inv_scale);
+            for (int q = 0; q < 18; ++q) x[q] = K::pull(src, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
+            x[18] = K::val(src.pop[18][row + i - 1], 18, src);
         }
-        collide<R>(x, ph.omega, ph.omega1, ph.fgrad);
+        K::collide_node(x, ph, src);
 #pragma unroll
-        for (int q = 0; q < 19; ++q) out[q].s[e] = Store<S, R>::store(x[q], q, dst.scale);
+        for (int q = 0; q < 19; ++q) out[q].s[e] = K::store(x[q], q, dst);
         if ((e == 0 && t == 0) || (e == VW - 1 && t == nvec - 1)) {  // x = 1 or x = l column
             const int side = (e == 0 && t == 0) ? 0 : 1;
 #pragma unroll
@@ -144,26 +197,34 @@ __global__ void __launch_bounds__(256) k_stream_collide_vec(Lat<S, R> src, Lat<S
     for (int q = 0; q < 19; ++q) st_pack<S, VW>(dst.pop[q] + row + (int64_t)t * VW, out[q]);
 }
 
+// Nodes per thread of the vector kernels: 16-byte vectors (4 FP32, 2 FP64,
+// 8 FP16/BF16) or 8-byte vectors (half that).
 template <typename S> struct VecWidth { static constexpr int value = 16 / sizeof(S); };
+
+template <typename S, typename R, int VW>
+bool launch_vec(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph, cudaStream_t st) {
+    if (g.l % (32 * VW) != 0) return false;
+    const int nvec = g.l / VW;
+    int tx = nvec;
+    while (tx > 256) tx /= 2;  // nvec is a multiple of 32; keep tx a multiple of 32 dividing nvec
+    if (tx % 32 != 0 || nvec % tx != 0) tx = 32;
+    const int ty = (256 / tx) > 0 ? 256 / tx : 1;
+    dim3 block(tx, ty, 1);
+    dim3 grid(nvec / tx, (g.m + ty - 1) / ty, g.n);
+    k_stream_collide_vec<S, R, VW><<<grid, block, 0, st>>>(src, dst, g, ph);
+    return true;
+}
 
 }  // namespace
 
 template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph,
                            int variant, cudaStream_t st) {
+    // EUP_STEP_VARIANT bit 0: 16-byte vectors, bit 2: 8-byte vectors (when l allows);
+    // default: one node per thread, the fastest on B200 in every storage format measured.
     constexpr int VW = VecWidth<S>::value;
-    const bool vec_ok = (g.l % (32 * VW)) == 0;
-    if (!(variant & 1) && vec_ok) {
-        const int nvec = g.l / VW;
-        int tx = nvec;
-        while (tx > 256) tx /= 2;  // nvec is a multiple of 32; keep tx a multiple of 32 dividing nvec
-        if (tx % 32 != 0 || nvec % tx != 0) tx = 32;
-        const int ty = (256 / tx) > 0 ? 256 / tx : 1;
-        dim3 block(tx, ty, 1);
-        dim3 grid(nvec / tx, (g.m + ty - 1) / ty, g.n);
-        k_stream_collide_vec<S, R, VW><<<grid, block, 0, st>>>(src, dst, g, ph);
-        return;
-    }
+    if ((variant & 1) && launch_vec<S, R, VW>(src, dst, g, ph, st)) return;
+    if ((variant & 4) && launch_vec<S, R, (VW / 2 > 0 ? VW / 2 : 1)>(src, dst, g, ph, st)) return;
     const int bx = 128;
     dim3 grid((g.l + bx - 1) / bx, g.m, g.n);
     k_stream_collide_scalar<S, R><<<grid, bx, 0, st>>>(src, dst, g, ph);

@@ -261,6 +261,67 @@ __device__ __forceinline__ void collide(R* x, R omega, R omega1, R fgrad) {
     x[18] = omega1 * x[18] + (omega * de19);
 }
 
+// ---------------------------------------------------------------------------
+// 16-bit storage works on the stored quantity itself, D_q = (f_q - w_q)*S.
+// Because sum_q w_q = 1 and sum_q w_q c_q = 0, density and momentum follow
+// from D directly (rho - 1 = sum D / S, j = sum c D / S), and BGK maps
+// deviations to deviations:
+//   D'_q = (1-omega) D_q + S [omega (feq_q - w_q) + F_q],
+//   feq_q - w_q = w_q [(rho-1) + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)],
+// the equilibrium of CODE/SRC/col.F90:190-208 written about w_q.  Loads and
+// stores are then plain conversions and no step subtracts two nearly equal
+// numbers.  Arithmetic is FP32 with explicit fused multiply-adds.
+// ---------------------------------------------------------------------------
+template <typename S> struct DevStore { static constexpr bool value = false; };
+template <> struct DevStore<__half> {
+    static constexpr bool value = true;
+    static __device__ __forceinline__ float to_f(__half s) { return __half2float(s); }
+    static __device__ __forceinline__ __half from_f(float d) { return __float2half_rn(d); }
+};
+template <> struct DevStore<__nv_bfloat16> {
+    static constexpr bool value = true;
+    static __device__ __forceinline__ float to_f(__nv_bfloat16 s) { return __bfloat162float(s); }
+    static __device__ __forceinline__ __nv_bfloat16 from_f(float d) { return __float2bfloat16_rn(d); }
+};
+
+// One opposite pair (qp, qm) with c_qp . u = v, c_qm = -c_qp; fx = +-1/0 the
+// x component of c_qp (body force along x).
+__device__ __forceinline__ void dev_pair(float* D, int qp, int qm, float v, float w, float rm1, float rho, float t,
+                                         float oS, float omega1, float fS, float fx) {
+    const float a = __fmaf_rn(rho, __fmaf_rn(4.5f * v, v, -t), rm1);   // (rho-1) + rho (4.5 v^2 - 1.5 u^2)
+    const float b = 3.0f * rho * v;
+    const float ow = oS * w;
+    D[qp] = __fmaf_rn(omega1, D[qp], __fmaf_rn(ow, a + b, fx * fS));
+    D[qm] = __fmaf_rn(omega1, D[qm], __fmaf_rn(ow, a - b, -fx * fS));
+}
+
+__device__ __forceinline__ void collide_dev(float* D, float omega, float omega1, float fgrad, float S, float invS) {
+    float s = D[0];
+#pragma unroll
+    for (int q = 1; q < 19; ++q) s += D[q];
+    const float rm1 = s * invS;
+    const float rho = 1.0f + rm1;
+    const float jx = (D[0] + D[1] + D[2] + D[3] + D[4]) - (D[9] + D[10] + D[11] + D[12] + D[13]);
+    const float jy = (D[2] + D[6] + D[7] + D[8] + D[11]) - (D[0] + D[9] + D[15] + D[16] + D[17]);
+    const float jz = (D[3] + D[5] + D[6] + D[12] + D[17]) - (D[1] + D[8] + D[10] + D[14] + D[15]);
+    const float ri = invS / rho;
+    const float ux = jx * ri, uy = jy * ri, uz = jz * ri;
+    const float t = 1.5f * __fmaf_rn(ux, ux, __fmaf_rn(uy, uy, uz * uz));
+    const float oS = omega * S;
+    const float fS = S * fgrad * rho;
+    const float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
+    dev_pair(D, 4, 13, ux, w1, rm1, rho, t, oS, omega1, fS, 1.f);        // a05 / a14
+    dev_pair(D, 5, 14, uz, w1, rm1, rho, t, oS, omega1, fS, 0.f);        // a06 / a15
+    dev_pair(D, 7, 16, uy, w1, rm1, rho, t, oS, omega1, fS, 0.f);        // a08 / a17
+    dev_pair(D, 0, 11, ux - uy, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a01 / a12
+    dev_pair(D, 1, 12, ux - uz, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a02 / a13
+    dev_pair(D, 2, 9, ux + uy, w2, rm1, rho, t, oS, omega1, fS, 1.f);    // a03 / a10
+    dev_pair(D, 3, 10, ux + uz, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a04 / a11
+    dev_pair(D, 6, 15, uy + uz, w2, rm1, rho, t, oS, omega1, fS, 0.f);   // a07 / a16
+    dev_pair(D, 8, 17, uy - uz, w2, rm1, rho, t, oS, omega1, fS, 0.f);   // a09 / a18
+    D[18] = __fmaf_rn(omega1, D[18], oS * w0 * __fmaf_rn(-rho, t, rm1));  // a19
+}
+
 // Physical constants of one run, rounded to the arithmetic type the way
 // CODE/SRC/hencol.F90:30-39 rounds them to mykind.
 template <typename R>

@@ -59,5 +59,6 @@ def test_fullsize_fp16_tracks_fp32(eup, require_gpu, shell):
     p16, f16, m16 = out[eup.FP16_DEV]
     rel = np.linalg.norm(p16[:, 1:] - p32[:, 1:]) / np.linalg.norm(p32[:, 1:])
     assert rel < 1e-3, rel
-    assert abs(m16[0] - m32[0]) / m32[0] < 1e-6
+    # open inflow/outflow system: the total mass follows the (slightly different) flow
+    assert abs(m16[0] - m32[0]) / m32[0] < 2e-4
     assert abs(f16[0] - f32[0]) / abs(f32[0]) < 5e-3

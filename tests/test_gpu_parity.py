@@ -44,7 +44,7 @@ CASES = [
     ("obstacle_on_faces", (24, 12, 10), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _wall_touch),
     ("noslip_y_periodic_z_inflow", (20, 10, 9), (5, 4, 1, 1, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
     ("freeslip_z_periodic_y", (20, 10, 9), (5, 4, 0, 0, 3, 3), 0.01, 0.0, 0.05, 0.0, _cyl),
-    # l a multiple of 128: the vectorised stream-collide kernel (16-byte rows) runs
+    # l a multiple of 128: with EUP_STEP_VARIANT the vectorised kernels can run (see below)
     ("vec_cylinder", (128, 24, 10), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
     ("vec_freeslip_all", (128, 18, 14), (5, 4, 3, 3, 3, 3), 0.0024, 0.0, 0.05, 0.0, _block),
     ("vec_periodic_x_body_force", (128, 12, 10), (0, 0, 3, 3, 1, 1), 0.05, 0.05, 0.0, 0.0, _wall_touch),
@@ -203,8 +203,8 @@ def test_deviation_storage_against_fp64(eup, require_gpu, prec):
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16", "bf16"])
 def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
-    """Vectorised vs one-node-per-thread stream-collide, CUDA graphs vs plain
-    launches: all four paths give the same bits in every storage format."""
+    """One-node-per-thread vs 16-byte and 8-byte vectorised stream-collide, CUDA
+    graphs vs plain launches: all paths give the same bits in every storage format."""
     l, m, n = 256, 20, 12
     code = {"fp32": eup.FP32, "fp64": eup.FP64, "fp16": eup.FP16_DEV, "bf16": eup.BF16_DEV}[prec]
     dt = np.float64 if prec == "fp64" else np.float32
@@ -212,7 +212,7 @@ def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
     a = eup.init_equilibrium(l, m, n, 0.05, 1e-3, 77, dt)
     cfg = eup.Config(l, m, n, bc=(5, 4, 3, 3, 0, 0), svisc=0.01, u_inflow=0.05, precision=code)
     res = []
-    for var in ("0", "1", "2", "3"):
+    for var in ("0", "1", "2", "3", "4", "6"):
         monkeypatch.setenv("EUP_STEP_VARIANT", var)
         with eup.Solver(cfg) as s:
             s.set_obstacles(obs)
