@@ -37,7 +37,7 @@ EXPORTED = [
     "eup_get_itime", "eup_get_forces", "eup_get_force_series", "eup_get_cd_series", "eup_get_monitor",
     "eup_get_probes", "eup_get_links", "eup_get_boundary_solid", "eup_read_obs_file", "eup_write_obs_file",
     "eup_read_raw_state", "eup_write_raw_state", "eup_init_equilibrium", "eup_geometry_cylinder_z",
-    "eup_geometry_reticular_shell",
+    "eup_geometry_reticular_shell", "eup_mem_force_noalloc",
 ]
 
 
@@ -92,6 +92,7 @@ def _load():
         "eup_geometry_cylinder_z": ([i32, i32, i32, dbl, dbl, dbl, vp], ctypes.c_int),
         "eup_geometry_reticular_shell": ([i32, i32, i32, dbl, dbl, dbl, dbl, dbl, dbl, dbl, ctypes.c_uint64, vp],
                                          ctypes.c_int),
+        "eup_mem_force_noalloc": ([i32, i32, i32, ctypes.c_int32 * 6, P19, i32, vp, vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

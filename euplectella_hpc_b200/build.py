@@ -22,7 +22,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libeup.so")
 
-SOURCES = ["abi.cu", "k_bc.cu", "k_step.cu", "k_setup.cu", "host.cpp"]
+SOURCES = ["abi.cu", "k_bc.cu", "k_step.cu", "k_setup.cu", "host.cpp", "noalloc.cu"]
 HEADERS = ["lbm_common.cuh", "internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-fopenmp,-Wall",

@@ -192,6 +192,27 @@ int eup_get_links(eup_handle* h, uint32_t* links);
  * entries are written. */
 int eup_get_boundary_solid(eup_handle* h, int64_t* list, int64_t cap, int64_t* count);
 
+/* No counterpart in the reference.  Momentum-exchange force (same definition
+ * as eup_get_forces) of a state that lives in the CALLER's device memory, for
+ * callers that cannot let a library allocate: e.g. a Fortran driver whose
+ * a01..a19 and obs are already device-resident under its own OpenACC data
+ * region, or code that captures its time loop into a CUDA graph, where
+ * cudaMalloc is not allowed.  Needs no handle and allocates nothing: its
+ * scratch is one fixed device array in the library (one FP64 partial per
+ * z-plane, at most 4096 planes, about 96 KiB per GPU, held until the process
+ * exits); lz > 4096 is rejected with EUP_ERR_UNSUPPORTED.
+ *   pops[19]  device pointers to the haloed arrays a01..a19(0:l+1,0:m+1,0:n+1),
+ *             float (elem_bytes 4) or double (8);
+ *   obs       device pointer to obs(1:l,1:m,1:n), 1 = solid;
+ *   bc[6]     reference face flags (axes with both faces periodic wrap);
+ *   force     device pointer receiving 3 doubles;
+ *   stream    cudaStream_t to run on (NULL: the legacy default stream).
+ * Asynchronous on `stream`.  The first call on each device looks up the
+ * scratch address (cudaGetSymbolAddress); make it before any stream capture.
+ * All calls share the scratch: calls that overlap on the GPU race. */
+int eup_mem_force_noalloc(int32_t l, int32_t m, int32_t n, const int32_t bc[6], const void* const pops[19],
+                          int32_t elem_bytes, const int32_t* obs, double* force, void* stream);
+
 /* ---- host utilities (no GPU) ---------------------------------------------- */
 
 /* Reads obs.RRRR.TTTTTTTT.bin (CODE/SRC/build.obs.F90:147-177): Fortran
