@@ -37,7 +37,8 @@ EXPORTED = [
     "eup_get_itime", "eup_get_forces", "eup_get_force_series", "eup_get_cd_series", "eup_get_monitor",
     "eup_get_probes", "eup_get_links", "eup_get_boundary_solid", "eup_read_obs_file", "eup_write_obs_file",
     "eup_read_raw_state", "eup_write_raw_state", "eup_init_equilibrium", "eup_geometry_cylinder_z",
-    "eup_geometry_reticular_shell", "eup_mem_force_noalloc",
+    "eup_geometry_reticular_shell", "eup_mem_force_noalloc", "eup_set_solid_fraction", "eup_adjoint_run",
+    "eup_geometry_ridged_shell",
 ]
 
 
@@ -59,6 +60,11 @@ class CConfig(ctypes.Structure):
         ("cd_span", ctypes.c_double),
         ("series_capacity", ctypes.c_int64),
     ]
+
+
+class AdjointConfig(ctypes.Structure):
+    _fields_ = [("nsteps", ctypes.c_int32), ("avg_steps", ctypes.c_int32), ("checkpoints", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 def _load():
@@ -93,6 +99,9 @@ def _load():
         "eup_geometry_reticular_shell": ([i32, i32, i32, dbl, dbl, dbl, dbl, dbl, dbl, dbl, ctypes.c_uint64, vp],
                                          ctypes.c_int),
         "eup_mem_force_noalloc": ([i32, i32, i32, ctypes.c_int32 * 6, P19, i32, vp, vp, vp], ctypes.c_int),
+        "eup_set_solid_fraction": ([vp, vp], ctypes.c_int),
+        "eup_geometry_ridged_shell": ([i32, i32, i32] + [dbl] * 12 + [ctypes.c_uint64, vp, vp], ctypes.c_int),
+        "eup_adjoint_run": ([vp, ctypes.POINTER(AdjointConfig), ctypes.POINTER(dbl), vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -276,6 +285,28 @@ class Solver:
         self._ck(lib.eup_get_links(self._h, out.ctypes.data))
         return out
 
+    def set_solid_fraction(self, ns):
+        """Partial-bounce-back solid fraction n_s(1:l,1:m,1:n) in [0,1] (shape (n, m, l)); None switches it off."""
+        if ns is None:
+            self._ck(lib.eup_set_solid_fraction(self._h, None))
+            return
+        ns = np.ascontiguousarray(ns, dtype=np.float64)
+        assert ns.shape == (self.cfg.lz, self.cfg.ly, self.cfg.lx)
+        self._keep_ns = ns
+        self._ck(lib.eup_set_solid_fraction(self._h, ns.ctypes.data))
+
+    def adjoint(self, nsteps: int, avg_steps: int, checkpoints: int = 0):
+        """Runs nsteps forward and the discrete adjoint back: returns (objective = mean C_d over the
+        last avg_steps steps, dJ/dn_s of shape (n, m, l), stats dict)."""
+        cfg = AdjointConfig(nsteps, avg_steps, checkpoints, 0)
+        obj = ctypes.c_double()
+        grad = np.zeros((self.cfg.lz, self.cfg.ly, self.cfg.lx), dtype=np.float64)
+        st = np.zeros(8, dtype=np.float64)
+        self._ck(lib.eup_adjoint_run(self._h, ctypes.byref(cfg), ctypes.byref(obj), grad.ctypes.data, st.ctypes.data))
+        keys = ["forward_ms", "reverse_ms", "recomputed_steps", "checkpoints", "segment_steps", "state_bytes",
+                "nsteps", "avg_steps"]
+        return obj.value, grad, dict(zip(keys, st.tolist()))
+
     def boundary_solid(self) -> np.ndarray:
         cnt = ctypes.c_int64()
         self._ck(lib.eup_get_boundary_solid(self._h, None, 0, ctypes.byref(cnt)))
@@ -331,3 +362,16 @@ def geometry_reticular_shell(l, m, n, x0, length, yc, zc, outer_d, strut_d, pitc
                                             float(outer_d), float(strut_d), float(pitch), int(seed),
                                             obs.ctypes.data))
     return obs
+
+
+def geometry_ridged_shell(l, m, n, x0, length, yc, zc, outer_d, strut_d, pitch, ridge_h, ridge_t, cap_t, pore_d,
+                          smooth_w, seed, with_derivative=False):
+    """Ridged reticular shell with a porous cap as a solid fraction (n, m, l); with
+    with_derivative also d ns / d ridge_h."""
+    ns = np.zeros((n, m, l), dtype=np.float64)
+    d = np.zeros_like(ns) if with_derivative else None
+    _check(lib.eup_geometry_ridged_shell(l, m, n, float(x0), float(length), float(yc), float(zc), float(outer_d),
+                                         float(strut_d), float(pitch), float(ridge_h), float(ridge_t), float(cap_t),
+                                         float(pore_d), float(smooth_w), int(seed), ns.ctypes.data,
+                                         d.ctypes.data if d is not None else None))
+    return (ns, d) if with_derivative else ns

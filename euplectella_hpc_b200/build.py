@@ -21,8 +21,9 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libeup.so")
+DRIVER = os.path.join(LIB_DIR, "eup_bgk3d")
 
-SOURCES = ["abi.cu", "k_bc.cu", "k_step.cu", "k_setup.cu", "host.cpp", "noalloc.cu"]
+SOURCES = ["abi.cu", "k_bc.cu", "k_step.cu", "k_setup.cu", "k_adjoint.cu", "host.cpp", "noalloc.cu"]
 HEADERS = ["lbm_common.cuh", "internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-fopenmp,-Wall",
@@ -70,6 +71,11 @@ def build(verbose: bool = False, force: bool = False) -> str:
         list(ex.map(run, jobs))
     if force or jobs or _stale(LIB, objs):
         run([nv, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fopenmp", "-o", LIB, *objs, "-lgomp"])
+    # the reference program's driver over the C ABI
+    drv_src = os.path.join(CSRC, "driver", "eup_bgk3d.cpp")
+    if force or _stale(DRIVER, [drv_src, LIB, os.path.join(ROOT, "include", "eup.h")]):
+        run([shutil.which("g++") or "g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), drv_src,
+             "-L", LIB_DIR, "-leup", "-Wl,-rpath,$ORIGIN", "-o", DRIVER])
     return LIB
 
 

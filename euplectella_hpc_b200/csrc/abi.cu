@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/eup.h"
@@ -42,6 +43,8 @@ struct eup_handle {
     bool has_state = false;
     double scale = 1.0;
     int variant = 0;  // EUP_STEP_VARIANT: bit 0/2 16/8-byte vector stream-collide, bit 1 no CUDA graphs
+    bool pbb = false;             // partial-bounce-back model active (solid fraction set)
+    void* ns = nullptr;           // solid fraction n_s per interior node, arithmetic type
     int64_t launches = 0;  // kernels launched by eup_step / eup_step_profiled
     int launches_per_step = 0;
     std::string err;
@@ -131,6 +134,17 @@ int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
     const Lat<S, R> src = make_lat<S, R>(h, src_idx), dst = make_lat<S, R>(h, src_idx ^ 1);
     int n = 0;
     if (pe) pe->mark(4 * s + 0, h->stream);
+    if constexpr (std::is_same<S, R>::value) {
+        if (h->pbb) {  // partial bounce-back: halo planes, then stream + PBB collide (force of the step)
+            if (pe) pe->mark(4 * s + 1, h->stream);
+            n += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
+            if (pe) pe->mark(4 * s + 2, h->stream);
+            launch_pbb_step<R>(src, dst, h->g, ph, static_cast<const R*>(h->ns), make_reduce(h), h->series, h->cap,
+                               h->d_itime, h->stream);
+            if (pe) pe->mark(4 * s + 3, h->stream);
+            return n + 1;
+        }
+    }
     // boundaries: bounce-back then halo planes (CODE/SRC/boundaries.F90:36-49,235-248)
     launch_bounce_drag<S, R>(src, h->g, bc, h->blist, h->blinks, h->nblist, true, make_reduce(h), h->series,
                              h->cap, h->d_itime, true, h->stream);
@@ -192,8 +206,10 @@ cudaError_t enqueue_steps(eup_handle* h, int32_t nsteps, PhaseEvents* pe = nullp
             h->itime += 1;
         }
     }
-    enqueue_drag_only<S, R>(h);
-    h->launches += 1;
+    if (!h->pbb) {  // the partial-bounce-back step records its force itself
+        enqueue_drag_only<S, R>(h);
+        h->launches += 1;
+    }
     return cudaSuccess;
 }
 
@@ -367,7 +383,7 @@ int eup_destroy(eup_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
     void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->blinks, h->partials, h->counter,
-                    h->series, h->dscratch, h->staging, h->xface, h->d_itime};
+                    h->series, h->dscratch, h->staging, h->xface, h->d_itime, h->ns};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -382,6 +398,10 @@ int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
     const Geo& g = h->g;
     int64_t nsolid = 0;
     for (int64_t t = 0; t < g.N; ++t) nsolid += (obs[t] == 1);
+    if (nsolid > 0 && h->pbb)
+        return fail(h, EUP_ERR_UNSUPPORTED,
+                    "eup_set_obstacles: a solid-fraction field is set; the partial-bounce-back model takes no "
+                    "halfway-bounce-back voxels (fold them into the field as n_s = 1)");
     if (h->cfg.bc[EUP_FRONT] == EUP_BC_OUTFLOW) {
         for (int64_t r = 0; r < (int64_t)g.m * g.n; ++r)
             if (obs[r * g.l + (g.l - 1)] == 1)
@@ -416,7 +436,7 @@ int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
         const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
         launch_bsolid_links(g, make_mask(h), bc, h->blist, cnt, h->blinks, h->stream);
     }
-    if (h->has_state) DISPATCH(h, enqueue_drag_only, h);
+    if (h->has_state && !h->pbb) DISPATCH(h, enqueue_drag_only, h);
     CK(h, cudaGetLastError());
     CK(h, cudaStreamSynchronize(h->stream));
     return EUP_OK;
@@ -441,7 +461,8 @@ int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, in
     h->itime = itime;
     h->series_first = itime;
     h->has_state = true;
-    DISPATCH(h, enqueue_drag_only, h);
+    if (h->pbb) CK(h, cudaMemsetAsync(h->series + 3 * (itime % h->cap), 0, 3 * sizeof(double), h->stream));
+    else DISPATCH(h, enqueue_drag_only, h);
     CK(h, cudaGetLastError());
     CK(h, cudaStreamSynchronize(h->stream));
     return EUP_OK;
@@ -634,6 +655,229 @@ int eup_get_boundary_solid(eup_handle* h, int64_t* list, int64_t cap, int64_t* c
         for (int64_t t = 0; t < n; ++t) list[t] = tmp[(size_t)t];
     }
     return EUP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Partial bounce-back and the checkpointed discrete adjoint
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * (n > 0 ? n : 1)); }
+};
+
+template <typename T>
+cudaError_t upload_vec(DevBuf<T>& b, const std::vector<T>& v) {
+    cudaError_t e = b.alloc(v.size());
+    if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    return e;
+}
+
+// Lattice view of an arbitrary state buffer (19 arrays of Nq elements).
+template <typename R>
+Lat<R, R> lat_at(const eup_handle* h, R* base, R* shell = nullptr) {
+    Lat<R, R> L = make_lat<R, R>(h, 0);
+    for (int q = 0; q < Q; ++q) L.pop[q] = base + (size_t)q * h->Nq;
+    if (shell) L.ghost = shell;
+    return L;
+}
+
+// Forward sweep with checkpoints, reverse sweep recomputing each segment once.
+// Schedule: K = ceil(T / slots) steps per segment, ceil(T / K) checkpoints
+// (states 0, K, 2K, ...) plus a K-state segment buffer: every forward step is
+// recomputed at most once (binomial checkpointing at repetition number 2).
+template <typename R>
+int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, double* grad_out, double* stats) {
+    const Geo& g = h->g;
+    const int T = ac->nsteps, A = ac->avg_steps;
+    const int slots = ac->checkpoints > 0 ? ac->checkpoints : 64;
+    const int K = (T + slots - 1) / slots;
+    const int nseg = (T + K - 1) / K;
+    const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
+    const double norm = 0.5 * h->cfg.cd_rho0 * h->cfg.cd_uref * h->cfg.cd_uref * h->cfg.cd_length * h->cfg.cd_span;
+    const double gamma = 1.0 / ((double)A * norm);
+    const Phys<R> ph = make_phys<R>(h);
+    const R* ns = static_cast<const R*>(h->ns);
+    cudaStream_t st = h->stream;
+
+    HaloAdjointTables tab;
+    std::string why;
+    if (build_halo_adjoint_tables(g, bc, &tab, &why) != EUP_OK) return fail(h, EUP_ERR_UNSUPPORTED, "eup_adjoint_run: " + why);
+    DevBuf<int64_t> d_ckey, d_cslot, d_oslot;
+    DevBuf<int32_t> d_cstart, d_ojk, d_ostart;
+    DevBuf<int8_t> d_oq;
+    CK(h, upload_vec(d_ckey, tab.copy_key));
+    CK(h, upload_vec(d_cstart, tab.copy_start));
+    CK(h, upload_vec(d_cslot, tab.copy_slot));
+    CK(h, upload_vec(d_ojk, tab.out_jk));
+    CK(h, upload_vec(d_ostart, tab.out_start));
+    CK(h, upload_vec(d_oslot, tab.out_slot));
+    CK(h, upload_vec(d_oq, tab.out_q));
+    HaloAdjointDevice td;
+    td.copy_key = d_ckey.p; td.copy_start = d_cstart.p; td.copy_slot = d_cslot.p; td.ncopy = (int64_t)tab.copy_key.size();
+    td.out_jk = d_ojk.p; td.out_start = d_ostart.p; td.out_slot = d_oslot.p; td.out_q = d_oq.p;
+    td.nout = (int64_t)tab.out_jk.size();
+
+    const size_t state = (size_t)Q * h->Nq;
+    const size_t shell = (size_t)Q * g.G;
+    DevBuf<R> ckpt, seg, seg_shell, lam, gmu, shell_save;
+    DevBuf<double> grad, scratch_series;
+    DevBuf<int64_t> scratch_itime;
+    CK(h, ckpt.alloc(state * nseg));
+    CK(h, seg.alloc(state * K));
+    CK(h, seg_shell.alloc(shell * K));
+    CK(h, lam.alloc(state * 2));
+    CK(h, gmu.alloc((size_t)Q * g.G));
+    CK(h, shell_save.alloc((size_t)Q * g.G));
+    CK(h, grad.alloc(g.N));
+    CK(h, scratch_series.alloc(3 * 2));
+    CK(h, scratch_itime.alloc(1));
+    CK(h, cudaMemsetAsync(grad.p, 0, sizeof(double) * g.N, st));
+    CK(h, cudaMemsetAsync(lam.p, 0, sizeof(R) * state * 2, st));
+    CK(h, cudaMemsetAsync(scratch_itime.p, 0, sizeof(int64_t), st));
+    const Reduce red = make_reduce(h);
+
+    cudaEvent_t ev[3];
+    for (auto& e : ev) CK(h, cudaEventCreate(&e));
+    // ---- forward sweep (the handle's own state, force series recorded) ----
+    const int64_t t0 = h->itime;
+    CK(h, cudaEventRecord(ev[0], st));
+    for (int s = 0; s < T; ++s) {
+        if (s % K == 0)
+            CK(h, cudaMemcpyAsync(ckpt.p + state * (s / K), h->lat[h->cur], sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
+        const Lat<R, R> src = make_lat<R, R>(h, h->cur), dst = make_lat<R, R>(h, h->cur ^ 1);
+        launch_bc<R, R>(src, g, bc, ph, st);
+        launch_pbb_step<R>(src, dst, g, ph, ns, red, h->series, h->cap, h->d_itime, st);
+        h->cur ^= 1;
+        h->itime += 1;
+    }
+    CK(h, cudaMemcpyAsync(shell_save.p, h->ghost, sizeof(R) * Q * g.G, cudaMemcpyDeviceToDevice, st));
+    CK(h, cudaEventRecord(ev[1], st));
+    CK(h, cudaGetLastError());
+    // objective: mean C_d over the last A steps (steps T-A+1 .. T)
+    std::vector<double> fser((size_t)3 * T);
+    CK(h, cudaStreamSynchronize(st));
+    for (int s = 1; s <= T; ++s) {
+        const int64_t pos = (t0 + s) % h->cap;
+        CK(h, cudaMemcpy(&fser[3 * (size_t)(s - 1)], h->series + 3 * pos, sizeof(double) * 3, cudaMemcpyDeviceToHost));
+    }
+    double J = 0.0;
+    for (int s = T - A + 1; s <= T; ++s) J += fser[3 * (size_t)(s - 1)];
+    J *= gamma;
+    if (!std::isfinite(J)) return fail(h, EUP_ERR_DIVERGED, "eup_adjoint_run: forward run diverged");
+
+    // ---- reverse sweep ----
+    // Every segment state keeps its own halo shell: the halo blocks of the step
+    // leaving it write there during recomputation and the adjoint step reads it.
+    // Slots no block writes hold their initial values, copied in once here.
+    for (int t = 0; t < K; ++t)
+        CK(h, cudaMemcpyAsync(seg_shell.p + shell * t, h->ghost, sizeof(R) * shell, cudaMemcpyDeviceToDevice, st));
+    int cur_lam = 0;  // lam[cur_lam] = adjoint of the state after the step being reversed
+    int64_t recomputed = 0;
+    for (int c = nseg - 1; c >= 0; --c) {
+        const int a = c * K, b = std::min(a + K, T);
+        // recompute states a .. b-1 into the segment buffer, with the halo of each
+        CK(h, cudaMemcpyAsync(seg.p, ckpt.p + state * c, sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
+        launch_fill_xface<R, R>(lat_at<R>(h, seg.p), g, st);
+        for (int s = a; s < b; ++s) {
+            const Lat<R, R> src = lat_at<R>(h, seg.p + state * (s - a), seg_shell.p + shell * (s - a));
+            launch_bc<R, R>(src, g, bc, ph, st);
+            if (s + 1 < b) {  // the step's x-face copy feeds the next halo blocks
+                const Lat<R, R> dst = lat_at<R>(h, seg.p + state * (s + 1 - a));
+                launch_pbb_step<R>(src, dst, g, ph, ns, red, scratch_series.p, 2, scratch_itime.p, st);
+                ++recomputed;
+            }
+        }
+        // adjoint steps b .. a+1: state s-1 -> s
+        for (int s = b; s > a; --s) {
+            const Lat<R, R> f = lat_at<R>(h, seg.p + state * (s - 1 - a), seg_shell.p + shell * (s - 1 - a));
+            const Lat<R, R> lin_ = lat_at<R>(h, lam.p + state * cur_lam), lout = lat_at<R>(h, lam.p + state * (cur_lam ^ 1));
+            const R gam = (s > T - A) ? (R)gamma : R(0);
+            launch_pbb_adjoint<R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st);
+            cur_lam ^= 1;
+        }
+    }
+    CK(h, cudaEventRecord(ev[2], st));
+    // restore the halo shell and x-face copy of the handle's current state
+    CK(h, cudaMemcpyAsync(h->ghost, shell_save.p, sizeof(R) * Q * g.G, cudaMemcpyDeviceToDevice, st));
+    launch_fill_xface<R, R>(make_lat<R, R>(h, h->cur), g, st);
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(grad_out, grad.p, sizeof(double) * g.N, cudaMemcpyDeviceToHost, st));
+    CK(h, cudaStreamSynchronize(st));
+    float fwd_ms = 0.f, rev_ms = 0.f;
+    cudaEventElapsedTime(&fwd_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&rev_ms, ev[1], ev[2]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    *objective = J;
+    if (stats) {
+        stats[0] = fwd_ms;
+        stats[1] = rev_ms;
+        stats[2] = (double)recomputed;
+        stats[3] = nseg;
+        stats[4] = K;
+        stats[5] = (double)(sizeof(R) * (state * (nseg + K + 2) + shell * K));
+        stats[6] = T;
+        stats[7] = A;
+    }
+    return EUP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int eup_set_solid_fraction(eup_handle* h, const double* ns) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    CK(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    if (!ns) {
+        if (h->ns) cudaFree(h->ns);
+        h->ns = nullptr;
+        h->pbb = false;
+        return EUP_OK;
+    }
+    if (h->prec != EUP_FP32 && h->prec != EUP_FP64)
+        return fail(h, EUP_ERR_UNSUPPORTED, "eup_set_solid_fraction: the partial-bounce-back model runs in FP32 or FP64");
+    if (h->nblist > 0 || h->bits)
+        return fail(h, EUP_ERR_UNSUPPORTED,
+                    "eup_set_solid_fraction: obstacles are set; fold them into the field as n_s = 1 instead");
+    const int64_t N = h->g.N;
+    for (int64_t t = 0; t < N; ++t)
+        if (!(ns[t] >= 0.0 && ns[t] <= 1.0))
+            return fail(h, EUP_ERR_INVALID_ARG, "eup_set_solid_fraction: n_s outside [0,1] at index " + std::to_string(t));
+    if (!h->ns) CK(h, cudaMalloc(&h->ns, h->rbytes * N));
+    if (h->prec == EUP_FP64) {
+        CK(h, cudaMemcpy(h->ns, ns, sizeof(double) * N, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> tmp((size_t)N);
+        for (int64_t t = 0; t < N; ++t) tmp[(size_t)t] = (float)ns[t];
+        CK(h, cudaMemcpy(h->ns, tmp.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+    }
+    h->pbb = true;
+    return EUP_OK;
+}
+
+int eup_adjoint_run(eup_handle* h, const eup_adjoint_config* cfg, double* objective, double* grad_ns,
+                    double stats[8]) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!cfg || !objective || !grad_ns) return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: null argument");
+    if (!h->pbb) return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: no solid-fraction field set");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: no state uploaded");
+    if (cfg->nsteps < 1 || cfg->avg_steps < 1 || cfg->avg_steps > cfg->nsteps || cfg->checkpoints < 0)
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: need 1 <= avg_steps <= nsteps, checkpoints >= 0");
+    if (!(h->cfg.cd_rho0 > 0 && h->cfg.cd_uref != 0 && h->cfg.cd_length > 0 && h->cfg.cd_span > 0))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: drag normalisation not set in eup_config");
+    if (h->prec == EUP_FP64) return adjoint_run<double>(h, cfg, objective, grad_ns, stats);
+    return adjoint_run<float>(h, cfg, objective, grad_ns, stats);
 }
 
 }  // extern "C"

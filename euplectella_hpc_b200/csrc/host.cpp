@@ -223,6 +223,87 @@ int eup_geometry_cylinder_z(int32_t l, int32_t m, int32_t n, double xc, double y
     return EUP_OK;
 }
 
+int eup_geometry_ridged_shell(int32_t l, int32_t m, int32_t n, double x0, double length, double yc, double zc,
+                              double outer_d, double strut_d, double pitch, double ridge_h, double ridge_t,
+                              double cap_t, double pore_d, double smooth_w, uint64_t seed, double* ns, double* dns_dh) {
+    if (!ns || l < 1 || m < 1 || n < 1 || !(ridge_h >= 0) || !(ridge_t > 0) || !(cap_t >= 0) || !(pore_d > 0))
+        return herr(EUP_ERR_INVALID_ARG, "eup_geometry_ridged_shell: bad argument");
+    const int64_t N = (int64_t)l * m * n;
+    std::vector<int32_t> shell((size_t)N);
+    int rc = eup_geometry_reticular_shell(l, m, n, x0, length, yc, zc, outer_d, strut_d, pitch, seed, shell.data());
+    if (rc != EUP_OK) return rc;
+    const double PI = 3.14159265358979323846;
+    const double Ro = 0.5 * outer_d;            // outer surface of the shell
+    const double period = 2.0 * PI * Ro;        // unrolled circumference at the outer surface
+    const double phase = period * ((double)(splitmix64(seed ^ 0xA5A5A5A5ull) >> 11) * (1.0 / 9007199254740992.0));
+    // porous cap: pores of diameter pore_d on a square grid of pitch 2*pore_d, each
+    // centre jittered by up to pore_d/4 (seeded), kept if the pore fits inside r < Ro - 2
+    std::vector<double> py, pz;
+    const double cp = 2.0 * pore_d;
+    int cnt = 0;
+    for (double a = -Ro; a <= Ro; a += cp)
+        for (double b = -Ro; b <= Ro; b += cp, ++cnt) {
+            const uint64_t h1 = splitmix64(seed + 7919ull * (uint64_t)cnt), h2 = splitmix64(h1);
+            const double ja = a + 0.25 * pore_d * (2.0 * ((double)(h1 >> 11) / 9007199254740992.0) - 1.0);
+            const double jb = b + 0.25 * pore_d * (2.0 * ((double)(h2 >> 11) / 9007199254740992.0) - 1.0);
+            if (std::sqrt(ja * ja + jb * jb) + 0.5 * pore_d < Ro - 2.0) {
+                py.push_back(ja);
+                pz.push_back(jb);
+            }
+        }
+    const double w = smooth_w > 0 ? smooth_w : 0.0;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int32_t k = 1; k <= n; ++k)
+        for (int32_t j = 1; j <= m; ++j) {
+            const double dy = j - yc, dz = k - zc;
+            const double r = std::sqrt(dy * dy + dz * dz);
+            const double s = wrap_pos(Ro * std::atan2(dz, dy) - phase, period);
+            for (int32_t i = 1; i <= l; ++i) {
+                const int64_t o = (int64_t)(i - 1) + (int64_t)l * ((j - 1) + (int64_t)m * (k - 1));
+                double v = shell[(size_t)o] ? 1.0 : 0.0, dv = 0.0;
+                const double u = i - x0;
+                // cap: the last cap_t of the shell's length, r < Ro, minus the pores
+                if (u >= length - cap_t && u <= length && r < Ro) {
+                    bool pore = false;
+                    for (size_t p = 0; p < py.size() && !pore; ++p) {
+                        const double ey = dy - py[p], ez = dz - pz[p];
+                        pore = ey * ey + ez * ez <= 0.25 * pore_d * pore_d;
+                    }
+                    if (!pore) v = 1.0;
+                }
+                // two helical ridges at +-45 degrees on the outer surface: band of width
+                // ridge_t about s = +-u (mod circumference), radially from Ro to Ro + h
+                if (u >= 0 && u <= length && r > Ro - 1.0 && r < Ro + ridge_h + 4.0 * w + 1.0) {
+                    double dperp = 1e30;
+                    for (int sg = -1; sg <= 1; sg += 2) {
+                        double d = wrap_pos(s - sg * u, period);
+                        d = std::fmin(d, period - d) / std::sqrt(2.0);
+                        dperp = std::fmin(dperp, d);
+                    }
+                    if (dperp <= 0.5 * ridge_t && r >= Ro - 0.5) {
+                        double rv, rd;
+                        if (w > 0) {
+                            const double z = (Ro + ridge_h - r) / w;
+                            rv = 0.5 * (1.0 + std::tanh(z));
+                            const double c = std::cosh(z);
+                            rd = 0.5 / (w * c * c);
+                        } else {
+                            rv = (r <= Ro + ridge_h) ? 1.0 : 0.0;
+                            rd = 0.0;
+                        }
+                        if (rv > v) {
+                            v = rv;
+                            dv = rd;
+                        }
+                    }
+                }
+                ns[o] = v;
+                if (dns_dh) dns_dh[o] = dv;
+            }
+        }
+    return EUP_OK;
+}
+
 int eup_geometry_reticular_shell(int32_t l, int32_t m, int32_t n, double x0, double length, double yc, double zc,
                                  double outer_d, double strut_d, double pitch, uint64_t seed, int32_t* obs) {
     if (!obs || l < 1 || m < 1 || n < 1 || !(outer_d > strut_d) || !(strut_d > 0) || !(pitch > 0) || !(length > 0))

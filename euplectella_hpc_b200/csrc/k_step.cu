@@ -39,34 +39,57 @@ struct KOps {
     }
 };
 
-// One thread per node; grid (ceil(l/bx), m, n).
+// Streamed populations of interior node (i, j, k); rowlin = l*((j-1) + m*(k-1))
+// is the linear index of x = 1 on its row (32-bit: one lattice holds fewer than
+// 2^31 nodes).  Every source row pointer depends on the row only, so it is the
+// same for the whole warp and each load is that pointer plus the thread's x.
+// Rows on the y/z boundary planes (warp-uniform) resolve every pull through
+// the halo shell.  Elsewhere all 18 shifted loads are issued unconditionally --
+// for such rows every shifted index stays inside [0, N): D3Q19 has no (1,1,1)
+// diagonals, so x = 0 of row (j', k') is x = l of row (j'-1, k') with j' >= 1,
+// k' >= 2 or j' >= 2 -- and the five x-halo values of the first/last node of a
+// row replace them afterwards.
 template <typename S, typename R>
-__global__ void __launch_bounds__(128) k_stream_collide_scalar(Lat<S, R> src, Lat<S, R> dst, Geo g, Phys<R> ph) {
+__device__ __forceinline__ void gather_node(const Lat<S, R>& src, const Geo& g, int i, int j, int k, int rowlin,
+                                            R (&x)[19]) {
     using K = KOps<S, R>;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    if (i > g.l) return;
-    const int64_t lin = g.lin(i, j, k);
-    R x[19];
-    const bool face = (i == 1) | (i == g.l) | (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-    if (!face) {
+    const int l = g.l, lm = (int)g.lm;
+    const bool face_yz = (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
+    if (!face_yz) {
 #pragma unroll
         for (int q = 0; q < 18; ++q) {
-            const int64_t s = lin - cx_of(q) - (int64_t)cy_of(q) * g.l - (int64_t)cz_of(q) * g.lm;
-            x[q] = K::val(src.pop[q][s], q, src);
+            const S* rp = src.pop[q] + (rowlin - cy_of(q) * l - cz_of(q) * lm);
+            x[q] = K::val(rp[i - 1 - cx_of(q)], q, src);
+        }
+        if (i == 1) {
+#pragma unroll
+            for (int q = 0; q < 18; ++q)
+                if (cx_of(q) == 1)
+                    x[q] = K::from_shell(src.ghost[(int64_t)q * g.G + g.gidx(0, j - cy_of(q), k - cz_of(q))], q, src);
+        }
+        if (i == l) {
+#pragma unroll
+            for (int q = 0; q < 18; ++q)
+                if (cx_of(q) == -1)
+                    x[q] = K::from_shell(src.ghost[(int64_t)q * g.G + g.gidx(l + 1, j - cy_of(q), k - cz_of(q))], q,
+                                         src);
         }
     } else {
 #pragma unroll
         for (int q = 0; q < 18; ++q) x[q] = K::pull(src, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
     }
-    x[18] = K::val(src.pop[18][lin], 18, src);
-    K::collide_node(x, ph, src);
+    x[18] = K::val(src.pop[18][rowlin + i - 1], 18, src);
+}
+
+template <typename S, typename R>
+__device__ __forceinline__ void scatter_node(const Lat<S, R>& dst, const Geo& g, int i, int j, int k, int rowlin,
+                                             const R (&x)[19]) {
+    using K = KOps<S, R>;
     S out[19];
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
         out[q] = K::store(x[q], q, dst);
-        dst.pop[q][lin] = out[q];
+        (dst.pop[q] + rowlin)[i - 1] = out[q];
     }
     if (i == 1 || i == g.l) {
 #pragma unroll
@@ -76,6 +99,20 @@ __global__ void __launch_bounds__(128) k_stream_collide_scalar(Lat<S, R> src, La
             if (i == g.l) dst.xface[xface_idx(g, 1, q, j, k)] = v;
         }
     }
+}
+
+// One thread per node; grid (ceil(l/bx), m, n).
+template <typename S, typename R>
+__global__ void __launch_bounds__(128) k_stream_collide_scalar(Lat<S, R> src, Lat<S, R> dst, Geo g, Phys<R> ph) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > g.l) return;
+    const int rowlin = g.l * ((j - 1) + g.m * (k - 1));
+    R x[19];
+    gather_node(src, g, i, j, k, rowlin, x);
+    KOps<S, R>::collide_node(x, ph, src);
+    scatter_node(dst, g, i, j, k, rowlin, x);
 }
 
 // ---------------------------------------------------------------------------
@@ -220,8 +257,8 @@ bool launch_vec(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const 
 template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph,
                            int variant, cudaStream_t st) {
-    // EUP_STEP_VARIANT bit 0: 16-byte vectors, bit 2: 8-byte vectors (when l allows);
-    // default: one node per thread, the fastest on B200 in every storage format measured.
+    // EUP_STEP_VARIANT bit 0: 16-byte vectors, bit 2: 8-byte vectors (when l allows); default: one
+    // node per thread, the fastest on B200 in every storage format measured.
     constexpr int VW = VecWidth<S>::value;
     if ((variant & 1) && launch_vec<S, R, VW>(src, dst, g, ph, st)) return;
     if ((variant & 4) && launch_vec<S, R, (VW / 2 > 0 ? VW / 2 : 1)>(src, dst, g, ph, st)) return;
@@ -241,3 +278,4 @@ template void launch_stream_collide<__nv_bfloat16, float>(const Lat<__nv_bfloat1
                                                           const Phys<float>&, int, cudaStream_t);
 
 }  // namespace eup
+

@@ -9,6 +9,8 @@ error of the time-averaged C_d over the last quarter of the run, relative
 difference of the FP64 mass sum at the last step, and the device time.
 
     python -m euplectella_hpc_b200.studies [--steps N] [--re 500,1000,2000] [--out FILE]
+
+Adjoint study (config 4): python -m euplectella_hpc_b200.studies --adjoint --steps 4000 [--fd 32]
 """
 from __future__ import annotations
 
@@ -83,12 +85,79 @@ def precision_study(re_list=(500.0, 1000.0, 2000.0), steps=20000):
     return rows
 
 
+def adjoint_study(steps=4000, avg_steps=1000, checkpoints=64, n_fd=32, h=1e-3, fd_seed=2027):
+    """Config-4 adjoint: mean C_d over the last avg_steps of `steps` on the 192x96x96 partial-
+    bounce-back channel.  Returns timings (adjoint with recomputation vs a plain forward run of the
+    same steps), the FP32-vs-FP64 adjoint gradient difference, and central finite differences of
+    FP64 forward runs at n_fd seeded voxels against the FP64 adjoint."""
+    from .workloads import pbb_cylinder_channel
+    out = {"steps": steps, "avg_steps": avg_steps, "checkpoints": checkpoints}
+    grads = {}
+    for name, prec, dt in (("fp32", FP32, np.float32), ("fp64", FP64, np.float64)):
+        wl = pbb_cylinder_channel(steps=steps, avg_steps=avg_steps, precision=prec)
+        a = wl.initial_state(dt)
+        with Solver(wl.cfg) as s:
+            s.set_solid_fraction(wl.ns)
+            s.upload(a)
+            fwd_ms = s.step_profiled(steps)[3]
+        with Solver(wl.cfg) as s:
+            s.set_solid_fraction(wl.ns)
+            s.upload(a)
+            J, g, st = s.adjoint(steps, avg_steps, checkpoints)
+        grads[name] = g
+        out[name] = {"objective": J, "forward_ms": fwd_ms, "adjoint_forward_sweep_ms": st["forward_ms"],
+                     "adjoint_reverse_ms": st["reverse_ms"],
+                     "adjoint_over_forward": (st["forward_ms"] + st["reverse_ms"]) / fwd_ms,
+                     "recomputed_steps": st["recomputed_steps"], "checkpoints_used": st["checkpoints"],
+                     "segment_steps": st["segment_steps"], "stored_state_bytes": st["state_bytes"]}
+    out["grad_fp32_vs_fp64_rel_l2"] = float(np.linalg.norm(grads["fp32"] - grads["fp64"]) /
+                                            np.linalg.norm(grads["fp64"]))
+    # central differences (FP64) at seeded voxels away from the [0,1] bounds
+    wl = pbb_cylinder_channel(steps=steps, avg_steps=avg_steps, precision=FP64)
+    a = wl.initial_state(np.float64)
+    norm = 0.5 * wl.cfg.cd_rho0 * wl.cfg.cd_uref ** 2 * wl.cfg.cd_length * wl.cfg.cd_span
+
+    def objective(ns):
+        with Solver(wl.cfg) as s:
+            s.set_solid_fraction(ns)
+            s.upload(a)
+            s.step(steps)
+            return s.force_series(steps - avg_steps + 1, avg_steps)[:, 0].mean() / norm
+
+    rng = np.random.default_rng(fd_seed)
+    cand = np.argwhere((wl.ns > h) & (wl.ns < 1 - h))
+    pick = cand[rng.choice(len(cand), n_fd, replace=False)]
+    rows = []
+    for k, j, i in pick:
+        p, m = wl.ns.copy(), wl.ns.copy()
+        p[k, j, i] += h
+        m[k, j, i] -= h
+        fd = (objective(p) - objective(m)) / (2 * h)
+        ad = float(grads["fp64"][k, j, i])
+        rows.append({"voxel": [int(i) + 1, int(j) + 1, int(k) + 1], "ns": float(wl.ns[k, j, i]), "fd": fd,
+                     "adjoint": ad, "rel_err": abs(ad - fd) / max(abs(fd), 1e-300)})
+    out["fd"] = rows
+    errs = np.array([r["rel_err"] for r in rows])
+    out["fd_rel_err_max"] = float(errs.max())
+    out["fd_rel_err_median"] = float(np.median(errs))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--re", default="500,1000,2000")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--adjoint", action="store_true", help="run the config-4 adjoint study instead")
+    ap.add_argument("--fd", type=int, default=32)
     args = ap.parse_args()
+    if args.adjoint:
+        res = adjoint_study(steps=args.steps, n_fd=args.fd)
+        print(json.dumps(res))
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(res, f, indent=1)
+        return
     rows = precision_study(tuple(float(x) for x in args.re.split(",")), args.steps)
     for r in rows:
         print(json.dumps(r))

@@ -77,3 +77,46 @@ def reticular_shell_channel(lx=768, ly=384, lz=384, outer_d=96.0, length=256.0, 
     rin = 0.5 * outer_d - strut_d
     cavity = ((j - yc) ** 2 + (k - zc) ** 2 < rin * rin) & (i >= x0) & (i <= x0 + length)
     return Workload("reticular_shell_768x384x384_re2000", cfg, obs, steps, seed, probes, cavity)
+
+
+def _gauss(seed: int, n: int) -> np.ndarray:
+    """Seeded standard normals: Box-Muller on splitmix64(seed + 2t), splitmix64(seed + 2t + 1)."""
+    t = np.arange(n, dtype=np.uint64)
+    def mix(x):
+        with np.errstate(over="ignore"):
+            z = x + np.uint64(0x9E3779B97F4A7C15)
+            z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+            z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+            return z ^ (z >> np.uint64(31))
+    s = np.uint64(seed)
+    with np.errstate(over="ignore"):
+        u1 = ((mix(s + np.uint64(2) * t) >> np.uint64(11)).astype(np.float64) + 0.5) / 9007199254740992.0
+        u2 = ((mix(s + np.uint64(2) * t + np.uint64(1)) >> np.uint64(11)).astype(np.float64)) / 9007199254740992.0
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * math.pi * u2)
+
+
+def solid_fraction_cylinder(lx, ly, lz, d, xc, yc, sigma, seed, width=1.0, band=1e-3) -> np.ndarray:
+    """n_s = smoothed cylinder (axis z): 0.5 (1 - tanh((r - d/2)/width)), plus seeded
+    N(0, sigma) noise on the voxels of the body, i.e. where the smoothed field exceeds
+    `band` (noise on every voxel would turn the whole channel into a porous medium whose
+    drag swamps the cylinder's), clamped to [0, 1]; shape (lz, ly, lx)."""
+    k, j, i = np.meshgrid(np.arange(1, lz + 1), np.arange(1, ly + 1), np.arange(1, lx + 1), indexing="ij")
+    r = np.sqrt((i - xc) ** 2 + (j - yc) ** 2)
+    ns = 0.5 * (1.0 - np.tanh((r - 0.5 * d) / width))
+    noise = sigma * _gauss(seed, lx * ly * lz).reshape(lz, ly, lx)
+    ns = np.where(ns > band, ns + noise, ns)
+    return np.clip(ns, 0.0, 1.0)
+
+
+def pbb_cylinder_channel(lx=192, ly=96, lz=96, d=24.0, re=100.0, steps=4000, avg_steps=1000, sigma=0.05,
+                         seed=4242, precision=FP32) -> Workload:
+    """Adjoint workload: 192x96x96 channel (inlet 0.05, outflow, free-slip y, periodic z) holding a
+    partial-bounce-back solid fraction (smoothed D=24 cylinder + seeded Gaussian noise, sigma 0.05);
+    Re 100; objective mean C_d over the last 1000 of 4000 steps."""
+    nu = svisc_for(re, U_IN, d)
+    cfg = Config(lx, ly, lz, bc=(OUTFLOW, INFLOW, FREESLIP, FREESLIP, PERIODIC, PERIODIC), svisc=nu,
+                 u_inflow=U_IN, precision=precision, cd_rho0=1.0, cd_uref=U_IN, cd_length=d, cd_span=float(lz))
+    wl = Workload("pbb_cylinder_192x96x96_re100", cfg, np.zeros((lz, ly, lx), np.int32), steps, seed)
+    wl.ns = solid_fraction_cylinder(lx, ly, lz, d, lx / 4.0, (ly + 1) / 2.0, sigma, seed)
+    wl.avg_steps = avg_steps
+    return wl

@@ -213,6 +213,32 @@ int eup_get_boundary_solid(eup_handle* h, int64_t* list, int64_t cap, int64_t* c
 int eup_mem_force_noalloc(int32_t l, int32_t m, int32_t n, const int32_t bc[6], const void* const pops[19],
                           int32_t elem_bytes, const int32_t* obs, double* force, void* stream);
 
+/* ---- partial bounce-back and its adjoint ----------------------------------- */
+/* No counterpart in the reference (its solids are all-or-nothing voxels).  A
+ * solid fraction n_s(1:l,1:m,1:n) in [0,1] switches the handle to the
+ * partial-bounce-back collision of Walsh, Burwinkle & Saar (2009),
+ * f*_i = (1-n_s) BGK_i(f) + n_s f_opp(i), whose drag is sum 2 n_s j_x; the force
+ * of every step is recorded like eup_get_forces'.  FP32 or FP64 storage, no
+ * obstacles.  NULL switches the field off. */
+int eup_set_solid_fraction(eup_handle* h, const double* ns);
+
+typedef struct eup_adjoint_config {
+    int32_t nsteps;       /* forward steps T from the current state */
+    int32_t avg_steps;    /* objective: mean C_d over the last avg_steps steps */
+    int32_t checkpoints;  /* checkpoint slots; 0 selects 64 */
+    int32_t reserved;
+} eup_adjoint_config;
+
+/* Runs T partial-bounce-back steps from the current state and the discrete
+ * adjoint back to it: *objective = mean C_d over the last avg_steps steps,
+ * grad_ns[l*m*n] = d objective / d n_s per voxel (FP64, Fortran order).
+ * Checkpoints every K = ceil(T/checkpoints) steps and recomputes each segment
+ * once.  Leaves the handle at step itime + T.  stats (may be NULL): forward ms,
+ * reverse ms (recomputation + adjoint), recomputed steps, checkpoints, K,
+ * device bytes of stored states, T, avg_steps. */
+int eup_adjoint_run(eup_handle* h, const eup_adjoint_config* cfg, double* objective, double* grad_ns,
+                    double stats[8]);
+
 /* ---- host utilities (no GPU) ---------------------------------------------- */
 
 /* Reads obs.RRRR.TTTTTTTT.bin (CODE/SRC/build.obs.F90:147-177): Fortran
@@ -257,6 +283,19 @@ int eup_geometry_cylinder_z(int32_t l, int32_t m, int32_t n, double xc, double y
 int eup_geometry_reticular_shell(int32_t l, int32_t m, int32_t n, double x0, double length,
                                  double yc, double zc, double outer_d, double strut_d,
                                  double pitch, uint64_t seed, int32_t* obs);
+
+/* Ridged lattice shell: the reticular shell above plus two counter-rotating
+ * helical ridges at +-45 degrees (height ridge_h, width ridge_t) on its outer
+ * surface and a porous cap (thickness cap_t, seeded circular pores of
+ * diameter pore_d) closing its downstream end, as a solid fraction ns in
+ * [0,1] (double, Fortran order).  With smooth_w > 0 the ridges' radial extent
+ * is smoothed over smooth_w and dns_dh (may be NULL) receives d ns / d ridge_h,
+ * the chain from a ridge-height parameter to the voxel field; with
+ * smooth_w = 0 the field is 0/1 (ns >= 0.5 gives an obstacle mask). */
+int eup_geometry_ridged_shell(int32_t l, int32_t m, int32_t n, double x0, double length, double yc, double zc,
+                              double outer_d, double strut_d, double pitch, double ridge_h, double ridge_t,
+                              double cap_t, double pore_d, double smooth_w, uint64_t seed, double* ns,
+                              double* dns_dh);
 
 #ifdef __cplusplus
 }

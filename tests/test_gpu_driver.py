@@ -1,0 +1,53 @@
+"""The eup_bgk3d program: the reference's serial program over the C ABI, fed
+the reference's own input files (bgk.input namelist, obs.0000.00000000.bin,
+restore.00.00.00.bin).  Its save files must equal the oracle's state bit for
+bit and its drag lines the oracle's momentum exchange."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+DRIVER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "euplectella_hpc_b200", "_lib",
+                      "eup_bgk3d")
+
+
+def test_driver_runs_reference_inputs(eup, orc, require_gpu, tmp_path):
+    l, m, n = 40, 24, 12
+    obs = eup.geometry_cylinder_z(l, m, n, 12, 12.5, 3.5)
+    eup.write_obs_file(tmp_path / "obs.0000.00000000.bin", obs)
+    a = eup.init_equilibrium(l, m, n, 0.05, 1e-3, 17, np.float32)
+    eup.write_raw_state(tmp_path / "restore.00.00.00.bin", a, 100)
+    (tmp_path / "bgk.input").write_text(
+        "&parameters\n lx = 40\n ly = 24\n lz = 12\n proc_x = 1\n proc_y = 1\n proc_z = 1\n"
+        " svisc=0.01,0.005\n u0=0.05\n itfin=140\n ivtim=1000\n isignal=20\n itsave=20\n icheck=10\n"
+        " tstep=10\n irestart=1\n flag1=1\n flag2=2\n flag3=0\n init_v=0        /\n")
+    r = subprocess.run([DRIVER, "--preset", "cylinder_inf", "--drag-length", "7"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    # oracle with the CYLINDER_INF flags (in/out x, periodic y and z), u_inflow = u0
+    p = orc.params(l, m, n, [5, 4, 0, 0, 0, 0], svisc=0.01, u_inflow=0.05)
+    ref = a.copy()
+    forces = {}
+    for t in range(101, 141):
+        orc.run(p, ref, obs, 1)
+        if t % 10 == 0:
+            forces[t] = orc.mem_force(p, ref, obs)
+        if t % 20 == 0:
+            got, it = eup.read_raw_state(tmp_path / f"save.00.00.00.{t:08d}.bin", l, m, n)
+            assert it == t
+            keep = np.ones(got.shape[1:], bool)
+            keep[1:-1, 1:-1, 1:-1] = obs == 0
+            for q in range(19):
+                assert np.array_equal(got[q][keep], ref[q][keep]), (t, q)
+    lines = (tmp_path / "drag_mem.0000.dat").read_text().split("\n")
+    rows = [list(map(float, ln.split())) for ln in lines if ln.strip()]
+    assert [int(r_[0]) for r_ in rows] == [110, 120, 130, 140]
+    for row in rows:
+        np.testing.assert_allclose(row[1:4], forces[int(row[0])], rtol=1e-12, atol=1e-14)
+        assert abs(row[4] - row[1] / (0.5 * 0.05 ** 2 * 7 * n)) <= 1e-12 * abs(row[4])
+    probe = (tmp_path / "probe_g.0000.dat").read_text().split("\n")[0]
+    assert probe.startswith("     110") and "E" in probe
+    assert "Mlups" in (tmp_path / "bgk.perf").read_text()

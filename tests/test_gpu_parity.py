@@ -44,6 +44,8 @@ CASES = [
     ("obstacle_on_faces", (24, 12, 10), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _wall_touch),
     ("noslip_y_periodic_z_inflow", (20, 10, 9), (5, 4, 1, 1, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
     ("freeslip_z_periodic_y", (20, 10, 9), (5, 4, 0, 0, 3, 3), 0.01, 0.0, 0.05, 0.0, _cyl),
+    # l odd: rows start at every alignment
+    ("odd_length_inout", (21, 11, 9), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
     # l a multiple of 128: with EUP_STEP_VARIANT the vectorised kernels can run (see below)
     ("vec_cylinder", (128, 24, 10), (5, 4, 3, 3, 0, 0), 0.01, 0.0, 0.05, 0.0, _cyl),
     ("vec_freeslip_all", (128, 18, 14), (5, 4, 3, 3, 3, 3), 0.0024, 0.0, 0.05, 0.0, _block),

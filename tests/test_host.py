@@ -106,3 +106,32 @@ def test_geometry_reticular_shell(eup):
     rr = np.sqrt((jj - 36.5) ** 2 + (kk - 36.5) ** 2)
     ann = ((rr >= 20.5) & (rr <= 23.5)).sum() * 64
     assert 0.2 < obs[:, :, 40:104].sum() / ann < 0.9
+
+
+def test_geometry_ridged_shell(eup):
+    l, m, n = 160, 72, 72
+    args = (l, m, n, 40, 64, 36.5, 36.5, 48, 4, 16)
+    shell = eup.geometry_reticular_shell(*args, 7)
+    hard = eup.geometry_ridged_shell(*args, 4.0, 3.0, 4.0, 5.0, 0.0, 7)
+    assert set(np.unique(hard)) <= {0.0, 1.0}
+    # the shell is kept; ridges and cap only add solid
+    assert np.all(hard[shell == 1] == 1.0)
+    extra = (hard == 1.0) & (shell == 0)
+    k, j, i = np.nonzero(extra)
+    r = np.sqrt((j + 1 - 36.5) ** 2 + (k + 1 - 36.5) ** 2)
+    ridge = r >= 23.5                                            # ridges start half a voxel inside Ro
+    assert ridge.any() and r[ridge].max() <= 24 + 4 + 1e-9      # and stand at most ridge_h proud
+    cap = ~ridge
+    assert cap.any() and (i[cap] + 1).min() >= 40 + 64 - 4 - 1   # the cap closes the last cap_t of the body
+    # the porous cap has open pores
+    capsl = hard[:, :, 104 - 3:104]
+    jj, kk = np.meshgrid(np.arange(1, m + 1), np.arange(1, n + 1))
+    inside = np.sqrt((jj - 36.5) ** 2 + (kk - 36.5) ** 2) < 20
+    assert 0.1 < 1.0 - capsl[inside].mean() < 0.9
+    # smooth field: d ns / d h matches a central difference
+    ns, d = eup.geometry_ridged_shell(*args, 4.0, 3.0, 4.0, 5.0, 1.0, 7, with_derivative=True)
+    assert ns.min() >= 0.0 and ns.max() <= 1.0 and (d > 0).any()
+    hp = eup.geometry_ridged_shell(*args, 4.0 + 1e-5, 3.0, 4.0, 5.0, 1.0, 7)
+    hm = eup.geometry_ridged_shell(*args, 4.0 - 1e-5, 3.0, 4.0, 5.0, 1.0, 7)
+    fd = (hp - hm) / 2e-5
+    assert np.abs(fd - d).max() < 1e-5 * max(1.0, np.abs(d).max())
