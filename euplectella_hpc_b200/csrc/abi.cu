@@ -80,11 +80,23 @@ bool face_flag_ok(int face, int f) {
     }
 }
 
+// Population q of a lattice buffer: Nq elements per population, the node
+// values starting kPopPad elements in.  16-bit storage shifts population q by
+// cx_q elements, so that the pull a_q(x - c_q) of an even x reads an aligned
+// pair in every population (see the two-node stream-collide kernel); the
+// node-indexed view every kernel uses is unchanged.
+constexpr int64_t kPopPad = 64;
+
+template <typename S>
+S* pop_ptr(const eup_handle* h, void* base, int q) {
+    const int64_t shift = (DevStore<S>::value && q < 18) ? cx_of(q) : 0;
+    return static_cast<S*>(base) + (q * h->Nq + kPopPad + shift);
+}
+
 template <typename S, typename R>
 Lat<S, R> make_lat(const eup_handle* h, int which) {
     Lat<S, R> L;
-    char* base = static_cast<char*>(h->lat[which]);
-    for (int q = 0; q < Q; ++q) L.pop[q] = reinterpret_cast<S*>(base + (size_t)q * h->Nq * sizeof(S));
+    for (int q = 0; q < Q; ++q) L.pop[q] = pop_ptr<S>(h, h->lat[which], q);
     L.ghost = static_cast<R*>(h->ghost);
     L.xface = static_cast<R*>(h->xface);
     L.scale = (R)h->scale;
@@ -333,7 +345,7 @@ int eup_create(const eup_config* cfg, eup_handle** out) {
     h->rbytes = (h->prec == EUP_FP64) ? 8 : 4;
     h->scale = (h->prec == EUP_FP16_DEV || h->prec == EUP_BF16_DEV) ? (cfg->dev_scale > 0 ? cfg->dev_scale : 4096.0) : 1.0;
     h->cap = cfg->series_capacity > 0 ? cfg->series_capacity : (int64_t)1 << 20;
-    h->Nq = (N + 127) / 128 * 128;
+    h->Nq = (N + 2 * kPopPad + 127) / 128 * 128;
     if (const char* v = std::getenv("EUP_STEP_VARIANT")) h->variant = std::atoi(v);
 
     auto cleanup_fail = [&](int code) {
@@ -680,11 +692,11 @@ cudaError_t upload_vec(DevBuf<T>& b, const std::vector<T>& v) {
     return e;
 }
 
-// Lattice view of an arbitrary state buffer (19 arrays of Nq elements).
+// Lattice view of an arbitrary state buffer laid out like the handle's lattices.
 template <typename R>
 Lat<R, R> lat_at(const eup_handle* h, R* base, R* shell = nullptr) {
     Lat<R, R> L = make_lat<R, R>(h, 0);
-    for (int q = 0; q < Q; ++q) L.pop[q] = base + (size_t)q * h->Nq;
+    for (int q = 0; q < Q; ++q) L.pop[q] = pop_ptr<R>(h, base, q);
     if (shell) L.ghost = shell;
     return L;
 }

@@ -116,6 +116,140 @@ __global__ void __launch_bounds__(128) k_stream_collide_scalar(Lat<S, R> src, La
 }
 
 // ---------------------------------------------------------------------------
+// Pair kernel (FP32 arithmetic, l even): one thread streams and collides the
+// two x-adjacent nodes (i, i+1), i odd.  The collision runs once on F2 values
+// -- the packed FP32 instructions of sm_100 (fma .f32x2), rounded per lane
+// exactly as the scalar code -- so the FP32 instruction count per node halves
+// and the results equal the one-node kernel's bit for bit.  FP32 storage: the
+// pulls with cx = 0 and every store move both nodes as one aligned 8-byte
+// access, pulls with cx = +-1 are two scalar loads.  16-bit storage shifts
+// population q by cx_q elements in memory, so all 19 pulls are aligned 4-byte
+// loads (two nodes in one register: twice the bytes in flight per register);
+// the stores of the ten populations with cx = +-1 are then two scalar stores.
+// grid (ceil(l/2 / 128), m, n).
+// ---------------------------------------------------------------------------
+template <typename S> struct Vec2;
+template <> struct Vec2<float> {
+    using T = float2;
+    static __device__ __forceinline__ float2 unpack(float2 v) { return v; }
+    static __device__ __forceinline__ float2 pack(float2 v) { return v; }
+};
+template <> struct Vec2<__half> {
+    using T = __half2;
+    static __device__ __forceinline__ float2 unpack(__half2 v) { return __half22float2(v); }
+    static __device__ __forceinline__ __half2 pack(float2 v) { return __float22half2_rn(v); }
+};
+template <> struct Vec2<__nv_bfloat16> {
+    using T = __nv_bfloat162;
+    static __device__ __forceinline__ float2 unpack(__nv_bfloat162 v) { return __bfloat1622float2(v); }
+    static __device__ __forceinline__ __nv_bfloat162 pack(float2 v) { return __float22bfloat162_rn(v); }
+};
+
+template <typename S, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float> src, Lat<S, float> dst, Geo g,
+                                                                   Phys<float> ph) {
+    using K = KOps<S, float>;
+    using V2 = Vec2<S>;
+    using T2 = typename V2::T;
+    constexpr bool dev = DevStore<S>::value;
+    const int i = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x) + 1;  // first node; i + 1 <= l as l is even
+    const int j = blockIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > g.l) return;
+    const int l = g.l, lm = (int)g.lm;
+    const int rowlin = l * ((j - 1) + g.m * (k - 1));
+    const bool face_yz = (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
+    if (face_yz) {  // warp-uniform: node by node through the halo shell
+#pragma unroll 1
+        for (int e = 0; e < 2; ++e) {
+            float x[19];
+            gather_node(src, g, i + e, j, k, rowlin, x);
+            K::collide_node(x, ph, src);
+            scatter_node(dst, g, i + e, j, k, rowlin, x);
+        }
+        return;
+    }
+    F2 x[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        const int cx = (q == 18) ? 0 : cx_of(q), cy = (q == 18) ? 0 : cy_of(q), cz = (q == 18) ? 0 : cz_of(q);
+        const S* rp = src.pop[q] + (rowlin - cy * l - cz * lm);
+        if (dev) {  // aligned in the shifted layout whatever cx is
+            x[q] = F2(V2::unpack(*reinterpret_cast<const T2*>(rp + (i - 1 - cx))));
+        } else if (cx == 0) {
+            const float2 v = V2::unpack(*reinterpret_cast<const T2*>(rp + (i - 1)));
+            x[q] = F2(K::val(v.x, q, src), K::val(v.y, q, src));
+        } else {
+            // both shifted loads are in bounds (interior rows; see gather_node)
+            x[q] = F2(K::val(rp[i - 1 - cx], q, src), K::val(rp[i - cx], q, src));
+        }
+    }
+    if (i == 1) {
+#pragma unroll
+        for (int q = 0; q < 18; ++q)
+            if (cx_of(q) == 1)
+                x[q].v.x = K::from_shell(src.ghost[(int64_t)q * g.G + g.gidx(0, j - cy_of(q), k - cz_of(q))], q, src);
+    }
+    if (i + 1 == l) {
+#pragma unroll
+        for (int q = 0; q < 18; ++q)
+            if (cx_of(q) == -1)
+                x[q].v.y =
+                    K::from_shell(src.ghost[(int64_t)q * g.G + g.gidx(l + 1, j - cy_of(q), k - cz_of(q))], q, src);
+    }
+    if constexpr (dev) collide_dev<F2>(x, ph.omega, ph.omega1, ph.fgrad, src.scale, src.inv_scale);
+    else collide<F2>(x, F2(ph.omega), F2(ph.omega1), F2(ph.fgrad));
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        const T2 o = V2::pack(x[q].v);
+        S* op = dst.pop[q] + rowlin + (i - 1);
+        if (!dev || q == 18 || cx_of(q) == 0) {
+            *reinterpret_cast<T2*>(op) = o;
+        } else {  // odd address in the shifted layout
+            op[0] = reinterpret_cast<const S*>(&o)[0];
+            op[1] = reinterpret_cast<const S*>(&o)[1];
+        }
+        if (q < 18 && (i == 1 || i + 1 == l)) {  // x-face copy: the value a later lattice load returns
+            const S* os = reinterpret_cast<const S*>(&o);
+            if (i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = Store<S, float>::load(os[0], q, dst.inv_scale);
+            if (i + 1 == l) dst.xface[xface_idx(g, 1, q, j, k)] = Store<S, float>::load(os[1], q, dst.inv_scale);
+        }
+    }
+}
+
+template <typename S, typename R>
+bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph, int occ,
+                 cudaStream_t st) {
+    if constexpr (sizeof(R) != 4) {
+        return false;
+    } else {
+        if (g.l % 2 != 0) return false;
+        // pair accesses: FP32 at the node's own address, 16-bit storage at the address
+        // shifted back by cx_q (and its stores of cx = 0 populations)
+        constexpr bool dev = DevStore<S>::value;
+        for (int q = 0; q < Q; ++q) {
+            const int cx = (q == 18) ? 0 : cx_of(q);
+            const S* s0 = dev ? src.pop[q] - cx : src.pop[q];
+            if (reinterpret_cast<uintptr_t>(s0) % (2 * sizeof(S)) != 0) return false;
+            if ((!dev || cx == 0) && reinterpret_cast<uintptr_t>(dst.pop[q]) % (2 * sizeof(S)) != 0) return false;
+        }
+        const int bx = 128;
+        dim3 grid((g.l / 2 + bx - 1) / bx, g.m, g.n);
+        // resident blocks of 128 threads per SM the register budget is sized for: by default
+        // 6 (80 registers) for FP32 storage, 8 (64) for 16-bit storage, whose loads need fewer
+        const int minb = occ > 0 ? occ + 3 : (sizeof(S) == 4 ? 6 : 8);
+        switch (minb) {
+            case 4: k_stream_collide_pair<S, 4><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
+            case 5: k_stream_collide_pair<S, 5><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
+            case 6: k_stream_collide_pair<S, 6><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
+            case 7: k_stream_collide_pair<S, 7><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
+            default: k_stream_collide_pair<S, 8><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
+        }
+        return true;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Vectorised variant: each thread owns VW consecutive x-nodes of one (j,k)
 // row, so every population moves as one 16-byte (or 8-byte) load and store.
 // Pulls along x (cx = +-1) need one element of the neighbouring thread's
@@ -241,6 +375,10 @@ template <typename S> struct VecWidth { static constexpr int value = 16 / sizeof
 template <typename S, typename R, int VW>
 bool launch_vec(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph, cudaStream_t st) {
     if (g.l % (32 * VW) != 0) return false;
+    for (int q = 0; q < Q; ++q)  // every row must start on a vector boundary
+        if (reinterpret_cast<uintptr_t>(src.pop[q]) % (sizeof(S) * VW) != 0 ||
+            reinterpret_cast<uintptr_t>(dst.pop[q]) % (sizeof(S) * VW) != 0)
+            return false;
     const int nvec = g.l / VW;
     int tx = nvec;
     while (tx > 256) tx /= 2;  // nvec is a multiple of 32; keep tx a multiple of 32 dividing nvec
@@ -257,11 +395,13 @@ bool launch_vec(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const 
 template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph,
                            int variant, cudaStream_t st) {
-    // EUP_STEP_VARIANT bit 0: 16-byte vectors, bit 2: 8-byte vectors (when l allows); default: one
-    // node per thread, the fastest on B200 in every storage format measured.
+    // EUP_STEP_VARIANT bit 0: 16-byte vectors, bit 2: 8-byte vectors (when l allows), bit 3: one
+    // node per thread, bits 4-6: occupancy target of the two-node kernel (n + 3 blocks per SM);
+    // default: two nodes per thread (FP32 arithmetic, l even).
     constexpr int VW = VecWidth<S>::value;
     if ((variant & 1) && launch_vec<S, R, VW>(src, dst, g, ph, st)) return;
     if ((variant & 4) && launch_vec<S, R, (VW / 2 > 0 ? VW / 2 : 1)>(src, dst, g, ph, st)) return;
+    if (!(variant & 8) && launch_pair<S, R>(src, dst, g, ph, (variant >> 4) & 7, st)) return;
     const int bx = 128;
     dim3 grid((g.l + bx - 1) / bx, g.m, g.n);
     k_stream_collide_scalar<S, R><<<grid, bx, 0, st>>>(src, dst, g, ph);

@@ -54,6 +54,49 @@ template <> struct Const<double> {
     static __device__ __forceinline__ double p2() { return 1.0 / 36.0; }
 };
 
+// Two FP32 lanes operated on together with the packed FP32 instructions of
+// sm_100 (add/mul/fma .f32x2).  Each lane is rounded exactly as the scalar
+// operation, so code written once for R = float and R = F2 gives identical
+// bits per lane; F2 lets one thread collide two nodes with half the FP32
+// instructions.  Division has no packed form and runs per lane.
+struct F2 {
+    float2 v;
+    F2() = default;
+    __device__ __forceinline__ F2(float s) : v(make_float2(s, s)) {}
+    __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
+    __device__ __forceinline__ explicit F2(float2 w) : v(w) {}
+};
+// Every packed operation is issued as a packed fused multiply-add: a product is
+// fma(a, b, z) and a sum fma(a, u, b) with u = 1 and z = -0 read from constant
+// memory, each exactly the correctly rounded product or sum.  The code
+// generator fuses a packed multiply feeding a packed add into one fma (even
+// with an explicit .rn rounding modifier), which would skip a rounding of the
+// scalar reference-order arithmetic; with u and z unknown when the kernel is
+// compiled no operation can be rewritten as a plain multiply or add, and an
+// fma is never fused with another.
+__constant__ float2 kF2Unit = {1.0f, -0.0f};
+
+__device__ __forceinline__ F2 fma_rn(F2 a, F2 b, F2 c) {
+    F2 r;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n}"
+        : "=f"(r.v.x), "=f"(r.v.y)
+        : "f"(a.v.x), "f"(a.v.y), "f"(b.v.x), "f"(b.v.y), "f"(c.v.x), "f"(c.v.y));
+    return r;
+}
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return fma_rn(a, F2(kF2Unit.x), b); }
+__device__ __forceinline__ F2 operator-(F2 a) { return F2(-a.v.x, -a.v.y); }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return fma_rn(b, F2(-kF2Unit.x), a); }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return fma_rn(a, b, F2(kF2Unit.y)); }
+__device__ __forceinline__ F2 operator/(F2 a, F2 b) { return F2(a.v.x / b.v.x, a.v.y / b.v.y); }
+
+template <> struct Const<F2> {
+    static __device__ __forceinline__ F2 p0() { return F2(Const<float>::p0()); }
+    static __device__ __forceinline__ F2 p1() { return F2(Const<float>::p1()); }
+    static __device__ __forceinline__ F2 p2() { return F2(Const<float>::p2()); }
+};
+
 template <typename R>
 __device__ __forceinline__ R weight(int q) {
     const int c = wclass_of(q);
@@ -285,41 +328,43 @@ template <> struct DevStore<__nv_bfloat16> {
 };
 
 // One opposite pair (qp, qm) with c_qp . u = v, c_qm = -c_qp; fx = +-1/0 the
-// x component of c_qp (body force along x).
-__device__ __forceinline__ void dev_pair(float* D, int qp, int qm, float v, float w, float rm1, float rho, float t,
-                                         float oS, float omega1, float fS, float fx) {
-    const float a = __fmaf_rn(rho, __fmaf_rn(4.5f * v, v, -t), rm1);   // (rho-1) + rho (4.5 v^2 - 1.5 u^2)
-    const float b = 3.0f * rho * v;
-    const float ow = oS * w;
-    D[qp] = __fmaf_rn(omega1, D[qp], __fmaf_rn(ow, a + b, fx * fS));
-    D[qm] = __fmaf_rn(omega1, D[qm], __fmaf_rn(ow, a - b, -fx * fS));
+// x component of c_qp (body force along x).  V = float, or F2 for two nodes.
+template <typename V>
+__device__ __forceinline__ void dev_pair(V* D, int qp, int qm, V v, float w, V rm1, V rho, V t, V oS, float omega1,
+                                         V fS, float fx) {
+    const V a = fma_rn(rho, fma_rn(V(4.5f) * v, v, -t), rm1);   // (rho-1) + rho (4.5 v^2 - 1.5 u^2)
+    const V b = V(3.0f) * rho * v;
+    const V ow = oS * V(w);
+    D[qp] = fma_rn(V(omega1), D[qp], fma_rn(ow, a + b, V(fx) * fS));
+    D[qm] = fma_rn(V(omega1), D[qm], fma_rn(ow, a - b, V(-fx) * fS));
 }
 
-__device__ __forceinline__ void collide_dev(float* D, float omega, float omega1, float fgrad, float S, float invS) {
-    float s = D[0];
+template <typename V>
+__device__ __forceinline__ void collide_dev(V* D, float omega, float omega1, float fgrad, float S, float invS) {
+    V s = D[0];
 #pragma unroll
-    for (int q = 1; q < 19; ++q) s += D[q];
-    const float rm1 = s * invS;
-    const float rho = 1.0f + rm1;
-    const float jx = (D[0] + D[1] + D[2] + D[3] + D[4]) - (D[9] + D[10] + D[11] + D[12] + D[13]);
-    const float jy = (D[2] + D[6] + D[7] + D[8] + D[11]) - (D[0] + D[9] + D[15] + D[16] + D[17]);
-    const float jz = (D[3] + D[5] + D[6] + D[12] + D[17]) - (D[1] + D[8] + D[10] + D[14] + D[15]);
-    const float ri = invS / rho;
-    const float ux = jx * ri, uy = jy * ri, uz = jz * ri;
-    const float t = 1.5f * __fmaf_rn(ux, ux, __fmaf_rn(uy, uy, uz * uz));
-    const float oS = omega * S;
-    const float fS = S * fgrad * rho;
+    for (int q = 1; q < 19; ++q) s = s + D[q];
+    const V rm1 = s * V(invS);
+    const V rho = V(1.0f) + rm1;
+    const V jx = (D[0] + D[1] + D[2] + D[3] + D[4]) - (D[9] + D[10] + D[11] + D[12] + D[13]);
+    const V jy = (D[2] + D[6] + D[7] + D[8] + D[11]) - (D[0] + D[9] + D[15] + D[16] + D[17]);
+    const V jz = (D[3] + D[5] + D[6] + D[12] + D[17]) - (D[1] + D[8] + D[10] + D[14] + D[15]);
+    const V ri = V(invS) / rho;
+    const V ux = jx * ri, uy = jy * ri, uz = jz * ri;
+    const V t = V(1.5f) * fma_rn(ux, ux, fma_rn(uy, uy, uz * uz));
+    const V oS = V(omega * S);
+    const V fS = V(S * fgrad) * rho;
     const float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
-    dev_pair(D, 4, 13, ux, w1, rm1, rho, t, oS, omega1, fS, 1.f);        // a05 / a14
-    dev_pair(D, 5, 14, uz, w1, rm1, rho, t, oS, omega1, fS, 0.f);        // a06 / a15
-    dev_pair(D, 7, 16, uy, w1, rm1, rho, t, oS, omega1, fS, 0.f);        // a08 / a17
-    dev_pair(D, 0, 11, ux - uy, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a01 / a12
-    dev_pair(D, 1, 12, ux - uz, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a02 / a13
-    dev_pair(D, 2, 9, ux + uy, w2, rm1, rho, t, oS, omega1, fS, 1.f);    // a03 / a10
-    dev_pair(D, 3, 10, ux + uz, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a04 / a11
-    dev_pair(D, 6, 15, uy + uz, w2, rm1, rho, t, oS, omega1, fS, 0.f);   // a07 / a16
-    dev_pair(D, 8, 17, uy - uz, w2, rm1, rho, t, oS, omega1, fS, 0.f);   // a09 / a18
-    D[18] = __fmaf_rn(omega1, D[18], oS * w0 * __fmaf_rn(-rho, t, rm1));  // a19
+    dev_pair<V>(D, 4, 13, ux, w1, rm1, rho, t, oS, omega1, fS, 1.f);        // a05 / a14
+    dev_pair<V>(D, 5, 14, uz, w1, rm1, rho, t, oS, omega1, fS, 0.f);        // a06 / a15
+    dev_pair<V>(D, 7, 16, uy, w1, rm1, rho, t, oS, omega1, fS, 0.f);        // a08 / a17
+    dev_pair<V>(D, 0, 11, ux - uy, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a01 / a12
+    dev_pair<V>(D, 1, 12, ux - uz, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a02 / a13
+    dev_pair<V>(D, 2, 9, ux + uy, w2, rm1, rho, t, oS, omega1, fS, 1.f);    // a03 / a10
+    dev_pair<V>(D, 3, 10, ux + uz, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a04 / a11
+    dev_pair<V>(D, 6, 15, uy + uz, w2, rm1, rho, t, oS, omega1, fS, 0.f);   // a07 / a16
+    dev_pair<V>(D, 8, 17, uy - uz, w2, rm1, rho, t, oS, omega1, fS, 0.f);   // a09 / a18
+    D[18] = fma_rn(V(omega1), D[18], oS * V(w0) * fma_rn(-rho, t, rm1));   // a19
 }
 
 // Physical constants of one run, rounded to the arithmetic type the way
