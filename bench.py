@@ -253,7 +253,8 @@ def run_eup(args):
     peak, peak_src = measured_peak()
     tpn = traffic_per_node(args.precision)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": (tpn * wl.nodes if tpn is not None else None), "kernel": "k_stream_collide",
+            "traffic": (tpn * wl.nodes if tpn is not None else None),
+            "kernel": "k_stream_collide_scalar" if args.precision == "fp64" else "k_stream_collide_pair",
             "kernel_ms": k_ms, "peak_source": peak_src,
             "phase_ms_per_step": {"bounce_drag": ms[0] / args.steps, "halo_planes": ms[1] / args.steps,
                                   "stream_collide": k_ms, "step_without_graphs": ms[3] / args.steps}}

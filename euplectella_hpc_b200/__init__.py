@@ -38,7 +38,7 @@ EXPORTED = [
     "eup_get_probes", "eup_get_links", "eup_get_boundary_solid", "eup_read_obs_file", "eup_write_obs_file",
     "eup_read_raw_state", "eup_write_raw_state", "eup_init_equilibrium", "eup_geometry_cylinder_z",
     "eup_geometry_reticular_shell", "eup_mem_force_noalloc", "eup_set_solid_fraction", "eup_adjoint_run",
-    "eup_geometry_ridged_shell",
+    "eup_geometry_ridged_shell", "eup_get_region_sums", "eup_init_state",
 ]
 
 
@@ -101,6 +101,8 @@ def _load():
         "eup_mem_force_noalloc": ([i32, i32, i32, ctypes.c_int32 * 6, P19, i32, vp, vp, vp], ctypes.c_int),
         "eup_set_solid_fraction": ([vp, vp], ctypes.c_int),
         "eup_geometry_ridged_shell": ([i32, i32, i32] + [dbl] * 12 + [ctypes.c_uint64, vp, vp], ctypes.c_int),
+        "eup_get_region_sums": ([vp, vp, vp], ctypes.c_int),
+        "eup_init_state": ([vp, dbl, dbl, ctypes.c_uint64, i64], ctypes.c_int),
         "eup_adjoint_run": ([vp, ctypes.POINTER(AdjointConfig), ctypes.POINTER(dbl), vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -278,6 +280,19 @@ class Solver:
         ijk = np.ascontiguousarray(np.asarray(ijk, dtype=np.int32).reshape(-1, 3))
         out = np.zeros((ijk.shape[0], 4), dtype=np.float64)
         self._ck(lib.eup_get_probes(self._h, ijk.shape[0], ijk.ctypes.data, out.ctypes.data))
+        return out
+
+    def init_state(self, u_in, amp, seed, itime=0):
+        """Seeded equilibrium state generated on the device (same bits as upload(init_equilibrium(...)))."""
+        self._ck(lib.eup_init_state(self._h, float(u_in), float(amp), int(seed), int(itime)))
+
+    def region_sums(self, region) -> np.ndarray:
+        """FP64 {count, sum rho, sum ux, sum uy, sum uz, sum u^2} over the fluid nodes where
+        region (shape (n, m, l), truthy = included) is set."""
+        r = np.ascontiguousarray(np.asarray(region, dtype=bool).astype(np.uint8))
+        assert r.shape == (self.cfg.lz, self.cfg.ly, self.cfg.lx)
+        out = np.zeros(6, dtype=np.float64)
+        self._ck(lib.eup_get_region_sums(self._h, r.ctypes.data, out.ctypes.data))
         return out
 
     def links(self) -> np.ndarray:

@@ -273,6 +273,11 @@ void monitor_dispatch(eup_handle* h) {
     launch_monitor<S, R>(make_lat<S, R>(h, h->cur), h->g, make_mask(h), make_reduce(h), h->dscratch, h->stream);
 }
 template <typename S, typename R>
+void region_dispatch(eup_handle* h, const uint8_t* d_region) {
+    launch_region_sums<S, R>(make_lat<S, R>(h, h->cur), h->g, make_mask(h), d_region, make_reduce(h), h->dscratch,
+                             h->stream);
+}
+template <typename S, typename R>
 void probes_dispatch(eup_handle* h, int npts, const int32_t* d_ijk, double* d_out) {
     launch_probes<S, R>(make_lat<S, R>(h, h->cur), h->g, npts, d_ijk, d_out, h->stream);
 }
@@ -480,6 +485,31 @@ int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, in
     return EUP_OK;
 }
 
+int eup_init_state(eup_handle* h, double u_in, double amp, uint64_t seed, int64_t itime) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!std::isfinite(u_in) || !std::isfinite(amp)) return fail(h, EUP_ERR_INVALID_ARG, "eup_init_state: bad velocity");
+    const Geo& g = h->g;
+    const int eb = (h->prec == EUP_FP64) ? 8 : 4;  // what eup_init_equilibrium would hand to eup_upload
+    const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * eb;
+    if ((rc = ensure_staging(h, bytes))) return rc;
+    for (int q = 0; q < Q; ++q) {
+        if (eb == 8) launch_init_population<double>(static_cast<double*>(h->staging), g, q, u_in, amp, seed, h->stream);
+        else launch_init_population<float>(static_cast<float*>(h->staging), g, q, u_in, amp, seed, h->stream);
+        DISPATCH(h, upload_q, h, q, eb);
+    }
+    CK(h, cudaMemcpyAsync(h->d_itime, &itime, sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+    DISPATCH(h, fill_xface_dispatch, h);
+    h->itime = itime;
+    h->series_first = itime;
+    h->has_state = true;
+    if (h->pbb) CK(h, cudaMemsetAsync(h->series + 3 * (itime % h->cap), 0, 3 * sizeof(double), h->stream));
+    else DISPATCH(h, enqueue_drag_only, h);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
 int eup_download(eup_handle* h, void* const pops[19], int32_t elem_bytes) {
     int rc = check_handle(h);
     if (rc) return rc;
@@ -615,6 +645,27 @@ int eup_get_monitor(eup_handle* h, double out[5]) {
     CK(h, cudaStreamSynchronize(h->stream));
     for (int c = 0; c < 5; ++c)
         if (!std::isfinite(out[c])) return fail(h, EUP_ERR_DIVERGED, "eup_get_monitor: non-finite FP64 sum (run diverged)");
+    return EUP_OK;
+}
+
+int eup_get_region_sums(eup_handle* h, const uint8_t* region, double out[6]) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!region || !out) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_region_sums: null argument");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_region_sums: no state uploaded");
+    uint8_t* d_region = nullptr;
+    CK(h, cudaMalloc(&d_region, (size_t)h->g.N));
+    cudaError_t e = cudaMemcpyAsync(d_region, region, (size_t)h->g.N, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        DISPATCH(h, region_dispatch, h, d_region);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, h->dscratch, sizeof(double) * 6, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_region);
+    if (e != cudaSuccess) return cuda_fail(h, e, "eup_get_region_sums");
+    for (int c = 0; c < 6; ++c)
+        if (!std::isfinite(out[c])) return fail(h, EUP_ERR_DIVERGED, "eup_get_region_sums: non-finite FP64 sum");
     return EUP_OK;
 }
 

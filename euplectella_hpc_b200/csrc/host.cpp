@@ -7,6 +7,9 @@
 #include <vector>
 
 #include "../../include/eup.h"
+#include "init_eq.h"
+
+using eup::splitmix64;
 
 // Shared with the device entry points: eup_last_error(NULL) reports it.
 void eup_internal_set_error(const std::string& msg);
@@ -47,46 +50,6 @@ bool write_record(FILE* f, const void* src, int64_t bytes) {
            std::fwrite(&m, 4, 1, f) == 1;
 }
 
-uint64_t splitmix64(uint64_t x) {
-    uint64_t z = x + 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-
-// Equilibrium of CODE/SRC/init.F90:194-232 for one node, in type T.
-template <typename T>
-void equilibrium(T xj, T yj, T zj, T out[19]) {
-    const T rf = T(3), qf = T(1.5), t3 = T(3), one = T(1), crho = T(1);
-    const T p0 = (T)(1.0 / 3.0), p1 = (T)(1.0 / 18.0), p2 = (T)(1.0 / 36.0);
-    const T cvsq = xj * xj + yj * yj + zj * zj;
-    const T c[19] = {
-        rf * (xj - yj) + qf * (t3 * (xj - yj) * (xj - yj) - cvsq),
-        rf * (xj - zj) + qf * (t3 * (xj - zj) * (xj - zj) - cvsq),
-        rf * (xj + yj) + qf * (t3 * (xj + yj) * (xj + yj) - cvsq),
-        rf * (xj + zj) + qf * (t3 * (xj + zj) * (xj + zj) - cvsq),
-        rf * (xj) + qf * (t3 * (xj) * (xj) - cvsq),
-        rf * (zj) + qf * (t3 * (zj) * (zj) - cvsq),
-        rf * (yj + zj) + qf * (t3 * (yj + zj) * (yj + zj) - cvsq),
-        rf * (yj) + qf * (t3 * (yj) * (yj) - cvsq),
-        rf * (yj - zj) + qf * (t3 * (yj - zj) * (yj - zj) - cvsq),
-        rf * (-xj - yj) + qf * (t3 * (xj + yj) * (xj + yj) - cvsq),
-        rf * (-xj - zj) + qf * (t3 * (xj + zj) * (xj + zj) - cvsq),
-        rf * (-xj + yj) + qf * (t3 * (xj - yj) * (xj - yj) - cvsq),
-        rf * (-xj + zj) + qf * (t3 * (xj - zj) * (xj - zj) - cvsq),
-        rf * (-xj) + qf * (t3 * (xj) * (xj) - cvsq),
-        rf * (-zj) + qf * (t3 * (zj) * (zj) - cvsq),
-        rf * (-yj - zj) + qf * (t3 * (yj + zj) * (yj + zj) - cvsq),
-        rf * (-yj) + qf * (t3 * (yj) * (yj) - cvsq),
-        rf * (-yj + zj) + qf * (t3 * (yj - zj) * (yj - zj) - cvsq),
-        rf * (T(0)) + qf * (t3 * (T(0)) * (T(0)) - cvsq),
-    };
-    static const int wc[19] = {2, 2, 2, 2, 1, 1, 2, 1, 2, 2, 2, 2, 2, 1, 1, 2, 1, 2, 0};
-    for (int q = 0; q < 19; ++q) {
-        const T w = wc[q] == 0 ? p0 : (wc[q] == 1 ? p1 : p2);
-        out[q] = crho * w * (one + c[q]);
-    }
-}
 
 template <typename T>
 void init_state(int32_t l, int32_t m, int32_t n, double u_in, double amp, uint64_t seed, void* const pops[19]) {
@@ -95,13 +58,8 @@ void init_state(int32_t l, int32_t m, int32_t n, double u_in, double amp, uint64
     for (int q = 0; q < 19; ++q) dst[q] = static_cast<T*>(pops[q]);
 #pragma omp parallel for schedule(static)
     for (int64_t L = 0; L < total; ++L) {
-        double xi[3];
-        for (int c = 0; c < 3; ++c) {
-            const uint64_t h = splitmix64(seed + 3u * (uint64_t)L + (uint64_t)c);
-            xi[c] = (double)(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
-        }
         T f[19];
-        equilibrium<T>((T)(u_in + amp * xi[0]), (T)(amp * xi[1]), (T)(amp * xi[2]), f);
+        eup::init_node<T>(L, u_in, amp, seed, f);
         for (int q = 0; q < 19; ++q) dst[q][L] = f[q];
     }
 }

@@ -119,6 +119,16 @@ template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g,
                            const Phys<R>& ph, int variant, cudaStream_t st);
 
+// FP64 sums over the fluid nodes of a region (device byte mask, one per node) into out[6].
+template <typename S, typename R>
+void launch_region_sums(const Lat<S, R>& L, const Geo& g, const Mask& mk, const uint8_t* region, const Reduce& red,
+                        double* out, cudaStream_t st);
+
+// Population q of the seeded equilibrium initial state (init_eq.h) into a
+// haloed staging array of (l+2)(m+2)(n+2) elements.
+template <typename T>
+void launch_init_population(T* staging, const Geo& g, int q, double u_in, double amp, uint64_t seed, cudaStream_t st);
+
 // FP64 sums of CODE/SRC/diagno.F90 into out[5] (device pointer).
 template <typename S, typename R>
 void launch_monitor(const Lat<S, R>& L, const Geo& g, const Mask& mk, const Reduce& red,

@@ -3,6 +3,7 @@
 // (CODE/SRC/bcond.obs.F90), the FP64 monitor (CODE/SRC/diagno.F90), probes
 // (CODE/SRC/probe_global.F90) and the host-layout scatter/gather used by
 // upload and download.  All of it is O(surface) or O(solid surface) work.
+#include "init_eq.h"
 #include "internal.h"
 
 namespace eup {
@@ -403,6 +404,45 @@ __global__ void k_monitor(Lat<S, R> L, Geo g, Mask mk, Reduce red, double* out) 
     block_reduce_store<5>(s, red, out);
 }
 
+// FP64 sums over the fluid nodes with region[lin] != 0 (the cavity of a shell,
+// a probe box, ...): {count, sum rho, sum ux, sum uy, sum uz, sum u^2}, u = j/rho
+// as CODE/SRC/diagno.F90:86-105 computes it.
+template <typename S, typename R>
+__global__ void k_region_sums(Lat<S, R> L, Geo g, Mask mk, const uint8_t* region, Reduce red, double* out) {
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.N;
+         lin += (int64_t)gridDim.x * blockDim.x) {
+        if (!region[lin]) continue;
+        const int i = (int)(lin % g.l) + 1;
+        const int j = (int)((lin / g.l) % g.m) + 1;
+        const int k = (int)(lin / g.lm) + 1;
+        if (mk.solid(g, i, j, k)) continue;
+        double a[19];
+#pragma unroll
+        for (int q = 0; q < 19; ++q) a[q] = (double)Store<S, R>::load(L.pop[q][lin], q, L.inv_scale);
+        double rho = 0.0;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) rho += a[q];
+        const double ri = 1.0 / rho;
+        const double xj = (a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13]) * ri;
+        const double yj = (a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17]) * ri;
+        const double zj = (a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15]) * ri;
+        s[0] += 1.0; s[1] += rho; s[2] += xj; s[3] += yj; s[4] += zj; s[5] += xj * xj + yj * yj + zj * zj;
+    }
+    block_reduce_store<6>(s, red, out);
+}
+
+// Population q of the seeded equilibrium state (init_eq.h) over the haloed
+// node range, into a staging buffer laid out like one host array.
+template <typename T>
+__global__ void k_init_population(T* out, int q, int64_t total, double u_in, double amp, uint64_t seed) {
+    for (int64_t L = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; L < total; L += (int64_t)gridDim.x * blockDim.x) {
+        T f[19];
+        init_node<T>(L, u_in, amp, seed, f);
+        out[L] = f[q];
+    }
+}
+
 template <typename S, typename R>
 __global__ void k_probes(Lat<S, R> L, Geo g, int npts, const int32_t* ijk, double* out) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -540,6 +580,21 @@ void launch_monitor(const Lat<S, R>& L, const Geo& g, const Mask& mk, const Redu
 }
 
 template <typename S, typename R>
+void launch_region_sums(const Lat<S, R>& L, const Geo& g, const Mask& mk, const uint8_t* region, const Reduce& red,
+                        double* out, cudaStream_t st) {
+    const unsigned blocks = grid_for(g.N, kTpb, (unsigned)red.max_blocks);
+    k_region_sums<S, R><<<blocks, kTpb, 0, st>>>(L, g, mk, region, red, out);
+}
+
+template <typename T>
+void launch_init_population(T* staging, const Geo& g, int q, double u_in, double amp, uint64_t seed, cudaStream_t st) {
+    const int64_t total = (int64_t)(g.l + 2) * (g.m + 2) * (g.n + 2);
+    k_init_population<T><<<grid_for(total, kTpb), kTpb, 0, st>>>(staging, q, total, u_in, amp, seed);
+}
+template void launch_init_population<float>(float*, const Geo&, int, double, double, uint64_t, cudaStream_t);
+template void launch_init_population<double>(double*, const Geo&, int, double, double, uint64_t, cudaStream_t);
+
+template <typename S, typename R>
 void launch_probes(const Lat<S, R>& L, const Geo& g, int npts, const int32_t* ijk, double* out,
                    cudaStream_t st) {
     k_probes<S, R><<<(npts + 127) / 128, 128, 0, st>>>(L, g, npts, ijk, out);
@@ -563,6 +618,8 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
                                            const uint64_t*, int64_t, bool, const Reduce&, double*,     \
                                            int64_t, int64_t*, bool, cudaStream_t);                     \
     template void launch_fill_xface<S, R>(const Lat<S, R>&, const Geo&, cudaStream_t);                 \
+    template void launch_region_sums<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const uint8_t*,   \
+                                           const Reduce&, double*, cudaStream_t);                         \
     template void launch_monitor<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const Reduce&,       \
                                        double*, cudaStream_t);                                         \
     template void launch_probes<S, R>(const Lat<S, R>&, const Geo&, int, const int32_t*, double*,      \

@@ -12,8 +12,8 @@ import math
 
 import numpy as np
 
-from . import (FREESLIP, FP32, INFLOW, OUTFLOW, PERIODIC, Config, geometry_cylinder_z,
-               geometry_reticular_shell, init_equilibrium)
+from . import (FP16_DEV, FREESLIP, FP32, INFLOW, OUTFLOW, PERIODIC, Config, geometry_cylinder_z,
+               geometry_reticular_shell, geometry_ridged_shell, init_equilibrium)
 
 U_IN = 0.05          # inlet velocity of every configuration
 PERTURBATION = 1e-4  # amplitude of the seeded initial velocity perturbation
@@ -119,4 +119,67 @@ def pbb_cylinder_channel(lx=192, ly=96, lz=96, d=24.0, re=100.0, steps=4000, avg
     wl = Workload("pbb_cylinder_192x96x96_re100", cfg, np.zeros((lz, ly, lx), np.int32), steps, seed)
     wl.ns = solid_fraction_cylinder(lx, ly, lz, d, lx / 4.0, (ly + 1) / 2.0, sigma, seed)
     wl.avg_steps = avg_steps
+    return wl
+
+
+@dataclasses.dataclass
+class RidgedShell:
+    """Geometry parameters of the ridged lattice shell, in lattice units."""
+    x0: float
+    length: float
+    yc: float
+    zc: float
+    outer_d: float
+    strut_d: float
+    pitch: float
+    ridge_h: float
+    ridge_t: float
+    cap_t: float
+    pore_d: float
+    seed: int
+
+    def args(self, lx, ly, lz):
+        return (lx, ly, lz, self.x0, self.length, self.yc, self.zc, self.outer_d, self.strut_d, self.pitch)
+
+    def mask(self, lx, ly, lz) -> np.ndarray:
+        ns = geometry_ridged_shell(*self.args(lx, ly, lz), self.ridge_h, self.ridge_t, self.cap_t, self.pore_d, 0.0,
+                                   self.seed)
+        return (ns >= 0.5).astype(np.int32)
+
+    def field(self, lx, ly, lz, smooth_w, ridge_h=None):
+        """Solid fraction with smoothed ridges and d n_s / d ridge_h."""
+        h = self.ridge_h if ridge_h is None else ridge_h
+        return geometry_ridged_shell(*self.args(lx, ly, lz), h, self.ridge_t, self.cap_t, self.pore_d, smooth_w,
+                                     self.seed, with_derivative=True)
+
+
+def ridged_shell_channel(lx=1024, ly=512, lz=512, scale=1.0, re=2000.0, steps=10000, seed=2025,
+                         precision=FP16_DEV) -> Workload:
+    """Channel 1024x512x512 holding the reticular shell of the 768x384x384 case (outer D 96,
+    length 256, struts d=4 at pitch 16) plus two counter-rotating 45-degree helical ridges
+    (height 8, thickness 4) and a seeded porous cap (thickness 4, pores of diameter 10 on a
+    20-lu grid) at its downstream end; inlet 0.05, free-slip y and z, Re 2000 on the shell
+    diameter; FP16-stored deviations.  (A cap with 6-lu pores makes the BGK run diverge within
+    300 steps in every precision, FP64 included: the jets through pores that small are not
+    resolved at this viscosity.)  `scale` shrinks the channel and every length of the body
+    together (the viscosity follows Re on the scaled diameter)."""
+    lx, ly, lz = int(round(lx * scale)), int(round(ly * scale)), int(round(lz * scale))
+    body = RidgedShell(x0=lx / 4.0, length=256.0 * scale, yc=(ly + 1) / 2.0, zc=(lz + 1) / 2.0, outer_d=96.0 * scale,
+                       strut_d=4.0 * scale, pitch=16.0 * scale, ridge_h=8.0 * scale, ridge_t=4.0 * scale,
+                       cap_t=4.0 * scale, pore_d=10.0 * scale, seed=seed)
+    nu = svisc_for(re, U_IN, body.outer_d)
+    area = math.pi * body.outer_d * body.outer_d / 4.0
+    cfg = Config(lx, ly, lz, bc=(OUTFLOW, INFLOW, FREESLIP, FREESLIP, FREESLIP, FREESLIP), svisc=nu,
+                 u_inflow=U_IN, precision=precision, cd_rho0=1.0, cd_uref=U_IN, cd_length=body.outer_d,
+                 cd_span=area / body.outer_d)
+    obs = body.mask(lx, ly, lz)
+    yi, zi = int(round(body.yc)), int(round(body.zc))
+    probes = [(int(body.x0 - 32 * scale), yi, zi), (int(body.x0 + body.length / 2), yi, zi),
+              (int(body.x0 + body.length + 64 * scale), yi, zi)]
+    k, j, i = np.meshgrid(np.arange(1, lz + 1), np.arange(1, ly + 1), np.arange(1, lx + 1), indexing="ij",
+                          sparse=True)
+    rin = 0.5 * body.outer_d - body.strut_d
+    cavity = ((j - body.yc) ** 2 + (k - body.zc) ** 2 < rin * rin) & (i >= body.x0) & (i <= body.x0 + body.length)
+    wl = Workload(f"ridged_shell_{lx}x{ly}x{lz}_re{int(re)}", cfg, obs, steps, seed, probes, cavity)
+    wl.body = body
     return wl

@@ -120,6 +120,13 @@ int eup_set_obstacles(eup_handle* h, const int32_t* obs);
  * restart path (CODE/SRC/restore_raw.F90:43-63).  Sets the step counter. */
 int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, int64_t itime);
 
+/* The seeded equilibrium state of eup_init_equilibrium generated on the
+ * device: the same bits as eup_upload of eup_init_equilibrium's arrays
+ * (elem_bytes 8 for an FP64 handle, else 4), without host arrays or a
+ * host-to-device copy of the lattice.  No reference counterpart (the
+ * reference initialises on the host, CODE/SRC/init.F90). */
+int eup_init_state(eup_handle* h, double u_in, double amp, uint64_t seed, int64_t itime);
+
 /* Copies the current state back into 19 haloed host arrays: the interior from
  * the lattice, the halo from the halo shell, exactly what the reference's
  * arrays hold after a step.  Replaces the device-to-host copies of
@@ -177,6 +184,14 @@ int eup_get_cd_series(eup_handle* h, int64_t first_step, int32_t count, double* 
  * voxels counted as rho = 1, u = 0: out = {sum rho, sum ux, sum uy, sum uz,
  * sum u^2}.  EUP_ERR_DIVERGED when any sum is not finite. */
 int eup_get_monitor(eup_handle* h, double out[5]);
+
+/* FP64 sums over the fluid nodes whose byte in region (Fortran order, l*m*n,
+ * nonzero = included) is set: out = {count, sum rho, sum ux, sum uy, sum uz,
+ * sum u^2}.  Region means (the velocity inside a shell's cavity, a probe box)
+ * without downloading the populations.  No reference counterpart: the
+ * reference's diagnostics of this kind (CODE/SRC/varm.F90, prof_*.F90) sum
+ * whole planes and lines of the host arrays. */
+int eup_get_region_sums(eup_handle* h, const uint8_t* region, double out[6]);
 
 /* rho, ux, uy, uz (FP64) at npts interior nodes (1-based i,j,k triples), as
  * CODE/SRC/probe_global.F90:58-77 computes them. */

@@ -152,6 +152,46 @@ def test_probes_match_oracle(eup, orc, require_gpu):
                                        uy[k - 1, j - 1, i - 1], uz[k - 1, j - 1, i - 1]])
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16"])
+def test_device_init_equals_host_init_upload(eup, require_gpu, prec):
+    l, m, n = 40, 18, 12
+    code, dt = {"fp32": (eup.FP32, np.float32), "fp64": (eup.FP64, np.float64), "fp16": (eup.FP16_DEV, np.float32)}[prec]
+    cfg = eup.Config(l, m, n, bc=(5, 4, 3, 3, 0, 0), svisc=0.01, u_inflow=0.05, precision=code)
+    got = []
+    for dev in (False, True):
+        with eup.Solver(cfg) as s:
+            if dev:
+                s.init_state(0.05, 1e-3, 99, itime=3)
+            else:
+                s.upload(eup.init_equilibrium(l, m, n, 0.05, 1e-3, 99, dt), itime=3)
+            s.step(2)
+            got.append((s.download(dt), s.itime))
+    assert got[0][1] == got[1][1] == 5
+    assert np.array_equal(got[0][0], got[1][0])
+
+
+def test_region_sums_match_oracle(eup, orc, require_gpu):
+    case = CASES[0]
+    name, (l, m, n), bc, svisc, u0, uin, u00, builder = case
+    obs = builder(l, m, n)
+    a = eup.init_equilibrium(l, m, n, uin, 1e-3, 8, np.float32)
+    p = orc.params(l, m, n, bc, svisc=svisc, u_inflow=uin)
+    k, j, i = np.meshgrid(np.arange(1, n + 1), np.arange(1, m + 1), np.arange(1, l + 1), indexing="ij")
+    region = ((i - l / 2) ** 2 + (j - m / 2) ** 2 < (m / 3) ** 2) & (k > 2)
+    with eup.Solver(eup.Config(l, m, n, bc=bc, svisc=svisc, u_inflow=uin)) as s:
+        s.set_obstacles(obs)
+        s.upload(a)
+        s.step(6)
+        got = s.region_sums(region)
+    orc.run(p, a, obs, 6)
+    rho, ux, uy, uz = orc.macro(p, a)
+    sel = region & (obs == 0)
+    want = [sel.sum(), rho[sel].sum(), ux[sel].sum(), uy[sel].sum(), uz[sel].sum(),
+            (ux[sel] ** 2 + uy[sel] ** 2 + uz[sel] ** 2).sum()]
+    assert got[0] == want[0]
+    np.testing.assert_allclose(got[1:], want[1:], rtol=1e-12, atol=1e-15)
+
+
 def test_error_paths(eup, require_gpu):
     with eup.Solver(eup.Config(12, 8, 6)) as s:
         with pytest.raises(eup.EupError) as e:
