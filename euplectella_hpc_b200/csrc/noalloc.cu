@@ -3,9 +3,10 @@
 // eup_get_forces reduces through per-block partial sums that live in buffers
 // the handle allocated.  Some callers can hold no handle and must not let a
 // library allocate: a Fortran driver whose a01..a19 and obs already sit on the
-// GPU under its own OpenACC data region (the reference's GPU build) and which
-// calls from inside that region, or any code that records its time loop into
-// a CUDA graph, where cudaMalloc is not allowed during stream capture.  This
+// GPU under its own OpenACC data region (the reference's GPU build) and whose
+// runtime owns the device memory, or a code that hands out a fixed device-memory
+// budget through its own allocator, where an extra cudaMalloc would fail or
+// stall every stream on the device.  This
 // entry point reads the caller's device arrays in the reference's haloed
 // layout and writes the force to the caller's device memory; its only scratch
 // is the file-scope array below, fixed in size at load time.

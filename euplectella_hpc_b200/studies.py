@@ -103,7 +103,7 @@ def precision_study(re_list=(500.0, 1000.0, 2000.0), steps=20000):
 
 
 def adjoint_study(steps=4000, avg_steps=1000, checkpoints=64, n_fd=32, h=1e-3, fd_seed=2027):
-    """Config-4 adjoint: mean C_d over the last avg_steps of `steps` on the 192x96x96 partial-
+    """Adjoint of mean C_d over the last avg_steps of `steps` on the 192x96x96 partial-
     bounce-back channel.  Returns timings (adjoint with recomputation vs a plain forward run of the
     same steps), the FP32-vs-FP64 adjoint gradient difference, and central finite differences of
     FP64 forward runs at n_fd seeded voxels against the FP64 adjoint."""
@@ -285,7 +285,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--re", default="500,1000,2000")
     ap.add_argument("--out", default=None)
-    ap.add_argument("--adjoint", action="store_true", help="run the config-4 adjoint study instead")
+    ap.add_argument("--adjoint", action="store_true", help="run the 192x96x96 partial-bounce-back adjoint study instead")
     ap.add_argument("--fd", type=int, default=32)
     ap.add_argument("--production", choices=["shell", "ridged"], default=None,
                     help="forward run of the 768x384x384 reticular shell or the 1024x512x512 ridged shell")

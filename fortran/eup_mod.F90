@@ -4,10 +4,9 @@
 !     Declares the C ABI of include/eup.h for the Fortran driver of
 !     Euplectella_HPC (CODE/SRC/bgk3d.F90).  With this module the driver
 !     keeps its namelist, its arrays a01..a19(0:l+1,0:m+1,0:n+1) and all of
-!     its output routines; only the calls of the time loop change (see
-!     INTEGRATION.md for the patch of bgk3d.F90, initialize.F90 and
-!     diagnostic.F90).  Same pattern as the reference's own C interop in
-!     CODE/SRC/get_mem_mod.F90:1-10.
+!     its output routines; only the calls of the time loop change (in
+!     bgk3d.F90, initialize.F90 and diagnostic.F90).  Same pattern as the
+!     reference's own C interop in CODE/SRC/get_mem_mod.F90:1-10.
 ! =====================================================================
       module eup_mod
       use iso_c_binding
@@ -26,6 +25,10 @@
          real(c_double)     :: cd_rho0, cd_uref, cd_length, cd_span
          integer(c_int64_t) :: series_capacity
       end type eup_config
+
+      type, bind(c) :: eup_adjoint_config
+         integer(c_int32_t) :: nsteps, avg_steps, checkpoints, reserved
+      end type eup_adjoint_config
 
       interface
          integer(c_int) function eup_create(cfg, h) bind(c, name="eup_create")
@@ -89,6 +92,50 @@
          type(c_ptr) function eup_last_error(h) bind(c, name="eup_last_error")
             import :: c_ptr
             type(c_ptr), value :: h
+         end function
+
+         integer(c_int) function eup_step_profiled(h, nsteps, ms) bind(c, name="eup_step_profiled")
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: nsteps
+            real(c_double)            :: ms(4)
+         end function
+
+         integer(c_int) function eup_get_probes(h, npts, ijk, rho_u) bind(c, name="eup_get_probes")
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: npts
+            integer(c_int32_t)        :: ijk(3, *)
+            real(c_double)            :: rho_u(4, *)
+         end function
+
+         integer(c_int) function eup_get_region_sums(h, region, sums) bind(c, name="eup_get_region_sums")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            type(c_ptr), value :: region            ! c_loc of an integer(c_int8_t) mask(l,m,n)
+            real(c_double)     :: sums(6)
+         end function
+
+         integer(c_int) function eup_init_state(h, u_in, amp, seed, itime) bind(c, name="eup_init_state")
+            import :: c_int, c_ptr, c_double, c_int64_t
+            type(c_ptr), value         :: h
+            real(c_double), value      :: u_in, amp
+            integer(c_int64_t), value  :: seed, itime
+         end function
+
+         integer(c_int) function eup_set_solid_fraction(h, ns) bind(c, name="eup_set_solid_fraction")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            type(c_ptr), value :: ns                ! c_loc of real(c_double) ns(l,m,n), or c_null_ptr
+         end function
+
+         integer(c_int) function eup_adjoint_run(h, cfg, objective, grad_ns, stats) bind(c, name="eup_adjoint_run")
+            import :: c_int, c_ptr, c_double, eup_adjoint_config
+            type(c_ptr), value            :: h
+            type(eup_adjoint_config)      :: cfg
+            real(c_double)                :: objective
+            real(c_double)                :: grad_ns(*)
+            real(c_double)                :: stats(8)
          end function
 
          integer(c_int) function eup_read_obs_file(path, l, m, n, obs, nobs) bind(c, name="eup_read_obs_file")

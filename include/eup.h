@@ -211,8 +211,9 @@ int eup_get_boundary_solid(eup_handle* h, int64_t* list, int64_t cap, int64_t* c
  * as eup_get_forces) of a state that lives in the CALLER's device memory, for
  * callers that cannot let a library allocate: e.g. a Fortran driver whose
  * a01..a19 and obs are already device-resident under its own OpenACC data
- * region, or code that captures its time loop into a CUDA graph, where
- * cudaMalloc is not allowed.  Needs no handle and allocates nothing: its
+ * region and whose runtime owns the device memory, or a code with a fixed
+ * device-memory budget handed out by its own allocator, where an extra
+ * cudaMalloc would fail or stall the device.  Needs no handle and allocates nothing: its
  * scratch is one fixed device array in the library (one FP64 partial per
  * z-plane, at most 4096 planes, about 96 KiB per GPU, held until the process
  * exits); lz > 4096 is rejected with EUP_ERR_UNSUPPORTED.

@@ -1,6 +1,7 @@
 """eup_mem_force_noalloc: the momentum-exchange force for callers that cannot
 allocate device memory (a Fortran/OpenACC driver handing over its own
-device-resident arrays, or code inside a CUDA-graph capture).  It reads the
+device-resident arrays, or a code with a fixed device-memory budget managed by its
+own allocator).  It reads the
 caller's device arrays, writes to the caller's device output, and uses only
 the library's fixed scratch array.  Checked through the C ABI against
 eup_get_forces on the same state, on two calls in a row.  This file is
