@@ -38,7 +38,8 @@ EXPORTED = [
     "eup_get_probes", "eup_get_links", "eup_get_boundary_solid", "eup_read_obs_file", "eup_write_obs_file",
     "eup_read_raw_state", "eup_write_raw_state", "eup_init_equilibrium", "eup_geometry_cylinder_z",
     "eup_geometry_reticular_shell", "eup_mem_force_noalloc", "eup_set_solid_fraction", "eup_adjoint_run",
-    "eup_geometry_ridged_shell", "eup_get_region_sums", "eup_init_state",
+    "eup_geometry_ridged_shell", "eup_get_region_sums", "eup_init_state", "eup_get_line", "eup_get_plane_means",
+    "eup_get_cv_drag",
 ]
 
 
@@ -103,6 +104,9 @@ def _load():
         "eup_geometry_ridged_shell": ([i32, i32, i32] + [dbl] * 12 + [ctypes.c_uint64, vp, vp], ctypes.c_int),
         "eup_get_region_sums": ([vp, vp, vp], ctypes.c_int),
         "eup_init_state": ([vp, dbl, dbl, ctypes.c_uint64, i64], ctypes.c_int),
+        "eup_get_line": ([vp, i32, i32, i32, vp], ctypes.c_int),
+        "eup_get_plane_means": ([vp, i32, vp], ctypes.c_int),
+        "eup_get_cv_drag": ([vp, vp, vp], ctypes.c_int),
         "eup_adjoint_run": ([vp, ctypes.POINTER(AdjointConfig), ctypes.POINTER(dbl), vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -285,6 +289,27 @@ class Solver:
     def init_state(self, u_in, amp, seed, itime=0):
         """Seeded equilibrium state generated on the device (same bits as upload(init_equilibrium(...)))."""
         self._ck(lib.eup_init_state(self._h, float(u_in), float(amp), int(seed), int(itime)))
+
+    def line(self, axis, c1, c2) -> np.ndarray:
+        """prof_i/prof_j/prof_k line (axis 0/1/2) at the fixed coordinates c1, c2: rows (u, w, v, den)."""
+        n = (self.cfg.lx, self.cfg.ly, self.cfg.lz)[axis]
+        out = np.zeros((n, 4), dtype=np.float64)
+        self._ck(lib.eup_get_line(self._h, axis, c1, c2, out.ctypes.data))
+        return out
+
+    def plane_means(self, axis=2) -> np.ndarray:
+        """varm-style means (u, w, v, den) of every plane normal to axis."""
+        n = (self.cfg.lx, self.cfg.ly, self.cfg.lz)[axis]
+        out = np.zeros((n, 4), dtype=np.float64)
+        self._ck(lib.eup_get_plane_means(self._h, axis, out.ctypes.data))
+        return out
+
+    def cv_drag(self, box) -> np.ndarray:
+        """Control-volume drag (fluxX, fluxY) of box (xstart, xstop, ystart, ystop, zstart, zstop)."""
+        b = np.ascontiguousarray(np.asarray(box, dtype=np.int32))
+        out = np.zeros(2, dtype=np.float64)
+        self._ck(lib.eup_get_cv_drag(self._h, b.ctypes.data, out.ctypes.data))
+        return out
 
     def region_sums(self, region) -> np.ndarray:
         """FP64 {count, sum rho, sum ux, sum uy, sum uz, sum u^2} over the fluid nodes where

@@ -273,6 +273,19 @@ void monitor_dispatch(eup_handle* h) {
     launch_monitor<S, R>(make_lat<S, R>(h, h->cur), h->g, make_mask(h), make_reduce(h), h->dscratch, h->stream);
 }
 template <typename S, typename R>
+void line_dispatch(eup_handle* h, int axis, int c1, int c2, double* d_out) {
+    launch_line<S, R>(make_lat<S, R>(h, h->cur), h->g, axis, c1, c2, d_out, h->stream);
+}
+template <typename S, typename R>
+void plane_dispatch(eup_handle* h, int axis, double* d_out) {
+    launch_plane_means<S, R>(make_lat<S, R>(h, h->cur), h->g, axis, d_out, h->stream);
+}
+template <typename S, typename R>
+void cv_dispatch(eup_handle* h, const int* box) {
+    launch_cv_drag<S, R>(make_lat<S, R>(h, h->cur), h->g, box, make_phys<R>(h).omega, make_reduce(h), h->dscratch,
+                         h->stream);
+}
+template <typename S, typename R>
 void region_dispatch(eup_handle* h, const uint8_t* d_region) {
     launch_region_sums<S, R>(make_lat<S, R>(h, h->cur), h->g, make_mask(h), d_region, make_reduce(h), h->dscratch,
                              h->stream);
@@ -645,6 +658,69 @@ int eup_get_monitor(eup_handle* h, double out[5]) {
     CK(h, cudaStreamSynchronize(h->stream));
     for (int c = 0; c < 5; ++c)
         if (!std::isfinite(out[c])) return fail(h, EUP_ERR_DIVERGED, "eup_get_monitor: non-finite FP64 sum (run diverged)");
+    return EUP_OK;
+}
+
+int eup_get_line(eup_handle* h, int32_t axis, int32_t c1, int32_t c2, double* out) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    const Geo& g = h->g;
+    if (!out || axis < 0 || axis > 2) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_line: bad axis or null out");
+    const int e1 = axis == 0 ? g.m : g.l, e2 = axis == 2 ? g.m : g.n;
+    if (c1 < 1 || c1 > e1 || c2 < 1 || c2 > e2)
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_get_line: line outside the interior");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_line: no state uploaded");
+    const int len = axis == 0 ? g.l : (axis == 1 ? g.m : g.n);
+    if ((rc = ensure_staging(h, sizeof(double) * 4 * (size_t)len))) return rc;
+    DISPATCH(h, line_dispatch, h, axis, c1, c2, static_cast<double*>(h->staging));
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(out, h->staging, sizeof(double) * 4 * (size_t)len, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
+int eup_get_plane_means(eup_handle* h, int32_t axis, double* out) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    const Geo& g = h->g;
+    if (!out || axis < 0 || axis > 2) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_plane_means: bad axis or null out");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_plane_means: no state uploaded");
+    const int len = axis == 0 ? g.l : (axis == 1 ? g.m : g.n);
+    if ((rc = ensure_staging(h, sizeof(double) * 4 * (size_t)len))) return rc;
+    DISPATCH(h, plane_dispatch, h, axis, static_cast<double*>(h->staging));
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(out, h->staging, sizeof(double) * 4 * (size_t)len, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
+int eup_get_cv_drag(eup_handle* h, const int32_t box[6], double out[2]) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!box || !out) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_cv_drag: null argument");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_cv_drag: no state uploaded");
+    // clipping and face weights of CODE/SRC/flux_X.F90:56-156 with the serial offsets 0
+    const int ext[3] = {h->g.l, h->g.m, h->g.n};
+    int lo[3], hi[3], w[3][2];
+    out[0] = out[1] = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        const int s0 = box[2 * d], s1 = box[2 * d + 1];
+        if (s0 > s1) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_cv_drag: box start after stop");
+        w[d][0] = w[d][1] = 1;
+        if (s0 > ext[d] || s1 < 0) return EUP_OK;  // box misses the lattice
+        if (s0 > 0 && s1 <= ext[d]) { lo[d] = s0; hi[d] = s1; }
+        else if (s0 > 0) { lo[d] = s0; hi[d] = ext[d]; w[d][1] = 0; }
+        else if (s1 <= ext[d]) { lo[d] = 1; hi[d] = s1; w[d][0] = 0; }
+        else return EUP_OK;  // box around the whole lattice: no face inside
+    }
+    const int clipped[6] = {lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]};
+    DISPATCH(h, cv_dispatch, h, clipped);
+    CK(h, cudaGetLastError());
+    double f[4];
+    CK(h, cudaMemcpyAsync(f, h->dscratch, sizeof(double) * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    out[0] = -f[0] * w[0][0] + f[1] * w[0][1];
+    out[1] = f[2] * w[1][0] + f[3] * w[1][1];
     return EUP_OK;
 }
 

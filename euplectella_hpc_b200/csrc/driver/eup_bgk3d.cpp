@@ -11,11 +11,16 @@
 //                      (CODE/SRC/diagnostic.F90:143, CODE/SRC/probe_global.F90:77, format i8,4e14.6)
 //   drag_mem.0000.dat  every icheck: itime, Fx, Fy, Fz, C_d of the FP64 momentum exchange
 //   monitor.dat        every icheck: itime and the FP64 means of CODE/SRC/diagno.F90:157
+//   prof_i/prof_j/prof_k.0000.dat  every icheck: the lines (1..l, m/2, n/2), (l/2, 1..m, n/2),
+//                      (l/2, m/2, 1..n) (CODE/SRC/diagnostic.F90:137-139, prof_*.F90, format i5,4(e14.6,1x))
+//   u_med.000.000.000.dat  every icheck: z-plane means of CODE/SRC/varm.F90 (format i5,4(e14.6,1x))
+//   drag.0000.dat      with --cv-drag: control-volume drag of CODE/SRC/drag.F90:51-67 (R = 100,
+//                      delta = 52..67 step 5), one line "delta itime fluxX fluxY 0" per box
 //   save.00.00.00.TTTTTTTT.bin every itsave (CODE/SRC/save_raw.F90:41-78)
 //   bgk.perf           loop time and MLUPS (CODE/SRC/finalize.F90:58-124)
 //
 //   eup_bgk3d [--preset cylinder_inf|freeslip|driven|couette|check2d|channel | --bc f,r,ri,le,u,d]
-//             [--precision fp32|fp64|fp16|bf16] [--device N] [--drag-length D] [--input bgk.input]
+//             [--precision fp32|fp64|fp16|bf16] [--device N] [--drag-length D] [--cv-drag] [--input bgk.input]
 #include <chrono>
 #include <cctype>
 #include <cmath>
@@ -112,6 +117,7 @@ int die(const std::string& msg, eup_handle* h = nullptr) {
 int main(int argc, char** argv) {
     std::string input = "bgk.input", preset = "cylinder_inf", prec = "fp32", bcarg;
     int device = 0;
+    bool cv_drag = false;
     double drag_length = 0.0;
     for (int a = 1; a < argc; ++a) {
         const std::string s = argv[a];
@@ -122,6 +128,7 @@ int main(int argc, char** argv) {
         else if (s == "--precision") prec = next();
         else if (s == "--device") device = std::atoi(next().c_str());
         else if (s == "--drag-length") drag_length = std::atof(next().c_str());
+        else if (s == "--cv-drag") cv_drag = true;
         else return die("unknown option " + s);
     }
     std::string err;
@@ -196,6 +203,11 @@ int main(int argc, char** argv) {
     FILE* fprobe = std::fopen("probe_g.0000.dat", "w");
     FILE* fdrag = std::fopen("drag_mem.0000.dat", "w");
     FILE* fmon = std::fopen("monitor.dat", "w");
+    FILE* fprof[3] = {std::fopen("prof_i.0000.dat", "w"), std::fopen("prof_j.0000.dat", "w"),
+                      std::fopen("prof_k.0000.dat", "w")};
+    FILE* fvarm = std::fopen("u_med.000.000.000.dat", "w");
+    FILE* fcv = cv_drag ? std::fopen("drag.0000.dat", "w") : nullptr;
+    std::vector<double> prof((size_t)4 * std::max(lx, std::max(ly, lz)));
     const int32_t probe[3] = {8 * lx / 20, 9 * ly / 16, lz / 2 - 5};
     const bool probe_ok = probe[0] >= 1 && probe[1] >= 1 && probe[2] >= 1;
     const auto t0 = std::chrono::steady_clock::now();
@@ -221,6 +233,36 @@ int main(int argc, char** argv) {
             std::fprintf(fdrag, "%8ld %.15e %.15e %.15e %.15e\n", it, f[0], f[1], f[2], cd);
             std::fprintf(fmon, "%8ld%s %s %s %s %s\n", it, fmt_e(mon[1] * rdv).c_str(), fmt_e(mon[2] * rdv).c_str(),
                          fmt_e(mon[3] * rdv).c_str(), fmt_e(mon[0] * rdv).c_str(), fmt_e(mon[4] * rdv).c_str());
+            // prof_i(m/2, n/2), prof_j(l/2, n/2), prof_k(l/2, m/2) and varm: "# t=" header,
+            // i5,4(e14.6,1x) rows, two empty records
+            const int32_t lc[3][2] = {{ly / 2, lz / 2}, {lx / 2, lz / 2}, {lx / 2, ly / 2}};
+            const int32_t len[3] = {lx, ly, lz};
+            for (int ax = 0; ax < 3; ++ax) {
+                if (lc[ax][0] < 1 || lc[ax][1] < 1) continue;
+                if (eup_get_line(h, ax, lc[ax][0], lc[ax][1], prof.data()) != EUP_OK) return die("eup_get_line", h);
+                std::fprintf(fprof[ax], "# t=%7ld\n", it);
+                for (int t = 0; t < len[ax]; ++t)
+                    std::fprintf(fprof[ax], "%5d%s %s %s %s \n", t + 1, fmt_e(prof[4 * t]).c_str(),
+                                 fmt_e(prof[4 * t + 1]).c_str(), fmt_e(prof[4 * t + 2]).c_str(),
+                                 fmt_e(prof[4 * t + 3]).c_str());
+                std::fprintf(fprof[ax], "\n\n");
+            }
+            if (eup_get_plane_means(h, 2, prof.data()) != EUP_OK) return die("eup_get_plane_means", h);
+            std::fprintf(fvarm, "# t=%7ld\n", it);
+            for (int k = 0; k < lz; ++k)
+                std::fprintf(fvarm, "%5d%s %s %s %s \n", k + 1, fmt_e(prof[4 * k]).c_str(), fmt_e(prof[4 * k + 1]).c_str(),
+                             fmt_e(prof[4 * k + 2]).c_str(), fmt_e(prof[4 * k + 3]).c_str());
+            std::fprintf(fvarm, "\n\n");
+            if (fcv) {
+                const int radius = 100;  // hard-wired in CODE/SRC/drag.F90:48
+                for (int delta = 52; delta <= 67; delta += 5) {
+                    const int32_t box[6] = {lx / 4 - radius - delta, lx / 4 + radius + delta,
+                                            ly / 2 - radius - delta, ly / 2 + radius + delta, 1, lz};
+                    double fl[2];
+                    if (eup_get_cv_drag(h, box, fl) != EUP_OK) return die("eup_get_cv_drag", h);
+                    std::fprintf(fcv, "%12d%12ld %.8E %.8E %11d\n", delta, it, fl[0], fl[1], 0);
+                }
+            }
         }
         if (itsave > 0 && it % itsave == 0) {
             if (eup_download(h, pops, eb) != EUP_OK) return die("eup_download", h);
@@ -246,6 +288,9 @@ int main(int argc, char** argv) {
     std::fclose(fprobe);
     std::fclose(fdrag);
     std::fclose(fmon);
+    for (FILE* f : fprof) std::fclose(f);
+    std::fclose(fvarm);
+    if (fcv) std::fclose(fcv);
     eup_destroy(h);
     return 0;
 }

@@ -119,6 +119,17 @@ template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g,
                            const Phys<R>& ph, int variant, cudaStream_t st);
 
+// Reference-form diagnostics (CODE/SRC/prof_*.F90, varm.F90, flux_X/flux_Y.F90):
+// a line of per-node u, w, v, den in R; per-plane means; the FP64 face sums of
+// the control-volume stresses of box = {i1, i2, j1, j2, k1, k2} (already clipped).
+template <typename S, typename R>
+void launch_line(const Lat<S, R>& L, const Geo& g, int axis, int c1, int c2, double* out, cudaStream_t st);
+template <typename S, typename R>
+void launch_plane_means(const Lat<S, R>& L, const Geo& g, int axis, double* out, cudaStream_t st);
+template <typename S, typename R>
+void launch_cv_drag(const Lat<S, R>& L, const Geo& g, const int box[6], R omega, const Reduce& red, double* out,
+                    cudaStream_t st);
+
 // FP64 sums over the fluid nodes of a region (device byte mask, one per node) into out[6].
 template <typename S, typename R>
 void launch_region_sums(const Lat<S, R>& L, const Geo& g, const Mask& mk, const uint8_t* region, const Reduce& red,

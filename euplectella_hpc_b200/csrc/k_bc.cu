@@ -432,6 +432,150 @@ __global__ void k_region_sums(Lat<S, R> L, Geo g, Mask mk, const uint8_t* region
     block_reduce_store<6>(s, red, out);
 }
 
+// ---- reference-form diagnostics: line profiles, plane means, control-volume drag ----------
+
+// Macroscopic values of one interior node in R, in the expression order of
+// CODE/SRC/prof_i.F90:45-79 (div = true: momentum / den) and
+// CODE/SRC/varm.F90:53-85 (div = false: momentum * (1 / den)).
+template <typename S, typename R>
+__device__ __forceinline__ void ref_macro(const Lat<S, R>& L, int64_t lin, bool div, R& den, R& u, R& w, R& v) {
+    R f[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = Store<S, R>::load(L.pop[q][lin], q, L.inv_scale);
+    const R r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] + f[12] + f[13] +
+                f[14] + f[15] + f[16] + f[17] + f[18];
+    const R mx = f[0] + f[1] + f[2] + f[3] + f[4] - f[9] - f[10] - f[11] - f[12] - f[13];
+    const R my = f[2] + f[6] + f[7] + f[8] + f[11] - f[0] - f[9] - f[15] - f[16] - f[17];
+    const R mz = f[3] + f[5] + f[6] + f[12] + f[17] - f[1] - f[8] - f[10] - f[14] - f[15];
+    den = r;
+    if (div) {
+        u = mx / r; w = my / r; v = mz / r;
+    } else {
+        const R ri = R(1) / r;
+        u = mx * ri; w = my * ri; v = mz * ri;
+    }
+}
+
+// prof_i / prof_j / prof_k (axis 0/1/2) at the two fixed coordinates c1, c2:
+// out[4t + 0..3] = u, w (y), v (z), den of the t-th node, computed in R.
+template <typename S, typename R>
+__global__ void k_line(Lat<S, R> L, Geo g, int axis, int c1, int c2, double* out) {
+    const int len = axis == 0 ? g.l : (axis == 1 ? g.m : g.n);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (t > len) return;
+    const int i = axis == 0 ? t : c1, j = axis == 1 ? t : (axis == 0 ? c1 : c2), k = axis == 2 ? t : c2;
+    R den, u, w, v;
+    ref_macro(L, g.lin(i, j, k), true, den, u, w, v);
+    out[4 * (t - 1) + 0] = (double)u;
+    out[4 * (t - 1) + 1] = (double)w;
+    out[4 * (t - 1) + 2] = (double)v;
+    out[4 * (t - 1) + 3] = (double)den;
+}
+
+// One block per plane normal to `axis` (CODE/SRC/varm.F90:42-98 for axis z):
+// FP64 sums of u, w, v (momentum times 1/den in R) and den over the plane's
+// nodes, a fixed thread assignment and tree, then divided by the node count.
+template <typename S, typename R>
+__global__ void k_plane_means(Lat<S, R> L, Geo g, int axis, double* out) {
+    const int pl = blockIdx.x;  // 0-based plane
+    const int64_t cnt = axis == 0 ? (int64_t)g.m * g.n : (axis == 1 ? (int64_t)g.l * g.n : g.lm);
+    double s[4] = {0, 0, 0, 0};
+    for (int64_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+        int64_t lin;
+        if (axis == 2) lin = (int64_t)pl * g.lm + t;
+        else if (axis == 0) lin = pl + (int64_t)g.l * t;                             // t = (j-1) + m (k-1)
+        else lin = (t % g.l) + (int64_t)g.l * (pl + (int64_t)g.m * (t / g.l));       // t = (i-1) + l (k-1)
+        R den, u, w, v;
+        ref_macro(L, lin, false, den, u, w, v);
+        s[0] += (double)u; s[1] += (double)w; s[2] += (double)v; s[3] += (double)den;
+    }
+    __shared__ double sh[32][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_down_sync(0xffffffffu, s[c], o);
+    if (lane == 0)
+        for (int c = 0; c < 4; ++c) sh[warp][c] = s[c];
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 4; ++c) {
+            double a = 0.0;
+            for (int wv = 0; wv < (int)(blockDim.x >> 5); ++wv) a += sh[wv][c];
+            out[4 * pl + c] = a / (double)cnt;
+        }
+}
+
+// Non-equilibrium stresses xx and xy of one node, CODE/SRC/flux_X.F90:162-240
+// and CODE/SRC/flux_Y.F90, in R and the reference's expression order.
+template <typename S, typename R>
+__device__ __forceinline__ void ref_stress(const Lat<S, R>& L, int64_t lin, R omega, R& sxx, R& sxy) {
+    R f[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = Store<S, R>::load(L.pop[q][lin], q, L.inv_scale);
+    const R one = R(1), rf = R(3), qf = R(1.5), tre = R(3);
+    const R p1 = Const<R>::p1(), p2 = Const<R>::p2();
+    const R rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] + f[12] +
+                  f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+    const R rhoinv = one / rho;
+    const R xj = (f[0] + f[1] + f[2] + f[3] + f[4] - f[9] - f[10] - f[11] - f[12] - f[13]) * rhoinv;
+    const R yj = (f[2] + f[6] + f[7] + f[8] + f[11] - f[0] - f[9] - f[15] - f[16] - f[17]) * rhoinv;
+    const R zj = (f[3] + f[5] + f[6] + f[12] + f[17] - f[1] - f[8] - f[10] - f[14] - f[15]) * rhoinv;
+    const R cvsq = xj * xj + yj * yj + zj * zj;
+    auto fe = [&](R w, R e, R sq) { return rho * w * (one + rf * e + qf * (tre * sq * sq - cvsq)); };
+    const R e[18] = {fe(p2, xj - yj, xj - yj),  fe(p2, xj - zj, xj - zj),  fe(p2, xj + yj, xj + yj),
+                     fe(p2, xj + zj, xj + zj),  fe(p1, xj, xj),            fe(p1, zj, zj),
+                     fe(p2, yj + zj, yj + zj),  fe(p1, yj, yj),            fe(p2, yj - zj, yj - zj),
+                     fe(p2, -xj - yj, xj + yj), fe(p2, -xj - zj, xj + zj), fe(p2, -xj + yj, xj - yj),
+                     fe(p2, -xj + zj, xj - zj), fe(p1, -xj, xj),           fe(p1, -zj, zj),
+                     fe(p2, -yj - zj, yj + zj), fe(p1, -yj, yj),           fe(p2, -yj + zj, yj - zj)};
+    const R visc = one - R(0.5) * omega;
+    R xx = -rho / rf, xy = R(0);
+#pragma unroll
+    for (int q = 0; q < 18; ++q) {
+        const R fn = f[q] - e[q];
+        xx = xx - visc * R(cx_of(q)) * R(cx_of(q)) * fn;
+        xy = xy - visc * R(cx_of(q)) * R(cy_of(q)) * fn;
+    }
+    sxx = xx;
+    sxy = xy;
+}
+
+// The four faces of a control volume, FP64 sums: face 0/1 x = i1/i2 (stress
+// xx over j1..j2, k1..k2), face 2/3 y = j1/j2 (stress xy over i1..i2, k1..k2).
+struct CvBox {
+    int i1, i2, j1, j2, k1, k2;
+};
+
+template <typename S, typename R>
+__global__ void k_cv_drag(Lat<S, R> L, Geo g, CvBox b, R omega, Reduce red, double* out) {
+    const int64_t nx = (int64_t)(b.j2 - b.j1 + 1) * (b.k2 - b.k1 + 1);
+    const int64_t ny = (int64_t)(b.i2 - b.i1 + 1) * (b.k2 - b.k1 + 1);
+    const int64_t total = 2 * nx + 2 * ny;
+    double s[4] = {0, 0, 0, 0};
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        int face, i, j, k;
+        if (t < 2 * nx) {
+            face = (int)(t / nx);
+            const int64_t r = t % nx;
+            i = face ? b.i2 : b.i1;
+            j = b.j1 + (int)(r % (b.j2 - b.j1 + 1));
+            k = b.k1 + (int)(r / (b.j2 - b.j1 + 1));
+        } else {
+            const int64_t u = t - 2 * nx;
+            face = 2 + (int)(u / ny);
+            const int64_t r = u % ny;
+            j = face == 3 ? b.j2 : b.j1;
+            i = b.i1 + (int)(r % (b.i2 - b.i1 + 1));
+            k = b.k1 + (int)(r / (b.i2 - b.i1 + 1));
+        }
+        R xx, xy;
+        ref_stress(L, g.lin(i, j, k), omega, xx, xy);
+        s[face] += face < 2 ? (double)xx : (double)xy;
+    }
+    block_reduce_store<4>(s, red, out);
+}
+
 // Population q of the seeded equilibrium state (init_eq.h) over the haloed
 // node range, into a staging buffer laid out like one host array.
 template <typename T>
@@ -586,6 +730,27 @@ void launch_region_sums(const Lat<S, R>& L, const Geo& g, const Mask& mk, const 
     k_region_sums<S, R><<<blocks, kTpb, 0, st>>>(L, g, mk, region, red, out);
 }
 
+template <typename S, typename R>
+void launch_line(const Lat<S, R>& L, const Geo& g, int axis, int c1, int c2, double* out, cudaStream_t st) {
+    const int len = axis == 0 ? g.l : (axis == 1 ? g.m : g.n);
+    k_line<S, R><<<(len + 127) / 128, 128, 0, st>>>(L, g, axis, c1, c2, out);
+}
+
+template <typename S, typename R>
+void launch_plane_means(const Lat<S, R>& L, const Geo& g, int axis, double* out, cudaStream_t st) {
+    const int len = axis == 0 ? g.l : (axis == 1 ? g.m : g.n);
+    k_plane_means<S, R><<<len, 256, 0, st>>>(L, g, axis, out);
+}
+
+template <typename S, typename R>
+void launch_cv_drag(const Lat<S, R>& L, const Geo& g, const int box[6], R omega, const Reduce& red, double* out,
+                    cudaStream_t st) {
+    const CvBox b{box[0], box[1], box[2], box[3], box[4], box[5]};
+    const int64_t total = 2 * (int64_t)(b.j2 - b.j1 + 1) * (b.k2 - b.k1 + 1) +
+                          2 * (int64_t)(b.i2 - b.i1 + 1) * (b.k2 - b.k1 + 1);
+    k_cv_drag<S, R><<<grid_for(total, kTpb, (unsigned)red.max_blocks), kTpb, 0, st>>>(L, g, b, omega, red, out);
+}
+
 template <typename T>
 void launch_init_population(T* staging, const Geo& g, int q, double u_in, double amp, uint64_t seed, cudaStream_t st) {
     const int64_t total = (int64_t)(g.l + 2) * (g.m + 2) * (g.n + 2);
@@ -618,6 +783,10 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
                                            const uint64_t*, int64_t, bool, const Reduce&, double*,     \
                                            int64_t, int64_t*, bool, cudaStream_t);                     \
     template void launch_fill_xface<S, R>(const Lat<S, R>&, const Geo&, cudaStream_t);                 \
+    template void launch_line<S, R>(const Lat<S, R>&, const Geo&, int, int, int, double*, cudaStream_t);   \
+    template void launch_plane_means<S, R>(const Lat<S, R>&, const Geo&, int, double*, cudaStream_t);     \
+    template void launch_cv_drag<S, R>(const Lat<S, R>&, const Geo&, const int*, R, const Reduce&, double*, \
+                                       cudaStream_t);                                                     \
     template void launch_region_sums<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const uint8_t*,   \
                                            const Reduce&, double*, cudaStream_t);                         \
     template void launch_monitor<S, R>(const Lat<S, R>&, const Geo&, const Mask&, const Reduce&,       \

@@ -185,6 +185,29 @@ int eup_get_cd_series(eup_handle* h, int64_t first_step, int32_t count, double* 
  * sum u^2}.  EUP_ERR_DIVERGED when any sum is not finite. */
 int eup_get_monitor(eup_handle* h, double out[5]);
 
+/* Line profile of CODE/SRC/prof_i.F90 (axis 0, nodes (1..l, c1, c2)),
+ * prof_j.F90 (axis 1, (c1, 1..m, c2)) and prof_k.F90 (axis 2, (c1, c2, 1..n)):
+ * out[4t .. 4t+3] = u, w (y velocity), v (z velocity), den of the t-th node,
+ * computed in the arithmetic type in the reference's expression order (so FP32
+ * and FP64 runs reproduce the reference's values exactly), widened to double. */
+int eup_get_line(eup_handle* h, int32_t axis, int32_t c1, int32_t c2, double* out);
+
+/* Means over every plane normal to `axis` of u, w, v and den, as
+ * CODE/SRC/varm.F90:42-98 computes them for axis 2 (u_med files): per-node
+ * values in the arithmetic type, sums in FP64 (the reference sums in mykind).
+ * out[4p .. 4p+3] for plane p = 0..extent-1.  All nodes count, solid ones too,
+ * as in the reference (values at solid voxels are not those of the reference:
+ * see eup_set_obstacles). */
+int eup_get_plane_means(eup_handle* h, int32_t axis, double* out);
+
+/* Control-volume drag of CODE/SRC/drag.F90:51-67: box = {xstart, xstop,
+ * ystart, ystop, zstart, zstop} (1-based, clipped to the lattice with the face
+ * weights of CODE/SRC/flux_X.F90:56-156); out[0] = fluxX (sigma_xx over the
+ * two x faces), out[1] = fluxY (sigma_xy over the two y faces).  Per-node
+ * stresses in the arithmetic type as CODE/SRC/flux_X.F90:162-240 writes them,
+ * face sums in FP64. */
+int eup_get_cv_drag(eup_handle* h, const int32_t box[6], double out[2]);
+
 /* FP64 sums over the fluid nodes whose byte in region (Fortran order, l*m*n,
  * nonzero = included) is set: out = {count, sum rho, sum ux, sum uy, sum uz,
  * sum u^2}.  Region means (the velocity inside a shell's cavity, a probe box)

@@ -66,6 +66,11 @@ def lib():
             getattr(L, f"orc_{pfx}_monitor").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_void_p, ctypes.c_void_p]
             getattr(L, f"orc_{pfx}_macro").argtypes = [ctypes.POINTER(Params), PP] + [ctypes.c_void_p] * 4
             getattr(L, f"orc_{pfx}_constants").argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p]
+            getattr(L, f"orc_{pfx}_line").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_int32, ctypes.c_int32,
+                                                      ctypes.c_int32, ctypes.c_void_p]
+            getattr(L, f"orc_{pfx}_plane_means").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_int32,
+                                                             ctypes.c_void_p]
+            getattr(L, f"orc_{pfx}_cv_drag").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_links.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p]
         L.orc_boundary_solid.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p]
         L.orc_boundary_solid.restype = ctypes.c_int64
@@ -167,6 +172,30 @@ def macro(p, a):
     getattr(lib(), f"orc_{_pfx(a)}_macro")(ctypes.byref(p), _ptrs(a), rho.ctypes.data, ux.ctypes.data,
                                            uy.ctypes.data, uz.ctypes.data)
     return rho, ux, uy, uz
+
+
+def line(p, a, axis, c1, c2) -> np.ndarray:
+    """prof_i/prof_j/prof_k line (axis 0/1/2): rows (u, w, v, den) per node, computed in the state's type."""
+    n = (p.l, p.m, p.n)[axis]
+    out = np.zeros((n, 4), dtype=np.float64)
+    getattr(lib(), f"orc_{_pfx(a)}_line")(ctypes.byref(p), _ptrs(a), axis, c1, c2, out.ctypes.data)
+    return out
+
+
+def plane_means(p, a, axis) -> np.ndarray:
+    """varm-style plane means (u, w, v, den) of every plane normal to axis, FP64 accumulation."""
+    n = (p.l, p.m, p.n)[axis]
+    out = np.zeros((n, 4), dtype=np.float64)
+    getattr(lib(), f"orc_{_pfx(a)}_plane_means")(ctypes.byref(p), _ptrs(a), axis, out.ctypes.data)
+    return out
+
+
+def cv_drag(p, a, box) -> np.ndarray:
+    """Control-volume drag (fluxX, fluxY) of the box (xstart, xstop, ystart, ystop, zstart, zstop)."""
+    b = np.ascontiguousarray(np.asarray(box, dtype=np.int32))
+    out = np.zeros(2, dtype=np.float64)
+    getattr(lib(), f"orc_{_pfx(a)}_cv_drag")(ctypes.byref(p), _ptrs(a), b.ctypes.data, out.ctypes.data)
+    return out
 
 
 def links(p, obs) -> np.ndarray:

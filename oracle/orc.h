@@ -59,7 +59,13 @@ typedef struct orc_params {
     void orc_##P##_monitor(const orc_params* p, REAL* const a[19], const int32_t* obs,    \
                            double out[5]);                                                \
     void orc_##P##_macro(const orc_params* p, REAL* const a[19], double* rho,             \
-                         double* ux, double* uy, double* uz);
+                         double* ux, double* uy, double* uz);                             \
+    void orc_##P##_line(const orc_params* p, REAL* const a[19], int32_t axis, int32_t c1, \
+                        int32_t c2, double* out);                                         \
+    void orc_##P##_plane_means(const orc_params* p, REAL* const a[19], int32_t axis,      \
+                               double* out);                                              \
+    void orc_##P##_cv_drag(const orc_params* p, REAL* const a[19], const int32_t box[6],  \
+                           double out[2]);
 
 ORC_DECLARE(f, float)
 ORC_DECLARE(d, double)

@@ -647,6 +647,155 @@ void FN(macro)(const orc_params* p, REAL* const a[19], double* rho, double* ux, 
             }
 }
 
+/* Macroscopic values of one node in REAL, in the expression order of
+ * CODE/SRC/prof_i.F90:45-79 (and varm.F90:53-85): den = a01+...+a19, momentum
+ * sums as written there; velocity = momentum/den (div != 0) or
+ * momentum*(1/den) (div == 0, varm's rhoinv). */
+static void CAT(ref_macro_, P, )(REAL* const a[19], int64_t x, int div, REAL* den, REAL* u, REAL* w, REAL* v)
+{
+    const REAL r = a[0][x] + a[1][x] + a[2][x] + a[3][x] + a[4][x] + a[5][x] + a[6][x] + a[7][x] + a[8][x] +
+                   a[9][x] + a[10][x] + a[11][x] + a[12][x] + a[13][x] + a[14][x] + a[15][x] + a[16][x] +
+                   a[17][x] + a[18][x];
+    const REAL mx = a[0][x] + a[1][x] + a[2][x] + a[3][x] + a[4][x] - a[9][x] - a[10][x] - a[11][x] - a[12][x] - a[13][x];
+    const REAL my = a[2][x] + a[6][x] + a[7][x] + a[8][x] + a[11][x] - a[0][x] - a[9][x] - a[15][x] - a[16][x] - a[17][x];
+    const REAL mz = a[3][x] + a[5][x] + a[6][x] + a[12][x] + a[17][x] - a[1][x] - a[8][x] - a[10][x] - a[14][x] - a[15][x];
+    *den = r;
+    if (div) {
+        *u = mx / r; *w = my / r; *v = mz / r;
+    } else {
+        const REAL ri = UNO / r;
+        *u = mx * ri; *w = my * ri; *v = mz * ri;
+    }
+}
+
+/* Line profile of CODE/SRC/prof_i.F90 (axis 0, at j = c1, k = c2),
+ * prof_j.F90 (axis 1, i = c1, k = c2), prof_k.F90 (axis 2, i = c1, j = c2):
+ * out[4t + 0..3] = u, w (y), v (z), den of the t-th node, computed in REAL. */
+void FN(line)(const orc_params* p, REAL* const a[19], int32_t axis, int32_t c1, int32_t c2, double* out)
+{
+    DECL_SIZES(p);
+    const int len = axis == 0 ? l : (axis == 1 ? m : n);
+    for (int t = 1; t <= len; ++t) {
+        const int i = axis == 0 ? t : c1, j = axis == 1 ? t : (axis == 0 ? c1 : c2), k = axis == 2 ? t : c2;
+        REAL den, u, w, v;
+        CAT(ref_macro_, P, )(a, IDX(i, j, k), 1, &den, &u, &w, &v);
+        out[4 * (t - 1) + 0] = u; out[4 * (t - 1) + 1] = w; out[4 * (t - 1) + 2] = v; out[4 * (t - 1) + 3] = den;
+    }
+}
+
+/* Plane means of CODE/SRC/varm.F90:42-98 generalised to any axis: for every
+ * plane normal to `axis`, the mean over its nodes of u, w, v (momentum times
+ * 1/den in REAL) and den, accumulated in FP64 (the reference accumulates in
+ * mykind).  out[4p + 0..3]. */
+void FN(plane_means)(const orc_params* p, REAL* const a[19], int32_t axis, double* out)
+{
+    DECL_SIZES(p);
+    const int len = axis == 0 ? l : (axis == 1 ? m : n);
+    for (int q = 0; q < 4 * len; ++q) out[q] = 0.0;
+    for (int k = 1; k <= n; ++k)
+        for (int j = 1; j <= m; ++j)
+            for (int i = 1; i <= l; ++i) {
+                const int pl = (axis == 0 ? i : (axis == 1 ? j : k)) - 1;
+                REAL den, u, w, v;
+                CAT(ref_macro_, P, )(a, IDX(i, j, k), 0, &den, &u, &w, &v);
+                out[4 * pl + 0] += u; out[4 * pl + 1] += w; out[4 * pl + 2] += v; out[4 * pl + 3] += den;
+            }
+    const double cnt = axis == 0 ? (double)m * n : (axis == 1 ? (double)l * n : (double)l * m);
+    for (int q = 0; q < 4 * len; ++q) out[q] /= cnt;
+}
+
+/* Non-equilibrium stress of one node, CODE/SRC/flux_X.F90:162-240 (xx) and
+ * CODE/SRC/flux_Y.F90 (xy), in REAL and the reference's expression order. */
+static void CAT(ref_stress_, P, )(REAL* const a[19], int64_t x, REAL omega, REAL* sxx, REAL* sxy)
+{
+    static const int cxl[18] = {1, 1, 1, 1, 1, 0, 0, 0, 0, -1, -1, -1, -1, -1, 0, 0, 0, 0};
+    static const int cyl[18] = {-1, 0, 1, 0, 0, 0, 1, 1, 1, -1, 0, 1, 0, 0, 0, -1, -1, -1};
+    REAL f[19];
+    for (int q = 0; q < 19; ++q) f[q] = a[q][x];
+    const REAL rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] + f[12] +
+                     f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+    const REAL rhoinv = UNO / rho;
+    const REAL xj = (f[0] + f[1] + f[2] + f[3] + f[4] - f[9] - f[10] - f[11] - f[12] - f[13]) * rhoinv;
+    const REAL yj = (f[2] + f[6] + f[7] + f[8] + f[11] - f[0] - f[9] - f[15] - f[16] - f[17]) * rhoinv;
+    const REAL zj = (f[3] + f[5] + f[6] + f[12] + f[17] - f[1] - f[8] - f[10] - f[14] - f[15]) * rhoinv;
+    const REAL cvsq = xj * xj + yj * yj + zj * zj;
+    /* rho*w*(1 + rf*e + qf*(3*s*s - cvsq)) with e the signed and s the squared combination */
+#define FE(w, e, s) (rho * (w) * (UNO + RF * (e) + QF * (TRE * (s) * (s) - cvsq)))
+    REAL fe[18];
+    fe[0] = FE(P2, xj - yj, xj - yj);
+    fe[1] = FE(P2, xj - zj, xj - zj);
+    fe[2] = FE(P2, xj + yj, xj + yj);
+    fe[3] = FE(P2, xj + zj, xj + zj);
+    fe[4] = FE(P1, xj, xj);
+    fe[5] = FE(P1, zj, zj);
+    fe[6] = FE(P2, yj + zj, yj + zj);
+    fe[7] = FE(P1, yj, yj);
+    fe[8] = FE(P2, yj - zj, yj - zj);
+    fe[9] = FE(P2, -xj - yj, xj + yj);
+    fe[10] = FE(P2, -xj - zj, xj + zj);
+    fe[11] = FE(P2, -xj + yj, xj - yj);
+    fe[12] = FE(P2, -xj + zj, xj - zj);
+    fe[13] = FE(P1, -xj, xj);
+    fe[14] = FE(P1, -zj, zj);
+    fe[15] = FE(P2, -yj - zj, yj + zj);
+    fe[16] = FE(P1, -yj, yj);
+    fe[17] = FE(P2, -yj + zj, yj - zj);
+#undef FE
+    const REAL visc = UNO - (REAL)0.5 * omega;
+    REAL xx = -rho / RF, xy = ZERO;
+    for (int q = 0; q < 18; ++q) {
+        const REAL fn = f[q] - fe[q];
+        xx = xx - visc * (REAL)cxl[q] * (REAL)cxl[q] * fn;
+        xy = xy - visc * (REAL)cxl[q] * (REAL)cyl[q] * fn;
+    }
+    *sxx = xx;
+    *sxy = xy;
+}
+
+/* Control-volume drag of CODE/SRC/drag.F90:51-67 through flux_X.F90 and
+ * flux_Y.F90 (serial: offsets 0) for the box box[6] = {xstart, xstop, ystart,
+ * ystop, zstart, zstop}: the stresses summed in FP64 over the box faces
+ * (the reference sums in mykind).  out = {fluxX, fluxY}. */
+void FN(cv_drag)(const orc_params* p, REAL* const a[19], const int32_t box[6], double out[2])
+{
+    DECL_SIZES(p);
+    REAL omega, fgrad;
+    FN(constants)(p, &omega, &fgrad);
+    int lo[3], hi[3], nrm[3][2], ok[3];
+    const int ext[3] = {l, m, n};
+    for (int d = 0; d < 3; ++d) {
+        const int s0 = box[2 * d], s1 = box[2 * d + 1];
+        nrm[d][0] = nrm[d][1] = 1;
+        ok[d] = 1;
+        if (s0 > 0 && s1 <= ext[d]) { lo[d] = s0; hi[d] = s1; }
+        else if (s0 > 0 && s1 > ext[d]) { lo[d] = s0; hi[d] = ext[d]; nrm[d][1] = 0; }
+        else if (s0 <= 0 && s1 <= ext[d]) { lo[d] = 1; hi[d] = s1; nrm[d][0] = 0; }
+        else ok[d] = 0;
+        if (s0 > ext[d] || s1 < 0) ok[d] = 0;
+    }
+    out[0] = out[1] = 0.0;
+    if (!(ok[0] && ok[1] && ok[2])) return;
+    double fx[2] = {0.0, 0.0}, fy[2] = {0.0, 0.0};
+    for (int f = 0; f < 2; ++f) {
+        const int i0 = f ? hi[0] : lo[0];
+        for (int k = lo[2]; k <= hi[2]; ++k)
+            for (int j = lo[1]; j <= hi[1]; ++j) {
+                REAL xx, xy;
+                CAT(ref_stress_, P, )(a, IDX(i0, j, k), omega, &xx, &xy);
+                fx[f] += xx;
+            }
+        const int j0 = f ? hi[1] : lo[1];
+        for (int k = lo[2]; k <= hi[2]; ++k)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+                REAL xx, xy;
+                CAT(ref_stress_, P, )(a, IDX(i, j0, k), omega, &xx, &xy);
+                fy[f] += xy;
+            }
+    }
+    out[0] = -fx[0] * nrm[0][0] + fx[1] * nrm[0][1];
+    out[1] = fy[0] * nrm[1][0] + fy[1] * nrm[1][1];
+}
+
 #undef RF
 #undef QF
 #undef UNO

@@ -24,7 +24,7 @@ def test_driver_runs_reference_inputs(eup, orc, require_gpu, tmp_path):
         "&parameters\n lx = 40\n ly = 24\n lz = 12\n proc_x = 1\n proc_y = 1\n proc_z = 1\n"
         " svisc=0.01,0.005\n u0=0.05\n itfin=140\n ivtim=1000\n isignal=20\n itsave=20\n icheck=10\n"
         " tstep=10\n irestart=1\n flag1=1\n flag2=2\n flag3=0\n init_v=0        /\n")
-    r = subprocess.run([DRIVER, "--preset", "cylinder_inf", "--drag-length", "7"], cwd=tmp_path,
+    r = subprocess.run([DRIVER, "--preset", "cylinder_inf", "--drag-length", "7", "--cv-drag"], cwd=tmp_path,
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     # oracle with the CYLINDER_INF flags (in/out x, periodic y and z), u_inflow = u0
@@ -48,6 +48,25 @@ def test_driver_runs_reference_inputs(eup, orc, require_gpu, tmp_path):
     for row in rows:
         np.testing.assert_allclose(row[1:4], forces[int(row[0])], rtol=1e-12, atol=1e-14)
         assert abs(row[4] - row[1] / (0.5 * 0.05 ** 2 * 7 * n)) <= 1e-12 * abs(row[4])
+    # profiles and plane means of the last check (t = 140) against the oracle's final state,
+    # to the 6 significant digits of the e14.6 format (half a unit of the 6th digit: 5e-6 relative)
+    def last_block(name):
+        text = (tmp_path / name).read_text()
+        blk = text.split("# t=")[-1].split("\n")
+        assert int(blk[0]) == 140
+        return np.array([list(map(float, ln.split())) for ln in blk[1:] if ln.strip()])
+    for ax, fname, (c1, c2) in ((0, "prof_i.0000.dat", (m // 2, n // 2)), (1, "prof_j.0000.dat", (l // 2, n // 2)),
+                                (2, "prof_k.0000.dat", (l // 2, m // 2))):
+        rows_ = last_block(fname)
+        want = orc.line(p, ref, ax, c1, c2)
+        assert rows_.shape == (want.shape[0], 5)
+        fluid = [obs[c2 - 1, c1 - 1, :], obs[c2 - 1, :, c1 - 1], obs[:, c2 - 1, c1 - 1]][ax] == 0
+        bad = ~np.isclose(rows_[fluid, 1:], want[fluid], rtol=5e-6, atol=1e-12)
+        assert not bad.any(), (fname, np.argwhere(bad)[:5].tolist(), rows_[fluid][bad.any(1)][:3].tolist(),
+                               want[fluid][bad.any(1)][:3].tolist())
+    assert last_block("u_med.000.000.000.dat").shape == (n, 5)
+    cv = [ln.split() for ln in (tmp_path / "drag.0000.dat").read_text().split("\n") if ln.strip()]
+    assert len(cv) == 4 * 4 and [int(c[0]) for c in cv[:4]] == [52, 57, 62, 67]
     probe = (tmp_path / "probe_g.0000.dat").read_text().split("\n")[0]
     assert probe.startswith("     110") and "E" in probe
     assert "Mlups" in (tmp_path / "bgk.perf").read_text()

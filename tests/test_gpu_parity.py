@@ -170,6 +170,39 @@ def test_device_init_equals_host_init_upload(eup, require_gpu, prec):
     assert np.array_equal(got[0][0], got[1][0])
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_reference_diagnostics_match_oracle(eup, orc, require_gpu, prec):
+    """prof_i/j/k lines (exact), varm plane means and the control-volume drag (FP64 sums)."""
+    dtype, code = (np.float32, eup.FP32) if prec == "fp32" else (np.float64, eup.FP64)
+    # lid-driven box without obstacles: every node is fluid, so lines and planes compare everywhere
+    name, (l, m, n), bc, svisc, u0, uin, u00, builder = CASES[3]
+    a = eup.init_equilibrium(l, m, n, 0.02, 1e-3, 21, dtype)
+    p = orc.params(l, m, n, bc, svisc=svisc, u0=u0, u_inflow=uin, u00=u00)
+    with eup.Solver(eup.Config(l, m, n, bc=bc, svisc=svisc, u0=u0, u_inflow=uin, u00=u00, precision=code)) as s:
+        s.upload(a)
+        s.step(7)
+        lines = [s.line(0, m // 2, n // 2), s.line(1, l // 2, n // 2), s.line(2, l // 2, m // 2)]
+        planes = [s.plane_means(ax) for ax in range(3)]
+    orc.run(p, a, None, 7)
+    for ax, (c1, c2) in enumerate(((m // 2, n // 2), (l // 2, n // 2), (l // 2, m // 2))):
+        assert np.array_equal(lines[ax], orc.line(p, a, ax, c1, c2))
+        np.testing.assert_allclose(planes[ax], orc.plane_means(p, a, ax), rtol=1e-12, atol=1e-15)
+    # control volume around the cylinder of the inflow/outflow case, one box clipped by the lattice
+    name, (l, m, n), bc, svisc, u0, uin, u00, builder = CASES[0]
+    obs = builder(l, m, n)
+    a = eup.init_equilibrium(l, m, n, uin, 1e-3, 22, dtype)
+    p = orc.params(l, m, n, bc, svisc=svisc, u_inflow=uin)
+    boxes = [(3, 14, 3, 13, 1, n), (0, 14, 3, 13, 2, n - 1), (5, l + 3, 2, m, 1, n)]
+    with eup.Solver(eup.Config(l, m, n, bc=bc, svisc=svisc, u_inflow=uin, precision=code)) as s:
+        s.set_obstacles(obs)
+        s.upload(a)
+        s.step(9)
+        got = [s.cv_drag(b) for b in boxes]
+    orc.run(p, a, obs, 9)
+    for b, g in zip(boxes, got):
+        np.testing.assert_allclose(g, orc.cv_drag(p, a, b), rtol=1e-12, atol=1e-13)
+
+
 def test_region_sums_match_oracle(eup, orc, require_gpu):
     case = CASES[0]
     name, (l, m, n), bc, svisc, u0, uin, u00, builder = case
