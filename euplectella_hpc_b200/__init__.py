@@ -39,7 +39,7 @@ EXPORTED = [
     "eup_read_raw_state", "eup_write_raw_state", "eup_init_equilibrium", "eup_geometry_cylinder_z",
     "eup_geometry_reticular_shell", "eup_mem_force_noalloc", "eup_set_solid_fraction", "eup_adjoint_run",
     "eup_geometry_ridged_shell", "eup_get_region_sums", "eup_init_state", "eup_get_line", "eup_get_plane_means",
-    "eup_get_cv_drag",
+    "eup_get_cv_drag", "eup_save_state", "eup_restore_state",
 ]
 
 
@@ -107,6 +107,8 @@ def _load():
         "eup_get_line": ([vp, i32, i32, i32, vp], ctypes.c_int),
         "eup_get_plane_means": ([vp, i32, vp], ctypes.c_int),
         "eup_get_cv_drag": ([vp, vp, vp], ctypes.c_int),
+        "eup_save_state": ([vp, ctypes.c_char_p, i32], ctypes.c_int),
+        "eup_restore_state": ([vp, ctypes.c_char_p, i32], ctypes.c_int),
         "eup_adjoint_run": ([vp, ctypes.POINTER(AdjointConfig), ctypes.POINTER(dbl), vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -289,6 +291,14 @@ class Solver:
     def init_state(self, u_in, amp, seed, itime=0):
         """Seeded equilibrium state generated on the device (same bits as upload(init_equilibrium(...)))."""
         self._ck(lib.eup_init_state(self._h, float(u_in), float(amp), int(seed), int(itime)))
+
+    def save_state(self, path, elem_bytes=4):
+        """Checkpoint in the reference's raw format straight from the device."""
+        self._ck(lib.eup_save_state(self._h, os.fsencode(str(path)), elem_bytes))
+
+    def restore_state(self, path, elem_bytes=4):
+        """Restart from a file in the reference's raw format (sets the step counter)."""
+        self._ck(lib.eup_restore_state(self._h, os.fsencode(str(path)), elem_bytes))
 
     def line(self, axis, c1, c2) -> np.ndarray:
         """prof_i/prof_j/prof_k line (axis 0/1/2) at the fixed coordinates c1, c2: rows (u, w, v, den)."""

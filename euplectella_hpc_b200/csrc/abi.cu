@@ -50,6 +50,9 @@ struct eup_handle {
     std::string err;
 };
 
+bool eup_internal_read_record(FILE* f, void* dst, int64_t want, std::string* why);
+bool eup_internal_write_record(FILE* f, const void* src, int64_t bytes);
+
 namespace {
 
 thread_local std::string g_err;
@@ -295,6 +298,22 @@ void probes_dispatch(eup_handle* h, int npts, const int32_t* d_ijk, double* d_ou
     launch_probes<S, R>(make_lat<S, R>(h, h->cur), h->g, npts, d_ijk, d_out, h->stream);
 }
 
+// After the 19 populations of a new state are on the device: step counter,
+// x-face copy, and the force of the state (CODE/SRC/bgk3d.F90 records the drag
+// of every state reached, the initial one included).
+int finish_state(eup_handle* h, int64_t itime) {
+    CK(h, cudaMemcpyAsync(h->d_itime, &itime, sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
+    DISPATCH(h, fill_xface_dispatch, h);
+    h->itime = itime;
+    h->series_first = itime;
+    h->has_state = true;
+    if (h->pbb) CK(h, cudaMemsetAsync(h->series + 3 * (itime % h->cap), 0, 3 * sizeof(double), h->stream));
+    else DISPATCH(h, enqueue_drag_only, h);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
 int ensure_staging(eup_handle* h, size_t bytes) {
     if (h->staging_bytes >= bytes) return EUP_OK;
     if (h->staging) cudaFree(h->staging);
@@ -486,16 +505,7 @@ int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, in
         CK(h, cudaMemcpyAsync(h->staging, pops[q], bytes, cudaMemcpyHostToDevice, h->stream));
         DISPATCH(h, upload_q, h, q, elem_bytes);
     }
-    CK(h, cudaMemcpyAsync(h->d_itime, &itime, sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
-    DISPATCH(h, fill_xface_dispatch, h);
-    h->itime = itime;
-    h->series_first = itime;
-    h->has_state = true;
-    if (h->pbb) CK(h, cudaMemsetAsync(h->series + 3 * (itime % h->cap), 0, 3 * sizeof(double), h->stream));
-    else DISPATCH(h, enqueue_drag_only, h);
-    CK(h, cudaGetLastError());
-    CK(h, cudaStreamSynchronize(h->stream));
-    return EUP_OK;
+    return finish_state(h, itime);
 }
 
 int eup_init_state(eup_handle* h, double u_in, double amp, uint64_t seed, int64_t itime) {
@@ -511,16 +521,75 @@ int eup_init_state(eup_handle* h, double u_in, double amp, uint64_t seed, int64_
         else launch_init_population<float>(static_cast<float*>(h->staging), g, q, u_in, amp, seed, h->stream);
         DISPATCH(h, upload_q, h, q, eb);
     }
-    CK(h, cudaMemcpyAsync(h->d_itime, &itime, sizeof(int64_t), cudaMemcpyHostToDevice, h->stream));
-    DISPATCH(h, fill_xface_dispatch, h);
-    h->itime = itime;
-    h->series_first = itime;
-    h->has_state = true;
-    if (h->pbb) CK(h, cudaMemsetAsync(h->series + 3 * (itime % h->cap), 0, 3 * sizeof(double), h->stream));
-    else DISPATCH(h, enqueue_drag_only, h);
-    CK(h, cudaGetLastError());
-    CK(h, cudaStreamSynchronize(h->stream));
-    return EUP_OK;
+    return finish_state(h, itime);
+}
+
+int eup_save_state(eup_handle* h, const char* path, int32_t elem_bytes) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!path || (elem_bytes != 4 && elem_bytes != 8))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_save_state: need a path and elem_bytes 4 or 8");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_save_state: no state uploaded");
+    if (h->itime > 2147483647LL) return fail(h, EUP_ERR_UNSUPPORTED, "eup_save_state: itime beyond int32");
+    const Geo& g = h->g;
+    const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * elem_bytes;
+    if ((rc = ensure_staging(h, bytes))) return rc;
+    void* pinned = nullptr;
+    CK(h, cudaMallocHost(&pinned, bytes));
+    FILE* f = std::fopen(path, "wb");
+    int out = EUP_OK;
+    const int32_t it = (int32_t)h->itime;
+    if (!f) out = fail(h, EUP_ERR_IO, std::string("eup_save_state: cannot create ") + path);
+    else if (!eup_internal_write_record(f, &it, 4)) out = fail(h, EUP_ERR_IO, "eup_save_state: write failed");
+    for (int q = 0; q < Q && out == EUP_OK; ++q) {
+        DISPATCH(h, download_q, h, q, elem_bytes);
+        cudaError_t e = cudaMemcpyAsync(pinned, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) out = cuda_fail(h, e, "eup_save_state");
+        else if (!eup_internal_write_record(f, pinned, (int64_t)bytes))
+            out = fail(h, EUP_ERR_IO, "eup_save_state: write failed (records over 2 GiB are not supported)");
+    }
+    if (f) std::fclose(f);
+    cudaFreeHost(pinned);
+    return out;
+}
+
+int eup_restore_state(eup_handle* h, const char* path, int32_t elem_bytes) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!path || (elem_bytes != 4 && elem_bytes != 8))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_restore_state: need a path and elem_bytes 4 or 8");
+    const Geo& g = h->g;
+    const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * elem_bytes;
+    if ((rc = ensure_staging(h, bytes))) return rc;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(h, EUP_ERR_IO, std::string("eup_restore_state: cannot open ") + path);
+    void* pinned = nullptr;
+    cudaError_t e = cudaMallocHost(&pinned, bytes);
+    if (e != cudaSuccess) {
+        std::fclose(f);
+        return cuda_fail(h, e, "cudaMallocHost");
+    }
+    int out = EUP_OK;
+    int32_t it = 0;
+    std::string why;
+    if (!eup_internal_read_record(f, &it, 4, &why)) out = fail(h, EUP_ERR_IO, "eup_restore_state: itime: " + why);
+    for (int q = 0; q < Q && out == EUP_OK; ++q) {
+        if (!eup_internal_read_record(f, pinned, (int64_t)bytes, &why)) {
+            out = fail(h, EUP_ERR_IO, "eup_restore_state: population " + std::to_string(q + 1) + ": " + why);
+            break;
+        }
+        e = cudaMemcpyAsync(h->staging, pinned, bytes, cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) {
+            DISPATCH(h, upload_q, h, q, elem_bytes);
+            e = cudaStreamSynchronize(h->stream);  // the pinned buffer is refilled next
+        }
+        if (e != cudaSuccess) out = cuda_fail(h, e, "eup_restore_state");
+    }
+    std::fclose(f);
+    cudaFreeHost(pinned);
+    if (out != EUP_OK) return out;
+    return finish_state(h, it);
 }
 
 int eup_download(eup_handle* h, void* const pops[19], int32_t elem_bytes) {

@@ -80,6 +80,12 @@ inline double seg_dist(double u, double s, double u0, double s0, double u1, doub
 
 }  // namespace
 
+// Fortran sequential-record helpers for the device-side checkpoint entry points.
+bool eup_internal_read_record(FILE* f, void* dst, int64_t want, std::string* why) {
+    return read_record(f, dst, want, *why);
+}
+bool eup_internal_write_record(FILE* f, const void* src, int64_t bytes) { return write_record(f, src, bytes); }
+
 extern "C" {
 
 int eup_read_obs_file(const char* path, int32_t l, int32_t m, int32_t n, int32_t* obs, int64_t* nobs) {

@@ -127,6 +127,17 @@ int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, in
  * reference initialises on the host, CODE/SRC/init.F90). */
 int eup_init_state(eup_handle* h, double u_in, double amp, uint64_t seed, int64_t itime);
 
+/* Checkpoint files in the reference's raw format (CODE/SRC/save_raw.F90:41-78,
+ * restore_raw.F90:34-63: a record holding itime as int32, then 19 records of
+ * the haloed arrays, elem_bytes 4 or 8, gfortran 4-byte record markers)
+ * written from and read into the device state directly, one population at a
+ * time through a pinned buffer, with no 19-array host copy: 16-bit storage is
+ * expanded to float/double on the way out.  Records over 2 GiB (a population
+ * beyond 2^29 FP32 nodes) are rejected.  eup_restore_state sets the step
+ * counter from the file. */
+int eup_save_state(eup_handle* h, const char* path, int32_t elem_bytes);
+int eup_restore_state(eup_handle* h, const char* path, int32_t elem_bytes);
+
 /* Copies the current state back into 19 haloed host arrays: the interior from
  * the lattice, the halo from the halo shell, exactly what the reference's
  * arrays hold after a step.  Replaces the device-to-host copies of

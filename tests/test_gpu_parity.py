@@ -203,6 +203,32 @@ def test_reference_diagnostics_match_oracle(eup, orc, require_gpu, prec):
         np.testing.assert_allclose(g, orc.cv_drag(p, a, b), rtol=1e-12, atol=1e-13)
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_device_checkpoint_round_trip(eup, require_gpu, tmp_path, prec):
+    """eup_save_state writes what download + write_raw_state would; eup_restore_state
+    continues the run exactly."""
+    l, m, n = 36, 16, 10
+    code = eup.FP32 if prec == "fp32" else eup.FP16_DEV
+    obs = _cyl(l, m, n)
+    cfg = eup.Config(l, m, n, bc=(5, 4, 3, 3, 0, 0), svisc=0.01, u_inflow=0.05, precision=code)
+    with eup.Solver(cfg) as s:
+        s.set_obstacles(obs)
+        s.init_state(0.05, 1e-3, 31, itime=40)
+        s.step(6)
+        s.save_state(tmp_path / "save.bin")
+        ref = s.download(np.float32)
+        s.step(5)
+        ref_next = s.download(np.float32)
+    got, it = eup.read_raw_state(tmp_path / "save.bin", l, m, n)
+    assert it == 46 and np.array_equal(got, ref)
+    with eup.Solver(cfg) as s:
+        s.set_obstacles(obs)
+        s.restore_state(tmp_path / "save.bin")
+        assert s.itime == 46
+        s.step(5)
+        assert np.array_equal(s.download(np.float32), ref_next)
+
+
 def test_region_sums_match_oracle(eup, orc, require_gpu):
     case = CASES[0]
     name, (l, m, n), bc, svisc, u0, uin, u00, builder = case
