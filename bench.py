@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
+    ap.add_argument("--decomp", choices=["slabs", "replicas"], default="slabs",
+                    help="N > 1: x-slabs of one channel with the plane exchange every step (default), or "
+                         "independent replicas")
     return ap.parse_args()
 
 
@@ -307,10 +310,121 @@ def run_eup(args):
     return 0
 
 
+def run_slabs(args):
+    """N > 1, one process per GPU: a channel N times as long as the single-GPU workload, cut into
+    N x-slabs (each holding one copy of the body, so the per-GPU work is the single-GPU
+    workload's: weak scaling), stepped with the NCCL plane exchange between the halves of every
+    step.  Timed with CUDA events on each slab's stream, max over ranks."""
+    import dataclasses as dc
+
+    import torch
+    import torch.distributed as dist
+    import euplectella_hpc_b200 as E
+    from euplectella_hpc_b200.slabs import DistTransport, SlabSolver
+
+    world = int(os.environ["WORLD_SIZE"])
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    prec_code, sbytes, dtype_name = PRECISIONS[args.precision]
+    wl = make_workload(args.workload, prec_code)
+    gcfg = dc.replace(wl.cfg, lx=wl.cfg.lx * world, device=local)
+    slab = SlabSolver(gcfg, rank, world, DistTransport(rank, world))
+    assert slab.nx == wl.cfg.lx
+    s = slab.solver
+    s.set_obstacles(wl.obs)
+    s.init_state(0.05, 1e-4, wl.seed + rank)
+    slab.step(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = s.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(slab.stream)
+    slab.step(args.steps)
+    ev1.record(slab.stream)
+    ev1.synchronize()
+    launches = s.launches - launches0
+    t = torch.tensor([ev0.elapsed_time(ev1)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    # stream-collide share: events around the second half of each step (unpack of the received
+    # planes, stream-collide, force of the new state)
+    ms_end = 0.0
+    for _ in range(min(args.steps, 50)):
+        slab.begin()
+        slab.exchange()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(slab.stream)
+        slab.end()
+        a1.record(slab.stream)
+        a1.synchronize()
+        ms_end += a0.elapsed_time(a1)
+    clk = clocks.stop()
+    k_ms = ms_end / min(args.steps, 50)
+    nodes = wl.nodes
+    achieved = 2 * 19 * sbytes * nodes / (k_ms / 1e3) / 1e9
+    peak, peak_src = measured_peak()
+    tpn = traffic_per_node(args.precision)
+    value = world * nodes * args.steps / (t_ms / 1e3) / 1e6
+    e2e = None
+    if not args.no_e2e:
+        hdt = torch.float64 if args.precision == "fp64" else torch.float32
+        eb = 8 if args.precision == "fp64" else 4
+        host = torch.empty(s.shape, dtype=hdt, pin_memory=True)
+        hnp = host.numpy()
+        E.lib.eup_init_equilibrium(wl.cfg.lx, wl.cfg.ly, wl.cfg.lz, 0.05, 1e-4, wl.seed + rank, eb, E._ptrs(hnp))
+        ptrs = [hnp[q].ctypes.data for q in range(19)]
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(slab.stream)
+        s.upload_ptrs(ptrs, eb, itime=0)
+        for _ in range(args.steps):
+            slab.step(1)
+            slab.forces()
+        s.download_ptrs(ptrs, eb)
+        e1.record(slab.stream)
+        e1.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e_ms = float(te.item())
+        e2e = {"value": world * nodes * args.steps / (e_ms / 1e3) / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": world * hnp.nbytes / args.steps,
+               "d2h_bytes_per_step": world * (hnp.nbytes + 24 * args.steps) / args.steps, "ms_total": e_ms,
+               "path": "per slab: eup_upload(pinned) + K x (boundaries, NCCL plane exchange, stream, "
+                       "all-reduced force) + eup_download"}
+    f = slab.forces()
+    if rank == 0:
+        c = wl.cfg
+        line = {"metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": dtype_name, "data": "synthetic",
+                "config": {"workload": f"{wl.name} x{world} in series", "lattice": [c.lx * world, c.ly, c.lz],
+                           "nodes": nodes * world, "precision": args.precision, "bc": list(gcfg.bc),
+                           "svisc": c.svisc, "l2_flush": "inputs larger than L2",
+                           "parallelism": f"x-slabs x{world}, NCCL plane exchange every step"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": (tpn * nodes if tpn is not None else None),
+                             "kernel": "k_stream_collide_pair (+ plane unpack and force of the step)",
+                             "kernel_ms": k_ms, "peak_source": peak_src},
+                "e2e": e2e, "cpu_baseline": None, "clocks": clk, "gpu_launches": launches,
+                "drag": {"fx": float(f[0]), "itime": s.itime}}
+        print(json.dumps(line), flush=True)
+    s.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.decomp == "slabs":
+        return run_slabs(args)
     return run_eup(args)
 
 

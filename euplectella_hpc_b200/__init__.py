@@ -23,7 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libeup.so")
 
 # Boundary flag codes (CODE/SRC/build.bcond.F90:11-17) and face order.
-PERIODIC, NOSLIP, LID, FREESLIP, INFLOW, OUTFLOW = range(6)
+PERIODIC, NOSLIP, LID, FREESLIP, INFLOW, OUTFLOW, EXCHANGE = range(7)
 FRONT, REAR, RIGHT, LEFT, UP, DOWN = range(6)
 # Precision modes.
 FP32, FP64, FP16_DEV, BF16_DEV = range(4)
@@ -39,7 +39,8 @@ EXPORTED = [
     "eup_read_raw_state", "eup_write_raw_state", "eup_init_equilibrium", "eup_geometry_cylinder_z",
     "eup_geometry_reticular_shell", "eup_mem_force_noalloc", "eup_set_solid_fraction", "eup_adjoint_run",
     "eup_geometry_ridged_shell", "eup_get_region_sums", "eup_init_state", "eup_get_line", "eup_get_plane_means",
-    "eup_get_cv_drag", "eup_save_state", "eup_restore_state",
+    "eup_get_cv_drag", "eup_save_state", "eup_restore_state", "eup_step_boundaries", "eup_step_stream",
+    "eup_get_x_planes", "eup_set_x_planes",
 ]
 
 
@@ -108,6 +109,8 @@ def _load():
         "eup_get_plane_means": ([vp, i32, vp], ctypes.c_int),
         "eup_get_cv_drag": ([vp, vp, vp], ctypes.c_int),
         "eup_save_state": ([vp, ctypes.c_char_p, i32], ctypes.c_int),
+        "eup_step_boundaries": ([vp], ctypes.c_int), "eup_step_stream": ([vp], ctypes.c_int),
+        "eup_get_x_planes": ([vp, i32, vp], ctypes.c_int), "eup_set_x_planes": ([vp, i32, vp], ctypes.c_int),
         "eup_restore_state": ([vp, ctypes.c_char_p, i32], ctypes.c_int),
         "eup_adjoint_run": ([vp, ctypes.POINTER(AdjointConfig), ctypes.POINTER(dbl), vp, vp], ctypes.c_int),
     }
@@ -291,6 +294,22 @@ class Solver:
     def init_state(self, u_in, amp, seed, itime=0):
         """Seeded equilibrium state generated on the device (same bits as upload(init_equilibrium(...)))."""
         self._ck(lib.eup_init_state(self._h, float(u_in), float(amp), int(seed), int(itime)))
+
+    def step_boundaries(self):
+        """First half of an x-slab step: bounce-back + force, halo planes (asynchronous)."""
+        self._ck(lib.eup_step_boundaries(self._h))
+
+    def step_stream(self):
+        """Second half of an x-slab step: stream-collide, step counter (asynchronous)."""
+        self._ck(lib.eup_step_stream(self._h))
+
+    def get_x_planes(self, side, dev_ptr):
+        """Pack the 5 populations leaving through x = 1 (side 0) or x = l (side 1) into device memory."""
+        self._ck(lib.eup_get_x_planes(self._h, side, dev_ptr))
+
+    def set_x_planes(self, side, dev_ptr):
+        """Write received planes into the x = 0 (side 0) or x = l+1 (side 1) halo."""
+        self._ck(lib.eup_set_x_planes(self._h, side, dev_ptr))
 
     def save_state(self, path, elem_bytes=4):
         """Checkpoint in the reference's raw format straight from the device."""

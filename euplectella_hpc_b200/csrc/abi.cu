@@ -46,6 +46,7 @@ struct eup_handle {
     bool pbb = false;             // partial-bounce-back model active (solid fraction set)
     void* ns = nullptr;           // solid fraction n_s per interior node, arithmetic type
     int64_t launches = 0;  // kernels launched by eup_step / eup_step_profiled
+    bool mid_step = false;  // eup_step_boundaries done, eup_step_stream pending
     int launches_per_step = 0;
     std::string err;
 };
@@ -76,8 +77,8 @@ int cuda_fail(eup_handle* h, cudaError_t e, const char* what) {
 
 bool face_flag_ok(int face, int f) {
     switch (face) {
-        case EUP_FRONT: return f == 0 || f == 1 || f == 5;
-        case EUP_REAR: return f == 0 || f == 1 || f == 4;
+        case EUP_FRONT: return f == 0 || f == 1 || f == 5 || f == EUP_BC_EXCHANGE;
+        case EUP_REAR: return f == 0 || f == 1 || f == 4 || f == EUP_BC_EXCHANGE;
         case EUP_UP: return f == 0 || f == 1 || f == 2 || f == 3;
         default: return f == 0 || f == 1 || f == 3;
     }
@@ -172,6 +173,38 @@ int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
     n += 1;
     if (pe) pe->mark(4 * s + 3, h->stream);
     return n;
+}
+
+// The two halves of a step of an x-slab lattice (the plane exchange goes between).
+template <typename S, typename R>
+void enqueue_boundaries(eup_handle* h) {
+    const Phys<R> ph = make_phys<R>(h);
+    const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
+    const Lat<S, R> src = make_lat<S, R>(h, h->cur);
+    launch_bounce_drag<S, R>(src, h->g, bc, h->blist, h->blinks, h->nblist, true, make_reduce(h), h->series,
+                             h->cap, h->d_itime, true, h->stream);
+    h->launches += 1 + launch_bc<S, R>(src, h->g, bc, ph, h->stream);
+}
+
+template <typename S, typename R>
+void enqueue_stream(eup_handle* h) {
+    const Phys<R> ph = make_phys<R>(h);
+    launch_stream_collide<S, R>(make_lat<S, R>(h, h->cur), make_lat<S, R>(h, h->cur ^ 1), h->g, ph, h->variant,
+                                h->stream);
+    h->cur ^= 1;
+    h->itime += 1;
+    enqueue_drag_only<S, R>(h);  // the force of the state reached, as eup_step leaves it
+    h->launches += 2;
+}
+
+template <typename S, typename R>
+void pack_x_dispatch(eup_handle* h, int side, void* dst) {
+    launch_pack_x<S, R>(make_lat<S, R>(h, h->cur), h->g, side, static_cast<R*>(dst), h->stream);
+}
+
+template <typename S, typename R>
+void unpack_x_dispatch(eup_handle* h, int side, const void* src) {
+    launch_unpack_x<S, R>(make_lat<S, R>(h, h->cur), h->g, side, static_cast<const R*>(src), h->stream);
 }
 
 template <typename S, typename R>
@@ -307,6 +340,7 @@ int finish_state(eup_handle* h, int64_t itime) {
     h->itime = itime;
     h->series_first = itime;
     h->has_state = true;
+    h->mid_step = false;
     if (h->pbb) CK(h, cudaMemsetAsync(h->series + 3 * (itime % h->cap), 0, 3 * sizeof(double), h->stream));
     else DISPATCH(h, enqueue_drag_only, h);
     CK(h, cudaGetLastError());
@@ -322,6 +356,10 @@ int ensure_staging(eup_handle* h, size_t bytes) {
     CK(h, cudaMalloc(&h->staging, bytes));
     h->staging_bytes = bytes;
     return EUP_OK;
+}
+
+bool has_exchange_face(const eup_handle* h) {
+    return h->cfg.bc[EUP_FRONT] == EUP_BC_EXCHANGE || h->cfg.bc[EUP_REAR] == EUP_BC_EXCHANGE;
 }
 
 int check_handle(eup_handle* h) {
@@ -457,6 +495,15 @@ int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
                 return fail(h, EUP_ERR_UNSUPPORTED,
                             "eup_set_obstacles: solid voxel on the outflow plane i=l; the reference's outflow "
                             "there reads values whose order its bounce-back loop leaves undefined");
+    }
+    for (int side = 0; side < 2; ++side) {
+        if (h->cfg.bc[side == 0 ? EUP_REAR : EUP_FRONT] != EUP_BC_EXCHANGE) continue;
+        const int64_t col = side == 0 ? 0 : g.l - 1;
+        for (int64_t r = 0; r < (int64_t)g.m * g.n; ++r)
+            if (obs[r * g.l + col] == 1)
+                return fail(h, EUP_ERR_UNSUPPORTED,
+                            "eup_set_obstacles: solid voxel on a column next to an x-slab exchange face; move the "
+                            "slab boundary (bounce-back there would read the neighbour's previous state)");
     }
     CK(h, cudaStreamSynchronize(h->stream));
     drop_graphs(h);  // the captured steps hold the old mask and list pointers
@@ -617,10 +664,57 @@ int eup_step(eup_handle* h, int32_t nsteps) {
     if (rc) return rc;
     if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_step: no state uploaded");
     if (nsteps < 0) return fail(h, EUP_ERR_INVALID_ARG, "eup_step: nsteps < 0");
+    if (has_exchange_face(h))
+        return fail(h, EUP_ERR_INVALID_ARG,
+                    "eup_step: an x-slab lattice steps with eup_step_boundaries / eup_step_stream around the "
+                    "plane exchange");
     if (nsteps == 0) return EUP_OK;
     cudaError_t e = cudaSuccess;
     DISPATCH_RET(h, e, enqueue_steps, h, nsteps);
     if (e != cudaSuccess) return cuda_fail(h, e, "eup_step");
+    CK(h, cudaGetLastError());
+    return EUP_OK;
+}
+
+int eup_step_boundaries(eup_handle* h) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_boundaries: no state uploaded");
+    if (h->pbb) return fail(h, EUP_ERR_UNSUPPORTED, "eup_step_boundaries: not for the partial-bounce-back model");
+    if (h->mid_step) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_boundaries: eup_step_stream is due first");
+    DISPATCH(h, enqueue_boundaries, h);
+    CK(h, cudaGetLastError());
+    h->mid_step = true;
+    return EUP_OK;
+}
+
+int eup_step_stream(eup_handle* h) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!h->mid_step) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_stream: eup_step_boundaries is due first");
+    DISPATCH(h, enqueue_stream, h);
+    CK(h, cudaGetLastError());
+    h->mid_step = false;
+    return EUP_OK;
+}
+
+int eup_get_x_planes(eup_handle* h, int32_t side, void* dst) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!dst || (side != 0 && side != 1)) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_x_planes: bad side or null");
+    if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_get_x_planes: no state uploaded");
+    DISPATCH(h, pack_x_dispatch, h, side, dst);
+    CK(h, cudaGetLastError());
+    return EUP_OK;
+}
+
+int eup_set_x_planes(eup_handle* h, int32_t side, const void* src) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!src || (side != 0 && side != 1)) return fail(h, EUP_ERR_INVALID_ARG, "eup_set_x_planes: bad side or null");
+    if (h->cfg.bc[side == 0 ? EUP_REAR : EUP_FRONT] != EUP_BC_EXCHANGE)
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_set_x_planes: that face is not an exchange face");
+    DISPATCH(h, unpack_x_dispatch, h, side, src);
     CK(h, cudaGetLastError());
     return EUP_OK;
 }
@@ -631,6 +725,8 @@ int eup_step_profiled(eup_handle* h, int32_t nsteps, double ms[4]) {
     if (!ms) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_profiled: null ms");
     if (!h->has_state) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_profiled: no state uploaded");
     if (nsteps < 1) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_profiled: nsteps < 1");
+    if (has_exchange_face(h))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_step_profiled: not for an x-slab lattice");
     PhaseEvents pe;
     pe.ev.resize(4 * (size_t)nsteps + 1);
     for (auto& e : pe.ev) CK(h, cudaEventCreate(&e));
@@ -1054,6 +1150,8 @@ int eup_set_solid_fraction(eup_handle* h, const double* ns) {
     }
     if (h->prec != EUP_FP32 && h->prec != EUP_FP64)
         return fail(h, EUP_ERR_UNSUPPORTED, "eup_set_solid_fraction: the partial-bounce-back model runs in FP32 or FP64");
+    if (has_exchange_face(h))
+        return fail(h, EUP_ERR_UNSUPPORTED, "eup_set_solid_fraction: not offered on an x-slab lattice");
     if (h->nblist > 0 || h->bits)
         return fail(h, EUP_ERR_UNSUPPORTED,
                     "eup_set_solid_fraction: obstacles are set; fold them into the field as n_s = 1 instead");

@@ -110,6 +110,12 @@ void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const int bc[6], const
                         const uint64_t* links, int64_t nlist, bool do_bounce, const Reduce& red, double* series,
                         int64_t cap, int64_t* d_itime, bool advance, cudaStream_t st);
 
+// x-slab faces: the five populations crossing an x face, (m+2)(n+2) values each.
+template <typename S, typename R>
+void launch_pack_x(const Lat<S, R>& L, const Geo& g, int side, R* out, cudaStream_t st);
+template <typename S, typename R>
+void launch_unpack_x(const Lat<S, R>& L, const Geo& g, int side, const R* in, cudaStream_t st);
+
 // x-face copy of the current lattice (needed once after an upload).
 template <typename S, typename R>
 void launch_fill_xface(const Lat<S, R>& L, const Geo& g, cudaStream_t st);

@@ -645,12 +645,55 @@ unsigned grid_for(int64_t work, int tpb, unsigned cap = 148u * 16u) {
 
 }  // namespace
 
+// x-slab faces: pack the five populations leaving through column x = 1 (side 0,
+// cx = -1: q 9..13) or x = l (side 1, cx = +1: q 0..4), halo rows j = 0, m+1
+// and k = 0, n+1 included, as a later load returns them; unpack received
+// planes into the x = 0 (side 0, q 0..4) or x = l+1 (side 1, q 9..13) halo.
+template <typename S, typename R>
+__global__ void k_pack_x(Lat<S, R> L, Geo g, int side, R* out) {
+    const int64_t plane = (int64_t)(g.m + 2) * (g.n + 2);
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 5 * plane) return;
+    const int c = (int)(t / plane);
+    const int64_t jk = t % plane;
+    const int j = (int)(jk % (g.m + 2)), k = (int)(jk / (g.m + 2));
+    const int q = side ? c : 9 + c;
+    const int i = side ? g.l : 1;
+    out[t] = bc_load(L, g, q, i, j, k);
+}
+
+template <typename S, typename R>
+__global__ void k_unpack_x(Lat<S, R> L, Geo g, int side, const R* in) {
+    const int64_t plane = (int64_t)(g.m + 2) * (g.n + 2);
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 5 * plane) return;
+    const int c = (int)(t / plane);
+    const int64_t jk = t % plane;
+    const int j = (int)(jk % (g.m + 2)), k = (int)(jk / (g.m + 2));
+    const int q = side ? 9 + c : c;
+    const int i = side ? g.l + 1 : 0;
+    L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)] = in[t];
+}
+
+template <typename S, typename R>
+void launch_pack_x(const Lat<S, R>& L, const Geo& g, int side, R* out, cudaStream_t st) {
+    const int64_t work = 5 * (int64_t)(g.m + 2) * (g.n + 2);
+    k_pack_x<S, R><<<(unsigned)((work + kTpb - 1) / kTpb), kTpb, 0, st>>>(L, g, side, out);
+}
+
+template <typename S, typename R>
+void launch_unpack_x(const Lat<S, R>& L, const Geo& g, int side, const R* in, cudaStream_t st) {
+    const int64_t work = 5 * (int64_t)(g.m + 2) * (g.n + 2);
+    k_unpack_x<S, R><<<(unsigned)((work + kTpb - 1) / kTpb), kTpb, 0, st>>>(L, g, side, in);
+}
+
 template <typename S, typename R>
 int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& ph, cudaStream_t st) {
     const int l = g.l, m = g.m, n = g.n;
-    int launches = 6;
-    // front
-    {
+    int launches = 4;
+    // front (an x-slab exchange face gets its plane from the neighbour instead)
+    if (bc[0] != 6) {
+        ++launches;
         const int f = bc[0];
         Range2 r = (f == 0) ? Range2{0, m + 1, 1, n} : Range2{1, m, 1, n};
         k_front<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, f);
@@ -661,7 +704,8 @@ int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& 
         }
     }
     // rear
-    {
+    if (bc[1] != 6) {
+        ++launches;
         const int f = bc[1];
         Range2 r = (f == 0) ? Range2{0, m + 1, 1, n} : (f == 1) ? Range2{1, m, 1, n} : Range2{0, m + 2, 0, n + 2};
         k_rear<S, R><<<r.blocks(kTpb), kTpb, 0, st>>>(L, g, r, f, ph.u_inflow);
@@ -783,6 +827,8 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
                                            const uint64_t*, int64_t, bool, const Reduce&, double*,     \
                                            int64_t, int64_t*, bool, cudaStream_t);                     \
     template void launch_fill_xface<S, R>(const Lat<S, R>&, const Geo&, cudaStream_t);                 \
+    template void launch_pack_x<S, R>(const Lat<S, R>&, const Geo&, int, R*, cudaStream_t);              \
+    template void launch_unpack_x<S, R>(const Lat<S, R>&, const Geo&, int, const R*, cudaStream_t);      \
     template void launch_line<S, R>(const Lat<S, R>&, const Geo&, int, int, int, double*, cudaStream_t);   \
     template void launch_plane_means<S, R>(const Lat<S, R>&, const Geo&, int, double*, cudaStream_t);     \
     template void launch_cv_drag<S, R>(const Lat<S, R>&, const Geo&, const int*, R, const Reduce&, double*, \

@@ -52,7 +52,10 @@ enum {
     EUP_BC_LID = 2,       /* up face only */
     EUP_BC_FREESLIP = 3,  /* up/down/left/right */
     EUP_BC_INFLOW = 4,    /* rear face only */
-    EUP_BC_OUTFLOW = 5    /* front face only */
+    EUP_BC_OUTFLOW = 5,   /* front face only */
+    EUP_BC_EXCHANGE = 6   /* front/rear: an x-slab face whose halo plane the caller fills from the
+                             neighbouring slab (eup_set_x_planes); no reference flag, the
+                             reference's MPI faces are implied by its process grid */
 };
 
 /* Face order of eup_config.bc (reference names front/rear/right/left/up/down). */
@@ -262,6 +265,35 @@ int eup_get_boundary_solid(eup_handle* h, int64_t* list, int64_t cap, int64_t* c
  * All calls share the scratch: calls that overlap on the GPU race. */
 int eup_mem_force_noalloc(int32_t l, int32_t m, int32_t n, const int32_t bc[6], const void* const pops[19],
                           int32_t elem_bytes, const int32_t* obs, double* force, void* stream);
+
+/* ---- x-slab decomposition (one GPU per slab) ----------------------------- */
+/* The time step in two halves for a lattice that is one x-slab of a larger
+ * one: eup_step_boundaries enqueues the bounce-back (with the force of the
+ * current state) and the halo planes; the caller then moves the x-face planes
+ * between neighbouring slabs (eup_get_x_planes / eup_set_x_planes, e.g. NCCL
+ * send/recv on the handle's stream); eup_step_stream enqueues stream-collide
+ * and advances the step.  Faces flagged EUP_BC_EXCHANGE get no halo kernel.
+ * With the planes exchanged after the halo kernels (their y/z halo rows
+ * included), an FP32 or FP64 run split into slabs equals the single-lattice
+ * run bit for bit (16-bit storage: to FP32 rounding of f, the halo's type),
+ * provided no solid voxel lies on a column next to an exchange face
+ * (eup_set_obstacles rejects that: its bounce-back would read the
+ * neighbour's state of the previous step).  Replaces the x part of
+ * CODE/SRC/bcond.comm.packed.F90:203-286, which exchanges before bcond_bc and
+ * so lags the halo rows by one step. */
+int eup_step_boundaries(eup_handle* h);
+int eup_step_stream(eup_handle* h);
+
+/* The five populations that cross an x face, (m+2)(n+2) values each, index
+ * (q', j + (m+2) k) for j = 0..m+1, k = 0..n+1, in the arithmetic type (float,
+ * or double for FP64), device pointers.  side 0: column x = 1, populations
+ * a10..a14 (heading to -x), for the left neighbour's x = l+1 plane; side 1:
+ * column x = l, a01..a05 (heading to +x), for the right neighbour's x = 0
+ * plane.  Enqueued on the handle's stream after eup_step_boundaries. */
+int eup_get_x_planes(eup_handle* h, int32_t side, void* dst);
+/* Writes received planes into the halo: side 0 fills x = 0 with a01..a05 (from
+ * the left neighbour's side 1), side 1 fills x = l+1 with a10..a14. */
+int eup_set_x_planes(eup_handle* h, int32_t side, const void* src);
 
 /* ---- partial bounce-back and its adjoint ----------------------------------- */
 /* No counterpart in the reference (its solids are all-or-nothing voxels).  A

@@ -1,0 +1,140 @@
+"""x-slab decomposition on the GPU.  Slabs of one lattice, stepped with the
+plane exchange between the halves of each step, must equal the single-lattice
+run bit for bit.  Two forms: several slabs in one process (exchange by device
+copies), and two processes exchanging through torch.distributed (gloo, host
+staging) -- both ranks on the one GPU a test gets, which is fine here because
+no kernel waits on another rank: the host orders every exchange."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+L, M, N = 60, 18, 10
+
+
+def _case(eup, precision):
+    bc = (eup.OUTFLOW, eup.INFLOW, eup.FREESLIP, eup.FREESLIP, eup.PERIODIC, eup.PERIODIC)
+    cfg = eup.Config(L, M, N, bc=bc, svisc=0.01, u_inflow=0.05, precision=precision, cd_uref=0.05, cd_length=6,
+                     cd_span=N)
+    obs = eup.geometry_cylinder_z(L, M, N, 8, 9.5, 3)  # solid columns 5..11, away from every slab face
+    return cfg, obs
+
+
+def _single(eup, cfg, obs, a, steps, dt):
+    with eup.Solver(cfg) as s:
+        s.set_obstacles(obs)
+        s.upload(a)
+        s.step(steps)
+        return s.download(dt), s.forces()
+
+
+@pytest.mark.parametrize("prec,world", [("fp32", 3), ("fp64", 2), ("fp16", 4)])
+def test_slabs_in_one_process_equal_single_lattice(eup, require_gpu, prec, world):
+    from euplectella_hpc_b200.slabs import SlabSolver, gather_state, step_in_process
+    code, dt = {"fp32": (eup.FP32, np.float32), "fp64": (eup.FP64, np.float64), "fp16": (eup.FP16_DEV, np.float32)}[prec]
+    cfg, obs = _case(eup, code)
+    a = eup.init_equilibrium(L, M, N, 0.05, 1e-3, 5, dt)
+    steps = 30
+    ref, f_ref = _single(eup, cfg, obs, a, steps, dt)
+    slabs = [SlabSolver(cfg, r, world) for r in range(world)]
+    try:
+        for s in slabs:
+            s.set_obstacles(obs)
+            s.upload(a)
+        step_in_process(slabs, steps)
+        got = gather_state(slabs, dt)
+        f = sum(s.solver.forces() for s in slabs)
+        assert all(s.solver.itime == steps for s in slabs)
+    finally:
+        for s in slabs:
+            s.solver.close()
+    keep = np.ones(got.shape[1:], bool)
+    keep[1:-1, 1:-1, 1:-1] = obs == 0
+    if prec == "fp16":
+        # 16-bit storage keeps deviations in the lattice but f in the FP32 halo, so a pull across
+        # a slab face reads the deviation back through f; where that rounding moves a stored
+        # deviation by one 16-bit step (2^-5 / 4096 = 7.6e-6 in f for |f - w| < 1/64) the runs
+        # part by that quantum: a few quanta at most, almost everywhere none
+        d = np.abs(got - ref)[:, keep]
+        assert d.max() < 8 * 7.7e-6, d.max()
+        assert d.mean() < 2e-6, d.mean()
+        np.testing.assert_allclose(f, f_ref, rtol=0, atol=1e-3 * np.abs(f_ref).max())
+        return
+    for q in range(19):
+        bad = (got[q] != ref[q]) & keep
+        assert not bad.any(), f"population {q + 1}: {bad.sum()} mismatches, first at {np.argwhere(bad)[0]}"
+    np.testing.assert_allclose(f, f_ref, rtol=1e-12, atol=1e-14)
+
+
+def test_slab_guards(eup, require_gpu):
+    from euplectella_hpc_b200.slabs import slab_config
+    cfg, obs = _case(eup, eup.FP32)
+    c1 = slab_config(cfg, 1, 3)
+    with eup.Solver(c1) as s:
+        s.upload(eup.init_equilibrium(c1.lx, M, N, 0.05, 0, 1, np.float32))
+        with pytest.raises(eup.EupError):
+            s.step(1)                      # an x-slab steps only in halves
+        with pytest.raises(eup.EupError):
+            s.step_stream()                # the boundaries half comes first
+        bad = np.zeros((N, M, c1.lx), np.int32)
+        bad[3, 4, 0] = 1                   # solid next to the rear exchange face
+        with pytest.raises(eup.EupError):
+            s.set_obstacles(bad)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_worker(rank, world, port, prec, steps, out_dir):
+    import torch
+    import torch.distributed as dist
+    import euplectella_hpc_b200 as eup
+    from euplectella_hpc_b200.slabs import DistTransport, SlabSolver
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        code, dt = (eup.FP32, np.float32) if prec == "fp32" else (eup.FP64, np.float64)
+        cfg, obs = _case(eup, code)
+        a = eup.init_equilibrium(L, M, N, 0.05, 1e-3, 5, dt)
+        s = SlabSolver(cfg, rank, world, DistTransport(rank, world))
+        s.set_obstacles(obs)
+        s.upload(a)
+        s.step(steps)
+        f = s.forces()
+        np.save(os.path.join(out_dir, f"slab{rank}.npy"), s.solver.download(dt))
+        np.save(os.path.join(out_dir, f"force{rank}.npy"), f)
+        s.solver.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_through_torch_distributed(eup, require_gpu, tmp_path):
+    import torch.multiprocessing as mp
+    from euplectella_hpc_b200.slabs import partition
+    world, steps = 2, 20
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_worker, args=(r, world, port, "fp32", steps, str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    cfg, obs = _case(eup, eup.FP32)
+    a = eup.init_equilibrium(L, M, N, 0.05, 1e-3, 5, np.float32)
+    ref, f_ref = _single(eup, cfg, obs, a, steps, np.float32)
+    for r, (x0, nx) in enumerate(partition(L, world)):
+        loc = np.load(tmp_path / f"slab{r}.npy")
+        fl = obs[:, :, x0 - 1:x0 - 1 + nx] == 0
+        for q in range(19):
+            got, want = loc[q][1:-1, 1:-1, 1:-1], ref[q][1:-1, 1:-1, x0:x0 + nx]
+            assert np.array_equal(got[fl], want[fl]), (r, q)
+        np.testing.assert_allclose(np.load(tmp_path / f"force{r}.npy"), f_ref, rtol=1e-12, atol=1e-14)
