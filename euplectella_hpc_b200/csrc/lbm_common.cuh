@@ -76,14 +76,7 @@ struct F2 {
 // fma is never fused with another.
 __constant__ float2 kF2Unit = {1.0f, -0.0f};
 
-__device__ __forceinline__ F2 fma_rn(F2 a, F2 b, F2 c) {
-    F2 r;
-    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
-        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n}"
-        : "=f"(r.v.x), "=f"(r.v.y)
-        : "f"(a.v.x), "f"(a.v.y), "f"(b.v.x), "f"(b.v.y), "f"(c.v.x), "f"(c.v.y));
-    return r;
-}
+__device__ __forceinline__ F2 fma_rn(F2 a, F2 b, F2 c) { return F2(__ffma2_rn(a.v, b.v, c.v)); }
 __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ F2 operator+(F2 a, F2 b) { return fma_rn(a, F2(kF2Unit.x), b); }
 __device__ __forceinline__ F2 operator-(F2 a) { return F2(-a.v.x, -a.v.y); }
