@@ -133,16 +133,22 @@ template <> struct Vec2<float> {
     using T = float2;
     static __device__ __forceinline__ float2 unpack(float2 v) { return v; }
     static __device__ __forceinline__ float2 pack(float2 v) { return v; }
+    static __device__ __forceinline__ float lo(float2 v) { return v.x; }
+    static __device__ __forceinline__ float hi(float2 v) { return v.y; }
 };
 template <> struct Vec2<__half> {
     using T = __half2;
     static __device__ __forceinline__ float2 unpack(__half2 v) { return __half22float2(v); }
     static __device__ __forceinline__ __half2 pack(float2 v) { return __float22half2_rn(v); }
+    static __device__ __forceinline__ __half lo(__half2 v) { return __low2half(v); }
+    static __device__ __forceinline__ __half hi(__half2 v) { return __high2half(v); }
 };
 template <> struct Vec2<__nv_bfloat16> {
     using T = __nv_bfloat162;
     static __device__ __forceinline__ float2 unpack(__nv_bfloat162 v) { return __bfloat1622float2(v); }
     static __device__ __forceinline__ __nv_bfloat162 pack(float2 v) { return __float22bfloat162_rn(v); }
+    static __device__ __forceinline__ __nv_bfloat16 lo(__nv_bfloat162 v) { return __low2bfloat16(v); }
+    static __device__ __forceinline__ __nv_bfloat16 hi(__nv_bfloat162 v) { return __high2bfloat16(v); }
 };
 
 template <typename S, int MINB>
@@ -199,6 +205,14 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float>
     }
     if constexpr (dev) collide_dev<F2>(x, ph.omega, ph.omega1, ph.fgrad, src.scale, src.inv_scale);
     else collide<F2>(x, F2(ph.omega), F2(ph.omega1), F2(ph.fgrad));
+    if ((i == 1) | (i + 1 == l)) {  // x-face copy of the first/last column: the value a later load returns
+#pragma unroll
+        for (int q = 0; q < 18; ++q) {
+            const T2 o = V2::pack(x[q].v);
+            if (i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = Store<S, float>::load(V2::lo(o), q, dst.inv_scale);
+            if (i + 1 == l) dst.xface[xface_idx(g, 1, q, j, k)] = Store<S, float>::load(V2::hi(o), q, dst.inv_scale);
+        }
+    }
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
         const T2 o = V2::pack(x[q].v);
@@ -206,13 +220,8 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float>
         if (!dev || q == 18 || cx_of(q) == 0) {
             *reinterpret_cast<T2*>(op) = o;
         } else {  // odd address in the shifted layout
-            op[0] = reinterpret_cast<const S*>(&o)[0];
-            op[1] = reinterpret_cast<const S*>(&o)[1];
-        }
-        if (q < 18 && (i == 1 || i + 1 == l)) {  // x-face copy: the value a later lattice load returns
-            const S* os = reinterpret_cast<const S*>(&o);
-            if (i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = Store<S, float>::load(os[0], q, dst.inv_scale);
-            if (i + 1 == l) dst.xface[xface_idx(g, 1, q, j, k)] = Store<S, float>::load(os[1], q, dst.inv_scale);
+            op[0] = V2::lo(o);
+            op[1] = V2::hi(o);
         }
     }
 }
