@@ -40,7 +40,8 @@ EXPORTED = [
     "eup_geometry_reticular_shell", "eup_mem_force_noalloc", "eup_set_solid_fraction", "eup_adjoint_run",
     "eup_geometry_ridged_shell", "eup_get_region_sums", "eup_init_state", "eup_get_line", "eup_get_plane_means",
     "eup_get_cv_drag", "eup_save_state", "eup_restore_state", "eup_step_boundaries", "eup_step_stream",
-    "eup_get_x_planes", "eup_set_x_planes",
+    "eup_get_x_planes", "eup_set_x_planes", "eup_geometry_reference", "eup_voxelise", "eup_build_obstacles",
+    "eup_get_obstacles", "eup_write_obstacles",
 ]
 
 
@@ -62,6 +63,50 @@ class CConfig(ctypes.Structure):
         ("cd_span", ctypes.c_double),
         ("series_capacity", ctypes.c_int64),
     ]
+
+
+# Voxel shapes of eup_geometry and the variant bits of eup_geometry_reference.
+GEOM_NONE, GEOM_REF_SPHERE, GEOM_REF_COLUMN, GEOM_CYLINDER_Z, GEOM_RETICULAR_SHELL, GEOM_RIDGED_SHELL = range(6)
+GEOM_VARIANT_CYLINDER_INF, GEOM_VARIANT_TEST1 = 1, 2
+
+
+class Geometry(ctypes.Structure):
+    """eup_geometry: a voxel shape in global node coordinates (global index = local + offset)."""
+    _fields_ = [
+        ("kind", ctypes.c_int32), ("offset", ctypes.c_int32 * 3),
+        ("center", ctypes.c_int32 * 3), ("kstop", ctypes.c_int32), ("r2_lo", ctypes.c_int64), ("r2_hi", ctypes.c_int64),
+        ("xc", ctypes.c_double), ("yc", ctypes.c_double), ("zc", ctypes.c_double), ("radius", ctypes.c_double),
+        ("x0", ctypes.c_double), ("length", ctypes.c_double), ("outer_d", ctypes.c_double),
+        ("strut_d", ctypes.c_double), ("pitch", ctypes.c_double),
+        ("ridge_h", ctypes.c_double), ("ridge_t", ctypes.c_double), ("cap_t", ctypes.c_double),
+        ("pore_d", ctypes.c_double), ("seed", ctypes.c_uint64),
+    ]
+
+    def shifted(self, offset) -> "Geometry":
+        """A copy with another offset (an x-slab's x0 - 1, or the reference's mpicoords * local size)."""
+        g = Geometry.from_buffer_copy(self)
+        g.offset[:] = [int(v) for v in offset]
+        return g
+
+    @staticmethod
+    def cylinder_z(xc, yc, r) -> "Geometry":
+        g = Geometry(kind=GEOM_CYLINDER_Z)
+        g.xc, g.yc, g.radius = float(xc), float(yc), float(r)
+        return g
+
+    @staticmethod
+    def reticular_shell(x0, length, yc, zc, outer_d, strut_d, pitch, seed) -> "Geometry":
+        g = Geometry(kind=GEOM_RETICULAR_SHELL)
+        g.x0, g.length, g.yc, g.zc = float(x0), float(length), float(yc), float(zc)
+        g.outer_d, g.strut_d, g.pitch, g.seed = float(outer_d), float(strut_d), float(pitch), int(seed)
+        return g
+
+    @staticmethod
+    def ridged_shell(x0, length, yc, zc, outer_d, strut_d, pitch, ridge_h, ridge_t, cap_t, pore_d, seed) -> "Geometry":
+        g = Geometry.reticular_shell(x0, length, yc, zc, outer_d, strut_d, pitch, seed)
+        g.kind = GEOM_RIDGED_SHELL
+        g.ridge_h, g.ridge_t, g.cap_t, g.pore_d = float(ridge_h), float(ridge_t), float(cap_t), float(pore_d)
+        return g
 
 
 class AdjointConfig(ctypes.Structure):
@@ -113,7 +158,16 @@ def _load():
         "eup_get_x_planes": ([vp, i32, vp], ctypes.c_int), "eup_set_x_planes": ([vp, i32, vp], ctypes.c_int),
         "eup_restore_state": ([vp, ctypes.c_char_p, i32], ctypes.c_int),
         "eup_adjoint_run": ([vp, ctypes.POINTER(AdjointConfig), ctypes.POINTER(dbl), vp, vp], ctypes.c_int),
+        "eup_geometry_reference": ([i32, i32, i32, i32, i32, ctypes.POINTER(Geometry)], ctypes.c_int),
+        "eup_voxelise": ([ctypes.POINTER(Geometry), i32, i32, i32, vp], ctypes.c_int),
+        "eup_build_obstacles": ([vp, ctypes.POINTER(Geometry)], ctypes.c_int),
+        "eup_get_obstacles": ([vp, vp, ctypes.POINTER(i64)], ctypes.c_int),
+        "eup_write_obstacles": ([vp, ctypes.c_char_p], ctypes.c_int),
     }
+    # every entry point gets a prototype: an unprototyped call would pass pointers as C ints
+    missing = [name for name in EXPORTED if name not in sig]
+    if missing:
+        raise ImportError(f"no ctypes prototype for {missing}")
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
         fn.argtypes = args
@@ -218,6 +272,27 @@ class Solver:
         obs = np.ascontiguousarray(obs, dtype=np.int32)
         assert obs.shape == (self.cfg.lz, self.cfg.ly, self.cfg.lx)
         self._ck(lib.eup_set_obstacles(self._h, obs.ctypes.data))
+
+    def build_obstacles(self, geom: Geometry):
+        """Voxelises geom on the device into the solid mask and installs it (eup_build_obstacles)."""
+        self._ck(lib.eup_build_obstacles(self._h, ctypes.byref(geom)))
+
+    def obstacles(self) -> tuple[np.ndarray, int]:
+        """The installed mask obs (n, m, l) and its number of solid voxels."""
+        obs = np.empty((self.cfg.lz, self.cfg.ly, self.cfg.lx), dtype=np.int32)
+        n = ctypes.c_int64(0)
+        self._ck(lib.eup_get_obstacles(self._h, obs.ctypes.data, ctypes.byref(n)))
+        return obs, int(n.value)
+
+    def obstacle_count(self) -> int:
+        """Solid voxels of the installed mask (nothing crosses to the host but the count)."""
+        n = ctypes.c_int64(0)
+        self._ck(lib.eup_get_obstacles(self._h, None, ctypes.byref(n)))
+        return int(n.value)
+
+    def write_obstacles(self, path: str):
+        """The installed mask as an obstacle file obs.RRRR.TTTTTTTT.bin, listed on the device."""
+        self._ck(lib.eup_write_obstacles(self._h, os.fsencode(str(path))))
 
     def upload(self, pops: np.ndarray, itime: int = 0):
         pops = np.ascontiguousarray(pops)
@@ -417,6 +492,23 @@ def write_raw_state(path, pops: np.ndarray, itime: int):
     pops = np.ascontiguousarray(pops)
     _, n2, m2, l2 = pops.shape
     _check(lib.eup_write_raw_state(os.fsencode(path), l2 - 2, m2 - 2, n2 - 2, _elem(pops), _ptrs(pops), itime))
+
+
+def geometry_reference(flag2: int, lx: int, ly: int, lz: int, cylinder_inf: bool = False,
+                       test1: bool = False) -> Geometry:
+    """The obstacle CODE/SRC/build.obs.F90 creates for flag1 = 2 and this flag2 (1 sphere,
+    2 column, 3 half column) on the global lattice lx x ly x lz."""
+    g = Geometry()
+    variant = (GEOM_VARIANT_CYLINDER_INF if cylinder_inf else 0) | (GEOM_VARIANT_TEST1 if test1 else 0)
+    _check(lib.eup_geometry_reference(int(flag2), int(lx), int(ly), int(lz), variant, ctypes.byref(g)))
+    return g
+
+
+def voxelise(geom: Geometry, l: int, m: int, n: int) -> np.ndarray:
+    """The host voxeliser: obs (n, m, l) of geom, identical to the device's mask."""
+    obs = np.empty((n, m, l), dtype=np.int32)
+    _check(lib.eup_voxelise(ctypes.byref(geom), int(l), int(m), int(n), obs.ctypes.data))
+    return obs
 
 
 def geometry_cylinder_z(l, m, n, xc, yc, r) -> np.ndarray:

@@ -1,9 +1,10 @@
 """Builds the sm_100a shared library `_lib/libeup.so` in place with nvcc.
 
 Every CUDA translation unit is compiled for `sm_100a` only, with
-`--fmad=false` so that each floating-point operation rounds on its own, in
-source order (the FP32/FP64 step then matches an IEEE build of the reference's
-Fortran bit for bit).  The CUDA runtime is linked statically, so the library
+`--fmad=false` (host code: `-ffp-contract=off`) so that each floating-point
+operation rounds on its own, in source order (the FP32/FP64 step then matches
+an IEEE build of the reference's Fortran bit for bit, and the host and device
+voxelisers agree).  The CUDA runtime is linked statically, so the library
 loads on machines without a GPU driver (entry points then return
 EUP_ERR_NO_DEVICE).
 """
@@ -24,9 +25,9 @@ LIB = os.path.join(LIB_DIR, "libeup.so")
 DRIVER = os.path.join(LIB_DIR, "eup_bgk3d")
 
 SOURCES = ["abi.cu", "k_bc.cu", "k_step.cu", "k_setup.cu", "k_adjoint.cu", "host.cpp", "noalloc.cu"]
-HEADERS = ["lbm_common.cuh", "internal.h"]
+HEADERS = ["lbm_common.cuh", "internal.h", "geometry.h", "init_eq.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-fopenmp,-Wall",
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-fopenmp,-Wall,-ffp-contract=off",
           "-I", os.path.join(ROOT, "include")]
 
 

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/eup.h"
+#include "geometry.h"
 #include "internal.h"
 
 using namespace eup;
@@ -32,6 +33,7 @@ struct eup_handle {
     int32_t* blist = nullptr;
     uint64_t* blinks = nullptr;   // neighbour classification of each boundary-solid voxel
     int64_t nblist = 0;
+    int64_t nsolid = 0;           // solid voxels of the installed mask
     double* partials = nullptr;
     unsigned int* counter = nullptr;
     double* series = nullptr;
@@ -478,54 +480,51 @@ int eup_destroy(eup_handle* h) {
     return EUP_OK;
 }
 
-int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
-    int rc = check_handle(h);
-    if (rc) return rc;
-    if (!obs) return fail(h, EUP_ERR_INVALID_ARG, "eup_set_obstacles: null obs");
-    const Geo& g = h->g;
-    int64_t nsolid = 0;
-    for (int64_t t = 0; t < g.N; ++t) nsolid += (obs[t] == 1);
+}  // extern "C"
+
+namespace {
+
+// The checks eup_set_obstacles and eup_build_obstacles share, from the number of solid
+// voxels and of those on the columns i = 1 and i = l.
+int check_obstacles(eup_handle* h, const char* who, int64_t nsolid, int64_t on_first, int64_t on_last) {
     if (nsolid > 0 && h->pbb)
         return fail(h, EUP_ERR_UNSUPPORTED,
-                    "eup_set_obstacles: a solid-fraction field is set; the partial-bounce-back model takes no "
+                    std::string(who) + ": a solid-fraction field is set; the partial-bounce-back model takes no "
                     "halfway-bounce-back voxels (fold them into the field as n_s = 1)");
-    if (h->cfg.bc[EUP_FRONT] == EUP_BC_OUTFLOW) {
-        for (int64_t r = 0; r < (int64_t)g.m * g.n; ++r)
-            if (obs[r * g.l + (g.l - 1)] == 1)
-                return fail(h, EUP_ERR_UNSUPPORTED,
-                            "eup_set_obstacles: solid voxel on the outflow plane i=l; the reference's outflow "
-                            "there reads values whose order its bounce-back loop leaves undefined");
-    }
-    for (int side = 0; side < 2; ++side) {
-        if (h->cfg.bc[side == 0 ? EUP_REAR : EUP_FRONT] != EUP_BC_EXCHANGE) continue;
-        const int64_t col = side == 0 ? 0 : g.l - 1;
-        for (int64_t r = 0; r < (int64_t)g.m * g.n; ++r)
-            if (obs[r * g.l + col] == 1)
-                return fail(h, EUP_ERR_UNSUPPORTED,
-                            "eup_set_obstacles: solid voxel on a column next to an x-slab exchange face; move the "
-                            "slab boundary (bounce-back there would read the neighbour's previous state)");
-    }
-    CK(h, cudaStreamSynchronize(h->stream));
+    if (h->cfg.bc[EUP_FRONT] == EUP_BC_OUTFLOW && on_last > 0)
+        return fail(h, EUP_ERR_UNSUPPORTED,
+                    std::string(who) + ": solid voxel on the outflow plane i=l; the reference's outflow "
+                    "there reads values whose order its bounce-back loop leaves undefined");
+    if ((h->cfg.bc[EUP_REAR] == EUP_BC_EXCHANGE && on_first > 0) ||
+        (h->cfg.bc[EUP_FRONT] == EUP_BC_EXCHANGE && on_last > 0))
+        return fail(h, EUP_ERR_UNSUPPORTED,
+                    std::string(who) + ": solid voxel on a column next to an x-slab exchange face; move the "
+                    "slab boundary (bounce-back there would read the neighbour's previous state)");
+    return EUP_OK;
+}
+
+// Installs `bits` (m*n*wpr words, owned by the handle from here on; null or
+// nsolid == 0: no solids) in place of the current mask: the list of boundary
+// solids, their link words, and the drag of the current state.
+int install_mask(eup_handle* h, uint32_t* bits, int64_t nsolid) {
+    const Geo& g = h->g;
     drop_graphs(h);  // the captured steps hold the old mask and list pointers
-    if (h->bits) { cudaFree(h->bits); h->bits = nullptr; }
+    if (h->bits) cudaFree(h->bits);
     if (h->blist) { cudaFree(h->blist); h->blist = nullptr; }
     if (h->blinks) { cudaFree(h->blinks); h->blinks = nullptr; }
     h->nblist = 0;
-    h->wpr = (g.l + 31) / 32;
+    h->nsolid = 0;
+    if (nsolid <= 0 && bits) { cudaFree(bits); bits = nullptr; }
+    h->bits = bits;
     if (nsolid > 0) {
-        int32_t* d_obs = nullptr;
+        h->nsolid = nsolid;
         uint8_t* d_flags = nullptr;
-        CK(h, cudaMalloc(&d_obs, sizeof(int32_t) * g.N));
-        CK(h, cudaMemcpyAsync(d_obs, obs, sizeof(int32_t) * g.N, cudaMemcpyHostToDevice, h->stream));
-        CK(h, cudaMalloc(&h->bits, sizeof(uint32_t) * (size_t)g.m * g.n * h->wpr));
-        launch_build_mask(d_obs, g, h->bits, h->wpr, h->stream);
         CK(h, cudaMalloc(&d_flags, g.N));
         launch_flag_boundary_solid(g, make_mask(h), d_flags, h->stream);
-        CK(h, cudaMalloc(&h->blist, sizeof(int32_t) * (size_t)(nsolid > 0 ? nsolid : 1)));
+        CK(h, cudaMalloc(&h->blist, sizeof(int32_t) * (size_t)nsolid));
         cudaError_t e;
         const int64_t cnt = compact_flags(d_flags, g.N, h->blist, h->stream, &e);
         cudaFree(d_flags);
-        cudaFree(d_obs);
         if (e != cudaSuccess) return cuda_fail(h, e, "compact boundary solid list");
         h->nblist = cnt;
         CK(h, cudaMalloc(&h->blinks, sizeof(uint64_t) * (size_t)(cnt > 0 ? cnt : 1)));
@@ -536,6 +535,140 @@ int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
     CK(h, cudaGetLastError());
     CK(h, cudaStreamSynchronize(h->stream));
     return EUP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int eup_set_obstacles(eup_handle* h, const int32_t* obs) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!obs) return fail(h, EUP_ERR_INVALID_ARG, "eup_set_obstacles: null obs");
+    const Geo& g = h->g;
+    int64_t nsolid = 0, on_first = 0, on_last = 0;
+    for (int64_t t = 0; t < g.N; ++t) nsolid += (obs[t] == 1);
+    for (int64_t r = 0; r < (int64_t)g.m * g.n; ++r) {
+        on_first += (obs[r * g.l] == 1);
+        on_last += (obs[r * g.l + (g.l - 1)] == 1);
+    }
+    if ((rc = check_obstacles(h, "eup_set_obstacles", nsolid, on_first, on_last))) return rc;
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->wpr = (g.l + 31) / 32;
+    uint32_t* bits = nullptr;
+    if (nsolid > 0) {
+        int32_t* d_obs = nullptr;
+        CK(h, cudaMalloc(&d_obs, sizeof(int32_t) * g.N));
+        cudaError_t e = cudaMemcpyAsync(d_obs, obs, sizeof(int32_t) * g.N, cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) e = cudaMalloc(&bits, sizeof(uint32_t) * (size_t)g.m * g.n * h->wpr);
+        if (e == cudaSuccess) launch_build_mask(d_obs, g, bits, h->wpr, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        cudaFree(d_obs);
+        if (e != cudaSuccess) {
+            if (bits) cudaFree(bits);
+            return cuda_fail(h, e, "eup_set_obstacles: mask");
+        }
+    }
+    return install_mask(h, bits, nsolid);
+}
+
+int eup_build_obstacles(eup_handle* h, const eup_geometry* geo) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!geo) return fail(h, EUP_ERR_INVALID_ARG, "eup_build_obstacles: null geometry");
+    VoxShape S;
+    std::vector<double> pores;
+    std::string why;
+    if (!prepare_shape(*geo, &S, &pores, &why)) return fail(h, EUP_ERR_INVALID_ARG, "eup_build_obstacles: " + why);
+    const Geo& g = h->g;
+    CK(h, cudaStreamSynchronize(h->stream));
+    const int wpr = (g.l + 31) / 32;
+    uint32_t* bits = nullptr;
+    double* d_pores = nullptr;
+    unsigned long long* d_cnt = nullptr;
+    unsigned long long cnt[3] = {0, 0, 0};
+    cudaError_t e = cudaMalloc(&bits, sizeof(uint32_t) * (size_t)g.m * g.n * wpr);
+    if (e == cudaSuccess) e = cudaMalloc(&d_cnt, sizeof(cnt));
+    if (e == cudaSuccess && !pores.empty()) {
+        e = cudaMalloc(&d_pores, sizeof(double) * pores.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_pores, pores.data(), sizeof(double) * pores.size(), cudaMemcpyHostToDevice, h->stream);
+    }
+    S.ridge.pores = d_pores;
+    if (e == cudaSuccess) {
+        launch_voxelise(g, S, bits, wpr, h->stream);
+        launch_mask_counts(bits, g, wpr, d_cnt, h->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (d_pores) cudaFree(d_pores);
+    if (d_cnt) cudaFree(d_cnt);
+    if (e != cudaSuccess) {
+        if (bits) cudaFree(bits);
+        return cuda_fail(h, e, "eup_build_obstacles");
+    }
+    if ((rc = check_obstacles(h, "eup_build_obstacles", (int64_t)cnt[0], (int64_t)cnt[1], (int64_t)cnt[2]))) {
+        cudaFree(bits);
+        return rc;
+    }
+    h->wpr = wpr;
+    return install_mask(h, bits, (int64_t)cnt[0]);
+}
+
+int eup_get_obstacles(eup_handle* h, int32_t* obs, int64_t* nobs) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    const Geo& g = h->g;
+    if (nobs) *nobs = h->nsolid;
+    if (!obs) return EUP_OK;
+    if (!h->bits) {
+        std::memset(obs, 0, sizeof(int32_t) * (size_t)g.N);
+        return EUP_OK;
+    }
+    const int64_t rows = (int64_t)g.m * g.n;
+    std::vector<uint32_t> bits((size_t)(rows * h->wpr));
+    CK(h, cudaMemcpyAsync(bits.data(), h->bits, sizeof(uint32_t) * bits.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const int wpr = h->wpr, l = g.l;
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < rows; ++r)
+        for (int i = 0; i < l; ++i) obs[r * l + i] = (int32_t)((bits[(size_t)(r * wpr + (i >> 5))] >> (i & 31)) & 1u);
+    return EUP_OK;
+}
+
+int eup_write_obstacles(eup_handle* h, const char* path) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!path) return fail(h, EUP_ERR_INVALID_ARG, "eup_write_obstacles: null path");
+    const int64_t n = h->nsolid;
+    if (n > 2147483647LL) return fail(h, EUP_ERR_UNSUPPORTED, "eup_write_obstacles: more than 2^31-1 obstacles");
+    CK(h, cudaStreamSynchronize(h->stream));
+    int32_t* d_rec = nullptr;
+    int32_t* rec = nullptr;
+    const size_t bytes = sizeof(int32_t) * 5 * (size_t)n;
+    cudaError_t e = cudaSuccess;
+    if (n > 0) {
+        e = cudaMalloc(&d_rec, bytes);
+        if (e == cudaSuccess) e = cudaMallocHost(&rec, bytes);
+        if (e == cudaSuccess) e = obstacle_records(h->g, make_mask(h), n, d_rec, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(rec, d_rec, bytes, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+    int out = EUP_OK;
+    if (e != cudaSuccess) {
+        out = cuda_fail(h, e, "eup_write_obstacles");
+    } else {
+        FILE* f = std::fopen(path, "wb");
+        const int32_t c32 = (int32_t)n;
+        if (!f) out = fail(h, EUP_ERR_IO, std::string("eup_write_obstacles: cannot create ") + path);
+        else if (!eup_internal_write_record(f, &c32, 4) || (n > 0 && std::fwrite(rec, 1, bytes, f) != bytes))
+            out = fail(h, EUP_ERR_IO, "eup_write_obstacles: write failed");
+        if (f && std::fclose(f) != 0 && out == EUP_OK) out = fail(h, EUP_ERR_IO, "eup_write_obstacles: close failed");
+    }
+    if (d_rec) cudaFree(d_rec);
+    if (rec) cudaFreeHost(rec);
+    return out;
 }
 
 int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, int64_t itime) {

@@ -3,7 +3,9 @@
 //
 // Reads the reference's inputs unchanged: the namelist &parameters of
 // bgk.input (CODE/SRC/input.F90:46-61), the obstacle file
-// obs.0000.00000000.bin when flag1 = 1 (CODE/SRC/build.obs.F90:147-177) and,
+// obs.0000.00000000.bin when flag1 = 1 (CODE/SRC/build.obs.F90:147-177) or the
+// sphere/column/half column the reference creates when flag1 = 2 (flag2 = 1..3,
+// voxelised on the device; written back as obs.0000.00000000.bin when flag3 = 2) and,
 // with irestart = 1, restore.00.00.00.bin (CODE/SRC/restore_raw.F90:34-63).
 // The boundary preset, a compile-time -D flag in the reference
 // (CODE/SRC/build.bcond.F90), is a command-line option.  Writes:
@@ -139,7 +141,8 @@ int main(int argc, char** argv) {
     const int lx = (int)geti("lx", 0), ly = (int)geti("ly", 0), lz = (int)geti("lz", 0);
     const long itfin = geti("itfin", 0), icheck = geti("icheck", 0), itsave = geti("itsave", 0);
     const long isignal = geti("isignal", 0), irestart = geti("irestart", 0), init_v = geti("init_v", 0);
-    const long flag1 = geti("flag1", 2);
+    // CODE/SRC/input.F90:52-54 defaults: created column, VTK dump (not written here)
+    const long flag1 = geti("flag1", 2), flag2 = geti("flag2", 2), flag3 = geti("flag3", 1);
     double u0 = getd("u0", 0.0), u_inflow = 0.0, u00 = 0.0;
     if (lx < 1 || ly < 1 || lz < 1) return die("lx, ly, lz missing from " + input);
 
@@ -189,6 +192,23 @@ int main(int argc, char** argv) {
             return die("obstacle file", nullptr);
         if (eup_set_obstacles(h, obs.data()) != EUP_OK) return die("eup_set_obstacles", h);
         std::printf("INFO: num. obs       --> %lld\n", (long long)nobs);
+    } else if (flag1 == 2) {
+        // CODE/SRC/build.obs.F90:201-441: the shape is voxelised on the device
+        if (preset == "check2d") return die("flag1 = 2 with the check2d preset: the reference leaves the radius unset");
+        eup_geometry geo;
+        const int32_t variant = preset == "cylinder_inf" ? EUP_GEOM_VARIANT_CYLINDER_INF : 0;
+        if (eup_geometry_reference((int32_t)flag2, lx, ly, lz, variant, &geo) != EUP_OK)
+            return die("eup_geometry_reference", nullptr);
+        if (eup_build_obstacles(h, &geo) != EUP_OK) return die("eup_build_obstacles", h);
+        int64_t nobs = 0;
+        if (eup_get_obstacles(h, nullptr, &nobs) != EUP_OK) return die("eup_get_obstacles", h);
+        std::printf("INFO: num. obs       --> %lld\n", (long long)nobs);
+    } else if (flag1 != 0) {
+        return die("flag1 must be 0, 1 or 2");
+    }
+    if (flag3 == 2 && flag1 != 0) {  // CODE/SRC/build.obs.F90:506-541, listed on the device
+        if (eup_write_obstacles(h, "obs.0000.00000000.bin") != EUP_OK) return die("eup_write_obstacles", h);
+        std::printf("INFO: obstacle binary dump obs.0000.00000000.bin\n");
     }
     int64_t itstart = 0;
     if (irestart == 1) {

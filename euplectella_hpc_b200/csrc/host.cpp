@@ -1,5 +1,7 @@
 // Host utilities of the C ABI (no GPU): the reference's binary file formats,
-// the synthetic initial state and the synthetic geometries.
+// the synthetic initial state, the reference's created obstacles and the
+// host voxeliser (node tests shared with the device, geometry.h).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -7,6 +9,7 @@
 #include <vector>
 
 #include "../../include/eup.h"
+#include "geometry.h"
 #include "init_eq.h"
 
 using eup::splitmix64;
@@ -62,20 +65,6 @@ void init_state(int32_t l, int32_t m, int32_t n, double u_in, double amp, uint64
         eup::init_node<T>(L, u_in, amp, seed, f);
         for (int q = 0; q < 19; ++q) dst[q][L] = f[q];
     }
-}
-
-inline double wrap_pos(double a, double period) {
-    double r = std::fmod(a, period);
-    return r < 0 ? r + period : r;
-}
-
-// distance from point (u,s) to segment (u0,s0)-(u1,s1)
-inline double seg_dist(double u, double s, double u0, double s0, double u1, double s1) {
-    const double du = u1 - u0, ds = s1 - s0;
-    double t = ((u - u0) * du + (s - s0) * ds) / (du * du + ds * ds);
-    t = t < 0 ? 0 : (t > 1 ? 1 : t);
-    const double eu = u - (u0 + t * du), es = s - (s0 + t * ds);
-    return std::sqrt(eu * eu + es * es);
 }
 
 }  // namespace
@@ -176,95 +165,123 @@ int eup_init_equilibrium(int32_t l, int32_t m, int32_t n, double u_in, double am
     return EUP_OK;
 }
 
-int eup_geometry_cylinder_z(int32_t l, int32_t m, int32_t n, double xc, double yc, double r, int32_t* obs) {
-    if (!obs || l < 1 || m < 1 || n < 1 || !(r >= 0)) return herr(EUP_ERR_INVALID_ARG, "eup_geometry_cylinder_z: bad argument");
-    for (int32_t k = 1; k <= n; ++k)
-        for (int32_t j = 1; j <= m; ++j)
-            for (int32_t i = 1; i <= l; ++i) {
-                const double dx = i - xc, dy = j - yc;
-                obs[(int64_t)(i - 1) + (int64_t)l * ((j - 1) + (int64_t)m * (k - 1))] = (dx * dx + dy * dy <= r * r) ? 1 : 0;
-            }
+int eup_geometry_reference(int32_t flag2, int32_t lx, int32_t ly, int32_t lz, int32_t variant, eup_geometry* g) {
+    if (!g || lx < 1 || ly < 1 || lz < 1 || (variant & ~(EUP_GEOM_VARIANT_CYLINDER_INF | EUP_GEOM_VARIANT_TEST1)))
+        return herr(EUP_ERR_INVALID_ARG, "eup_geometry_reference: bad argument");
+    *g = eup_geometry{};
+    int32_t radius = 0;
+    // CODE/SRC/build.obs.F90:207-229 (sphere), :271-303 (column), :370-381 (half column)
+    if (flag2 == 1) {
+        g->kind = EUP_GEOM_REF_SPHERE;
+        g->center[0] = lx / 4; g->center[1] = ly / 2; g->center[2] = lz / 2;
+        radius = (variant & EUP_GEOM_VARIANT_TEST1) ? std::min(ly / 4, lz / 4) : 20;
+        g->r2_lo = (int64_t)(radius - 2) * (radius - 2);
+        g->r2_hi = (int64_t)(radius + 2) * (radius + 2);
+        return EUP_OK;
+    }
+    if (flag2 == 2 || flag2 == 3) {
+        g->kind = EUP_GEOM_REF_COLUMN;
+        g->center[0] = lx / 4; g->center[1] = ly / 2; g->center[2] = 0;
+        if (flag2 == 2 && (variant & EUP_GEOM_VARIANT_CYLINDER_INF)) {
+            radius = 100;
+            g->kstop = lz + 1;
+        } else if (flag2 == 2) {
+            radius = std::min(20, lx / 8);
+            g->kstop = lz;  // sizeZ = lz from startZ = 0: the top layer k = lz stays fluid
+        } else {
+            radius = std::min(20, lz / 8);
+            g->kstop = 60;
+        }
+        g->r2_lo = 0;
+        g->r2_hi = (int64_t)(radius + 2) * (radius + 2);
+        return EUP_OK;
+    }
+    return herr(EUP_ERR_UNSUPPORTED, "eup_geometry_reference: flag2 must be 1 (sphere), 2 (column) or 3 (half column)");
+}
+
+// The voxelisers' atan2 (geometry.h), exported for its accuracy test; not part of eup.h.
+double eup_internal_atan2_det(double y, double x) { return eup::atan2_det(y, x); }
+
+int eup_voxelise(const eup_geometry* g, int32_t l, int32_t m, int32_t n, int32_t* obs) {
+    if (!g || !obs || l < 1 || m < 1 || n < 1) return herr(EUP_ERR_INVALID_ARG, "eup_voxelise: bad argument");
+    eup::VoxShape S;
+    std::vector<double> pores;
+    std::string why;
+    if (!eup::prepare_shape(*g, &S, &pores, &why)) return herr(EUP_ERR_INVALID_ARG, "eup_voxelise: " + why);
+    S.ridge.pores = pores.data();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t row = 0; row < (int64_t)m * n; ++row) {
+        const int64_t gj = row % m + 1 + S.off[1], gk = row / m + 1 + S.off[2];
+        int32_t* o = obs + row * l;
+        for (int32_t i = 1; i <= l; ++i) o[i - 1] = eup::vox_solid(S, i + (int64_t)S.off[0], gj, gk) ? 1 : 0;
+    }
     return EUP_OK;
 }
+
+int eup_geometry_cylinder_z(int32_t l, int32_t m, int32_t n, double xc, double yc, double r, int32_t* obs) {
+    if (!obs || l < 1 || m < 1 || n < 1 || !(r >= 0)) return herr(EUP_ERR_INVALID_ARG, "eup_geometry_cylinder_z: bad argument");
+    eup_geometry g{};
+    g.kind = EUP_GEOM_CYLINDER_Z;
+    g.xc = xc; g.yc = yc; g.radius = r;
+    return eup_voxelise(&g, l, m, n, obs);
+}
+
+namespace {
+eup_geometry shell_geometry(int32_t kind, double x0, double length, double yc, double zc, double outer_d,
+                            double strut_d, double pitch, uint64_t seed) {
+    eup_geometry g{};
+    g.kind = kind;
+    g.x0 = x0; g.length = length; g.yc = yc; g.zc = zc;
+    g.outer_d = outer_d; g.strut_d = strut_d; g.pitch = pitch; g.seed = seed;
+    return g;
+}
+}  // namespace
 
 int eup_geometry_ridged_shell(int32_t l, int32_t m, int32_t n, double x0, double length, double yc, double zc,
                               double outer_d, double strut_d, double pitch, double ridge_h, double ridge_t,
                               double cap_t, double pore_d, double smooth_w, uint64_t seed, double* ns, double* dns_dh) {
-    if (!ns || l < 1 || m < 1 || n < 1 || !(ridge_h >= 0) || !(ridge_t > 0) || !(cap_t >= 0) || !(pore_d > 0))
-        return herr(EUP_ERR_INVALID_ARG, "eup_geometry_ridged_shell: bad argument");
-    const int64_t N = (int64_t)l * m * n;
-    std::vector<int32_t> shell((size_t)N);
-    int rc = eup_geometry_reticular_shell(l, m, n, x0, length, yc, zc, outer_d, strut_d, pitch, seed, shell.data());
-    if (rc != EUP_OK) return rc;
-    const double PI = 3.14159265358979323846;
-    const double Ro = 0.5 * outer_d;            // outer surface of the shell
-    const double period = 2.0 * PI * Ro;        // unrolled circumference at the outer surface
-    const double phase = period * ((double)(splitmix64(seed ^ 0xA5A5A5A5ull) >> 11) * (1.0 / 9007199254740992.0));
-    // porous cap: pores of diameter pore_d on a square grid of pitch 2*pore_d, each
-    // centre jittered by up to pore_d/4 (seeded), kept if the pore fits inside r < Ro - 2
-    std::vector<double> py, pz;
-    const double cp = 2.0 * pore_d;
-    int cnt = 0;
-    for (double a = -Ro; a <= Ro; a += cp)
-        for (double b = -Ro; b <= Ro; b += cp, ++cnt) {
-            const uint64_t h1 = splitmix64(seed + 7919ull * (uint64_t)cnt), h2 = splitmix64(h1);
-            const double ja = a + 0.25 * pore_d * (2.0 * ((double)(h1 >> 11) / 9007199254740992.0) - 1.0);
-            const double jb = b + 0.25 * pore_d * (2.0 * ((double)(h2 >> 11) / 9007199254740992.0) - 1.0);
-            if (std::sqrt(ja * ja + jb * jb) + 0.5 * pore_d < Ro - 2.0) {
-                py.push_back(ja);
-                pz.push_back(jb);
-            }
-        }
+    if (!ns || l < 1 || m < 1 || n < 1) return herr(EUP_ERR_INVALID_ARG, "eup_geometry_ridged_shell: bad argument");
+    eup_geometry g = shell_geometry(EUP_GEOM_RIDGED_SHELL, x0, length, yc, zc, outer_d, strut_d, pitch, seed);
+    g.ridge_h = ridge_h; g.ridge_t = ridge_t; g.cap_t = cap_t; g.pore_d = pore_d;
+    eup::VoxShape S;
+    std::vector<double> pores;
+    std::string why;
+    if (!eup::prepare_shape(g, &S, &pores, &why))
+        return herr(EUP_ERR_INVALID_ARG, "eup_geometry_ridged_shell: bad argument (" + why + ")");
+    S.ridge.pores = pores.data();
+    const eup::RidgeShape& R = S.ridge;
     const double w = smooth_w > 0 ? smooth_w : 0.0;
+    const double rmax = R.Ro + ridge_h + 4.0 * w + 1.0;
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int32_t k = 1; k <= n; ++k)
-        for (int32_t j = 1; j <= m; ++j) {
-            const double dy = j - yc, dz = k - zc;
-            const double r = std::sqrt(dy * dy + dz * dz);
-            const double s = wrap_pos(Ro * std::atan2(dz, dy) - phase, period);
-            for (int32_t i = 1; i <= l; ++i) {
-                const int64_t o = (int64_t)(i - 1) + (int64_t)l * ((j - 1) + (int64_t)m * (k - 1));
-                double v = shell[(size_t)o] ? 1.0 : 0.0, dv = 0.0;
-                const double u = i - x0;
-                // cap: the last cap_t of the shell's length, r < Ro, minus the pores
-                if (u >= length - cap_t && u <= length && r < Ro) {
-                    bool pore = false;
-                    for (size_t p = 0; p < py.size() && !pore; ++p) {
-                        const double ey = dy - py[p], ez = dz - pz[p];
-                        pore = ey * ey + ez * ez <= 0.25 * pore_d * pore_d;
-                    }
-                    if (!pore) v = 1.0;
+    for (int64_t row = 0; row < (int64_t)m * n; ++row) {
+        const int32_t j = (int32_t)(row % m) + 1, k = (int32_t)(row / m) + 1;
+        const double dy = j - yc, dz = k - zc;
+        for (int32_t i = 1; i <= l; ++i) {
+            const int64_t o = (int64_t)(i - 1) + (int64_t)l * row;
+            double v = eup::shell_solid(S.shell, i, j, k) ? 1.0 : 0.0, dv = 0.0;
+            const eup::RidgeHit hit = eup::ridge_test(R, i - x0, dy, dz, rmax);
+            if (hit.cap) v = 1.0;
+            // ridges: a step at Ro + ridge_h, or 0.5 (1 + tanh((Ro + h - r)/w)) with its h-derivative
+            if (hit.ridge_band) {
+                double rv, rd;
+                if (w > 0) {
+                    const double z = (R.Ro + ridge_h - hit.r) / w;
+                    rv = 0.5 * (1.0 + std::tanh(z));
+                    const double c = std::cosh(z);
+                    rd = 0.5 / (w * c * c);
+                } else {
+                    rv = (hit.r <= R.Ro + ridge_h) ? 1.0 : 0.0;
+                    rd = 0.0;
                 }
-                // two helical ridges at +-45 degrees on the outer surface: band of width
-                // ridge_t about s = +-u (mod circumference), radially from Ro to Ro + h
-                if (u >= 0 && u <= length && r > Ro - 1.0 && r < Ro + ridge_h + 4.0 * w + 1.0) {
-                    double dperp = 1e30;
-                    for (int sg = -1; sg <= 1; sg += 2) {
-                        double d = wrap_pos(s - sg * u, period);
-                        d = std::fmin(d, period - d) / std::sqrt(2.0);
-                        dperp = std::fmin(dperp, d);
-                    }
-                    if (dperp <= 0.5 * ridge_t && r >= Ro - 0.5) {
-                        double rv, rd;
-                        if (w > 0) {
-                            const double z = (Ro + ridge_h - r) / w;
-                            rv = 0.5 * (1.0 + std::tanh(z));
-                            const double c = std::cosh(z);
-                            rd = 0.5 / (w * c * c);
-                        } else {
-                            rv = (r <= Ro + ridge_h) ? 1.0 : 0.0;
-                            rd = 0.0;
-                        }
-                        if (rv > v) {
-                            v = rv;
-                            dv = rd;
-                        }
-                    }
+                if (rv > v) {
+                    v = rv;
+                    dv = rd;
                 }
-                ns[o] = v;
-                if (dns_dh) dns_dh[o] = dv;
             }
+            ns[o] = v;
+            if (dns_dh) dns_dh[o] = dv;
         }
+    }
     return EUP_OK;
 }
 
@@ -272,54 +289,8 @@ int eup_geometry_reticular_shell(int32_t l, int32_t m, int32_t n, double x0, dou
                                  double outer_d, double strut_d, double pitch, uint64_t seed, int32_t* obs) {
     if (!obs || l < 1 || m < 1 || n < 1 || !(outer_d > strut_d) || !(strut_d > 0) || !(pitch > 0) || !(length > 0))
         return herr(EUP_ERR_INVALID_ARG, "eup_geometry_reticular_shell: bad argument");
-    const double PI = 3.14159265358979323846;
-    const double rs = 0.5 * strut_d;
-    const double Rc = 0.5 * outer_d - rs;                 // strut centreline radius
-    int ntheta = (int)std::lround(2.0 * PI * Rc / pitch);
-    if (ntheta < 3) ntheta = 3;
-    const double period = 2.0 * PI * Rc;                  // unrolled circumference
-    const double ps = period / ntheta;                    // arc pitch
-    const int ncell = (int)std::lround(length / pitch);   // cells along x
-    const double ulen = ncell * pitch;
-    const double phase = ps * ((double)(splitmix64(seed) >> 11) * (1.0 / 9007199254740992.0));
-    std::memset(obs, 0, sizeof(int32_t) * (size_t)l * m * n);
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int32_t k = 1; k <= n; ++k)
-        for (int32_t j = 1; j <= m; ++j) {
-            const double dy = j - yc, dz = k - zc;
-            const double r = std::sqrt(dy * dy + dz * dz);
-            const double dr = r - Rc;
-            if (std::fabs(dr) > rs) continue;
-            const double s = wrap_pos(Rc * std::atan2(dz, dy) - phase, period);
-            const int b = (int)std::floor(s / ps);
-            for (int32_t i = 1; i <= l; ++i) {
-                const double u = i - x0;
-                if (u < -rs || u > ulen + rs) continue;
-                // longitudinal struts s = b*ps, running u in [0, ulen]
-                const double uc = u < 0 ? 0 : (u > ulen ? ulen : u);
-                const double ds_l = std::fmin(s - b * ps, (b + 1) * ps - s);
-                double d = std::sqrt(ds_l * ds_l + (u - uc) * (u - uc));
-                // rings u = a*pitch, a = 0..ncell
-                int a = (int)std::lround(u / pitch);
-                a = a < 0 ? 0 : (a > ncell ? ncell : a);
-                d = std::fmin(d, std::fabs(u - a * pitch));
-                // both diagonals of the cells with (ca + cb) even
-                const int ca0 = (int)std::floor(u / pitch);
-                for (int ca = ca0 - 1; ca <= ca0 + 1; ++ca) {
-                    if (ca < 0 || ca >= ncell) continue;
-                    for (int cb = b - 1; cb <= b + 1; ++cb) {
-                        const int cbw = ((cb % ntheta) + ntheta) % ntheta;
-                        if (((ca + cbw) & 1) != 0) continue;
-                        const double u0 = ca * pitch, s0 = cb * ps;
-                        d = std::fmin(d, seg_dist(u, s, u0, s0, u0 + pitch, s0 + ps));
-                        d = std::fmin(d, seg_dist(u, s, u0, s0 + ps, u0 + pitch, s0));
-                    }
-                }
-                if (dr * dr + d * d <= rs * rs)
-                    obs[(int64_t)(i - 1) + (int64_t)l * ((j - 1) + (int64_t)m * (k - 1))] = 1;
-            }
-        }
-    return EUP_OK;
+    const eup_geometry g = shell_geometry(EUP_GEOM_RETICULAR_SHELL, x0, length, yc, zc, outer_d, strut_d, pitch, seed);
+    return eup_voxelise(&g, l, m, n, obs);
 }
 
 }  // extern "C"

@@ -164,6 +164,14 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
 
 // Set-up kernels (k_setup.cu).
 void launch_build_mask(const int32_t* obs, const Geo& g, uint32_t* bits, int wpr, cudaStream_t st);
+// Device voxeliser (geometry.h): the bit-packed mask of shape S.
+struct VoxShape;
+void launch_voxelise(const Geo& g, const VoxShape& S, uint32_t* bits, int wpr, cudaStream_t st);
+// out[0..2] = solid voxels, solid voxels at i = 1, at i = l.
+void launch_mask_counts(const uint32_t* bits, const Geo& g, int wpr, unsigned long long* out, cudaStream_t st);
+// The nsolid solid voxels of the mask, i fastest, as Fortran records [12][i][j][k][12]
+// (rec holds 5 nsolid int32); synchronises st.
+cudaError_t obstacle_records(const Geo& g, const Mask& mk, int64_t nsolid, int32_t* rec, cudaStream_t st);
 void launch_flag_boundary_solid(const Geo& g, const Mask& mk, uint8_t* flags, cudaStream_t st);
 void launch_links(const Geo& g, const Mask& mk, uint32_t* links, cudaStream_t st);
 // Neighbour classification of each boundary-solid voxel: bit q (0..17) neighbour

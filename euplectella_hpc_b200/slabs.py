@@ -129,6 +129,12 @@ class SlabSolver:
     def set_obstacles(self, obs_global: np.ndarray):
         self.solver.set_obstacles(slab_obstacles(obs_global, self.x0, self.nx))
 
+    def build_obstacles(self, geom):
+        """Voxelises the global shape `geom` (an eup_geometry in global coordinates) on this
+        slab's GPU: the slab's block is the shape shifted by x0 - 1, as the reference offsets a
+        block by mpicoords * l (CODE/SRC/build.obs.F90:233-235)."""
+        self.solver.build_obstacles(geom.shifted((geom.offset[0] + self.x0 - 1, geom.offset[1], geom.offset[2])))
+
     def upload(self, pops_global: np.ndarray, itime: int = 0):
         self.solver.upload(slab_state(pops_global, self.x0, self.nx), itime)
 

@@ -14,16 +14,20 @@ Adjoint study (192x96x96 partial bounce-back channel):
     python -m euplectella_hpc_b200.studies --adjoint --steps 4000 [--fd 32]
 Production forward runs: python -m euplectella_hpc_b200.studies --production shell|ridged [--steps N]
 Ridge-height gradient:    python -m euplectella_hpc_b200.studies --ridge-adjoint
+Obstacle masks, host voxeliser + eup_set_obstacles against eup_build_obstacles:
+                          python -m euplectella_hpc_b200.studies --voxelise
 """
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
+import os
 import time
 
 import numpy as np
 
-from . import BF16_DEV, FP16_DEV, FP32, FP64, EupError, Solver
+from . import BF16_DEV, FP16_DEV, FP32, FP64, EupError, Solver, voxelise
 from .workloads import cylinder_channel
 
 CX = np.array([1, 1, 1, 1, 1, 0, 0, 0, 0, -1, -1, -1, -1, -1, 0, 0, 0, 0, 0], dtype=np.float64)
@@ -197,18 +201,18 @@ def production_run(which="shell", steps=None, precision=None, chunk=1000):
     velocity inside the body cavity at the end."""
     from .workloads import U_IN, PERTURBATION, reticular_shell_channel, ridged_shell_channel
     if which == "shell":
-        wl = reticular_shell_channel(precision=FP32 if precision is None else precision)
+        wl = reticular_shell_channel(precision=FP32 if precision is None else precision, host_mask=False)
     else:
-        wl = ridged_shell_channel(precision=FP16_DEV if precision is None else precision)
+        wl = ridged_shell_channel(precision=FP16_DEV if precision is None else precision, host_mask=False)
     steps = wl.steps if steps is None else steps
     c = wl.cfg
     sbytes = {FP32: 4, FP64: 8, FP16_DEV: 2, BF16_DEV: 2}[c.precision]
     peak, peak_kind = hbm_peak_gbs()
-    out = {"workload": wl.name, "nodes": wl.nodes, "steps": steps, "precision": c.precision, "nu": c.svisc,
-           "solid_voxels": int(wl.obs.sum())}
+    out = {"workload": wl.name, "nodes": wl.nodes, "steps": steps, "precision": c.precision, "nu": c.svisc}
     cd = np.zeros(steps + 1)
     with Solver(c) as s:
-        s.set_obstacles(wl.obs)
+        s.build_obstacles(wl.geometry)  # voxelised on the device: no host mask, no mask copy
+        out["solid_voxels"] = s.obstacle_count()
         s.init_state(U_IN, PERTURBATION, wl.seed)
         done, wall = 0, 0.0
         while done < steps:
@@ -290,6 +294,50 @@ def ridge_adjoint(scale=0.25, re=500.0, steps=2500, avg_steps=625, checkpoints=6
     return out
 
 
+def voxelise_timing(repeats=3):
+    """The production obstacle masks (768x384x384 reticular shell, 1024x512x512 ridged shell)
+    built and installed two ways, best of `repeats` wall times: the host voxeliser (OpenMP, all
+    host threads) followed by eup_set_obstacles, which copies the int32 mask (4 B per node) to
+    the device and packs it; and eup_build_obstacles, which voxelises on the device into the
+    packed mask.  Also the obstacle file: eup_write_obs_file from the host mask against
+    eup_write_obstacles, listed on the device."""
+    import tempfile
+    from . import lib
+    from .workloads import reticular_shell_channel, ridged_shell_channel
+    rows = []
+    for wl in (reticular_shell_channel(host_mask=False), ridged_shell_channel(host_mask=False)):
+        c = dataclasses.replace(wl.cfg, precision=FP16_DEV)
+        row = {"workload": wl.name, "nodes": wl.nodes, "host_threads": os.cpu_count()}
+        t_dev, t_vox, t_set, t_wdev, t_whost = [], [], [], [], []
+        with Solver(c) as s, tempfile.TemporaryDirectory() as tmp:
+            s.build_obstacles(wl.geometry)  # warm-up: first allocations, module load
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                s.build_obstacles(wl.geometry)
+                t_dev.append(time.perf_counter() - t0)
+            row["solid_voxels"] = s.obstacle_count()
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                obs = voxelise(wl.geometry, c.lx, c.ly, c.lz)
+                t1 = time.perf_counter()
+                s.set_obstacles(obs)
+                t_vox.append(t1 - t0)
+                t_set.append(time.perf_counter() - t1)
+            path = os.path.join(tmp, "obs.bin")
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                s.write_obstacles(path)
+                t_wdev.append(time.perf_counter() - t0)
+                t0 = time.perf_counter()
+                lib.eup_write_obs_file(path.encode(), c.lx, c.ly, c.lz, obs.ctypes.data)
+                t_whost.append(time.perf_counter() - t0)
+        row.update(device_build_s=min(t_dev), host_voxelise_s=min(t_vox), host_set_obstacles_s=min(t_set),
+                   host_total_s=min(a + b for a, b in zip(t_vox, t_set)), device_write_s=min(t_wdev),
+                   host_write_s=min(t_whost))
+        rows.append(row)
+    return rows
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=20000)
@@ -303,7 +351,16 @@ def main():
     ap.add_argument("--precision", choices=["fp32", "fp64", "fp16", "bf16"], default=None,
                     help="storage of a production run (default: the case's own)")
     ap.add_argument("--chunk", type=int, default=1000, help="steps between divergence checks of a production run")
+    ap.add_argument("--voxelise", action="store_true", help="time the production obstacle masks, host against device")
     args = ap.parse_args()
+    if args.voxelise:
+        rows = voxelise_timing()
+        for r in rows:
+            print(json.dumps(r))
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(rows, f, indent=1)
+        return
     if args.production or args.ridge_adjoint:
         prec = {None: None, "fp32": FP32, "fp64": FP64, "fp16": FP16_DEV, "bf16": BF16_DEV}[args.precision]
         res = production_run(args.production, None if args.steps == 20000 else args.steps, prec, args.chunk) \

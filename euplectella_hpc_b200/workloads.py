@@ -12,8 +12,8 @@ import math
 
 import numpy as np
 
-from . import (FP16_DEV, FREESLIP, FP32, INFLOW, OUTFLOW, PERIODIC, Config, geometry_cylinder_z,
-               geometry_reticular_shell, geometry_ridged_shell, init_equilibrium)
+from . import (FP16_DEV, FREESLIP, FP32, INFLOW, OUTFLOW, PERIODIC, Config, Geometry, geometry_ridged_shell,
+               init_equilibrium, voxelise)
 
 U_IN = 0.05          # inlet velocity of every configuration
 PERTURBATION = 1e-4  # amplitude of the seeded initial velocity perturbation
@@ -33,6 +33,7 @@ class Workload:
     seed: int
     probes: list = dataclasses.field(default_factory=list)
     cavity: np.ndarray | None = None  # boolean mask (n, m, l) of the body cavity
+    geometry: Geometry | None = None  # the body as a voxel shape (Solver.build_obstacles builds obs on the device)
 
     def initial_state(self, dtype=np.float32) -> np.ndarray:
         c = self.cfg
@@ -50,17 +51,19 @@ def cylinder_channel(lx=256, ly=128, lz=64, d=20.0, xc=64.0, yc=64.0, re=100.0, 
     nu = svisc_for(re, U_IN, d)
     cfg = Config(lx, ly, lz, bc=(OUTFLOW, INFLOW, FREESLIP, FREESLIP, PERIODIC, PERIODIC), svisc=nu,
                  u_inflow=U_IN, precision=precision, cd_rho0=1.0, cd_uref=U_IN, cd_length=d, cd_span=float(lz))
-    obs = geometry_cylinder_z(lx, ly, lz, xc, yc, 0.5 * d)
+    geom = Geometry.cylinder_z(xc, yc, 0.5 * d)
+    obs = voxelise(geom, lx, ly, lz)
     probes = [(int(xc + 2 * d), int(yc), lz // 2), (int(xc + 4 * d), int(yc + d // 2), lz // 2)]
-    return Workload("cylinder_256x128x64_re100", cfg, obs, steps, seed, probes)
+    return Workload("cylinder_256x128x64_re100", cfg, obs, steps, seed, probes, geometry=geom)
 
 
 def reticular_shell_channel(lx=768, ly=384, lz=384, outer_d=96.0, length=256.0, strut_d=4.0, pitch=16.0,
-                            re=2000.0, steps=20000, seed=2024, precision=FP32) -> Workload:
+                            re=2000.0, steps=20000, seed=2024, precision=FP32, host_mask=True) -> Workload:
     """Channel 768x384x384 with a reticular cylindrical shell (outer D 96, length 256,
     axis x, struts d=4 at pitch 16 plus diagonals in alternate cells), inlet 0.05,
     free-slip y and z (the reference's FREESLIP preset, CODE/SRC/build.bcond.F90:286-315),
-    Re 2000 on the shell diameter."""
+    Re 2000 on the shell diameter.  host_mask=False leaves obs None (build it on the device
+    from `geometry`)."""
     nu = svisc_for(re, U_IN, outer_d)
     x0 = lx / 4.0
     yc = zc = (ly + 1) / 2.0
@@ -68,7 +71,8 @@ def reticular_shell_channel(lx=768, ly=384, lz=384, outer_d=96.0, length=256.0, 
     cfg = Config(lx, ly, lz, bc=(OUTFLOW, INFLOW, FREESLIP, FREESLIP, FREESLIP, FREESLIP), svisc=nu,
                  u_inflow=U_IN, precision=precision, cd_rho0=1.0, cd_uref=U_IN, cd_length=outer_d,
                  cd_span=area / outer_d)
-    obs = geometry_reticular_shell(lx, ly, lz, x0, length, yc, zc, outer_d, strut_d, pitch, seed)
+    geom = Geometry.reticular_shell(x0, length, yc, zc, outer_d, strut_d, pitch, seed)
+    obs = voxelise(geom, lx, ly, lz) if host_mask else None
     yi, zi = int(round(yc)), int(round(zc))
     probes = [(int(x0 - 32), yi, zi), (int(x0 + length / 2), yi, zi), (int(x0 + length + 64), yi, zi)]
     # cavity: inside the strut centreline radius minus a strut radius, within the shell's x span
@@ -76,7 +80,7 @@ def reticular_shell_channel(lx=768, ly=384, lz=384, outer_d=96.0, length=256.0, 
                           sparse=True)
     rin = 0.5 * outer_d - strut_d
     cavity = ((j - yc) ** 2 + (k - zc) ** 2 < rin * rin) & (i >= x0) & (i <= x0 + length)
-    return Workload("reticular_shell_768x384x384_re2000", cfg, obs, steps, seed, probes, cavity)
+    return Workload("reticular_shell_768x384x384_re2000", cfg, obs, steps, seed, probes, cavity, geom)
 
 
 def _gauss(seed: int, n: int) -> np.ndarray:
@@ -141,10 +145,13 @@ class RidgedShell:
     def args(self, lx, ly, lz):
         return (lx, ly, lz, self.x0, self.length, self.yc, self.zc, self.outer_d, self.strut_d, self.pitch)
 
+    def geometry(self) -> Geometry:
+        return Geometry.ridged_shell(self.x0, self.length, self.yc, self.zc, self.outer_d, self.strut_d, self.pitch,
+                                     self.ridge_h, self.ridge_t, self.cap_t, self.pore_d, self.seed)
+
     def mask(self, lx, ly, lz) -> np.ndarray:
-        ns = geometry_ridged_shell(*self.args(lx, ly, lz), self.ridge_h, self.ridge_t, self.cap_t, self.pore_d, 0.0,
-                                   self.seed)
-        return (ns >= 0.5).astype(np.int32)
+        """The 0/1 obstacle: the field below at smooth_w = 0, thresholded at 1/2."""
+        return voxelise(self.geometry(), lx, ly, lz)
 
     def field(self, lx, ly, lz, smooth_w, ridge_h=None):
         """Solid fraction with smoothed ridges and d n_s / d ridge_h."""
@@ -154,7 +161,7 @@ class RidgedShell:
 
 
 def ridged_shell_channel(lx=1024, ly=512, lz=512, scale=1.0, re=2000.0, steps=10000, seed=2025,
-                         precision=FP16_DEV) -> Workload:
+                         precision=FP16_DEV, host_mask=True) -> Workload:
     """Channel 1024x512x512 holding the reticular shell of the 768x384x384 case (outer D 96,
     length 256, struts d=4 at pitch 16) plus two counter-rotating 45-degree helical ridges
     (height 8, thickness 4) and a seeded porous cap (thickness 4, pores of diameter 10 on a
@@ -162,7 +169,8 @@ def ridged_shell_channel(lx=1024, ly=512, lz=512, scale=1.0, re=2000.0, steps=10
     diameter; FP16-stored deviations.  (A cap with 6-lu pores makes the BGK run diverge within
     300 steps in every precision, FP64 included: the jets through pores that small are not
     resolved at this viscosity.)  `scale` shrinks the channel and every length of the body
-    together (the viscosity follows Re on the scaled diameter)."""
+    together (the viscosity follows Re on the scaled diameter).  host_mask=False leaves obs None
+    (build it on the device from `geometry`)."""
     lx, ly, lz = int(round(lx * scale)), int(round(ly * scale)), int(round(lz * scale))
     body = RidgedShell(x0=lx / 4.0, length=256.0 * scale, yc=(ly + 1) / 2.0, zc=(lz + 1) / 2.0, outer_d=96.0 * scale,
                        strut_d=4.0 * scale, pitch=16.0 * scale, ridge_h=8.0 * scale, ridge_t=4.0 * scale,
@@ -172,7 +180,7 @@ def ridged_shell_channel(lx=1024, ly=512, lz=512, scale=1.0, re=2000.0, steps=10
     cfg = Config(lx, ly, lz, bc=(OUTFLOW, INFLOW, FREESLIP, FREESLIP, FREESLIP, FREESLIP), svisc=nu,
                  u_inflow=U_IN, precision=precision, cd_rho0=1.0, cd_uref=U_IN, cd_length=body.outer_d,
                  cd_span=area / body.outer_d)
-    obs = body.mask(lx, ly, lz)
+    obs = body.mask(lx, ly, lz) if host_mask else None
     yi, zi = int(round(body.yc)), int(round(body.zc))
     probes = [(int(body.x0 - 32 * scale), yi, zi), (int(body.x0 + body.length / 2), yi, zi),
               (int(body.x0 + body.length + 64 * scale), yi, zi)]
@@ -180,6 +188,7 @@ def ridged_shell_channel(lx=1024, ly=512, lz=512, scale=1.0, re=2000.0, steps=10
                           sparse=True)
     rin = 0.5 * body.outer_d - body.strut_d
     cavity = ((j - body.yc) ** 2 + (k - body.zc) ** 2 < rin * rin) & (i >= body.x0) & (i <= body.x0 + body.length)
-    wl = Workload(f"ridged_shell_{lx}x{ly}x{lz}_re{int(re)}", cfg, obs, steps, seed, probes, cavity)
+    wl = Workload(f"ridged_shell_{lx}x{ly}x{lz}_re{int(re)}", cfg, obs, steps, seed, probes, cavity,
+                  body.geometry())
     wl.body = body
     return wl

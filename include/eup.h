@@ -116,6 +116,66 @@ const char* eup_last_error(const eup_handle* h);
  * iteration order of its bounce-back loop. */
 int eup_set_obstacles(eup_handle* h, const int32_t* obs);
 
+/* ---- obstacles built on the device ------------------------------------------ */
+
+/* Voxel shapes (eup_geometry.kind). */
+enum {
+    EUP_GEOM_NONE = 0,            /* no solid voxel */
+    EUP_GEOM_REF_SPHERE = 1,      /* spherical shell, CODE/SRC/build.obs.F90:207-268 (flag2 = 1) */
+    EUP_GEOM_REF_COLUMN = 2,      /* z-column, CODE/SRC/build.obs.F90:271-441 (flag2 = 2 and 3) */
+    EUP_GEOM_CYLINDER_Z = 3,      /* solid circular cylinder along z, as eup_geometry_cylinder_z */
+    EUP_GEOM_RETICULAR_SHELL = 4, /* as eup_geometry_reticular_shell */
+    EUP_GEOM_RIDGED_SHELL = 5     /* eup_geometry_ridged_shell with smooth_w = 0, as a 0/1 mask */
+};
+
+/* A voxel shape in global node coordinates (global index = local index + offset). */
+typedef struct eup_geometry {
+    int32_t kind;
+    int32_t offset[3];  /* global index of this lattice's node (1,1,1) minus 1: the reference's
+                           mpicoords(d) * (l, m, n) (CODE/SRC/build.obs.F90:233-235), an x-slab's x0 - 1 */
+    /* REF_SPHERE: solid where d2 = |center - global index|^2 (integers) satisfies
+     * r2_lo < d2 < r2_hi.  REF_COLUMN: the same in x and y with r2_lo <= d2 < r2_hi, for
+     * center[2] <= global k < kstop.  eup_geometry_reference fills them as the reference does. */
+    int32_t center[3];
+    int32_t kstop;
+    int64_t r2_lo, r2_hi;
+    /* CYLINDER_Z: xc, yc, radius.  Shells: x0, length, yc, zc, outer_d, strut_d, pitch, seed;
+     * RIDGED_SHELL also ridge_h, ridge_t, cap_t, pore_d (the eup_geometry_* helpers' arguments). */
+    double xc, yc, zc, radius;
+    double x0, length, outer_d, strut_d, pitch;
+    double ridge_h, ridge_t, cap_t, pore_d;
+    uint64_t seed;
+} eup_geometry;
+
+/* Variant bits of eup_geometry_reference: compile-time choices of the reference's build_obs. */
+enum { EUP_GEOM_VARIANT_CYLINDER_INF = 1, EUP_GEOM_VARIANT_TEST1 = 2 };
+
+/* The obstacle CODE/SRC/build.obs.F90 creates for flag1 = 2 on a global lattice
+ * lx x ly x lz: flag2 = 1 sphere (radius 20; min(ly/4, lz/4) with TEST1), 2 column
+ * (radius min(20, lx/8) over 1 <= k < lz; radius 100 over every k with CYLINDER_INF),
+ * 3 half column (radius min(20, lz/8), 1 <= k < 60), centred at (lx/4, ly/2[, lz/2]),
+ * offset 0.  No GPU.  -DCHECK2D leaves the reference's radius unset and is not offered. */
+int eup_geometry_reference(int32_t flag2, int32_t lx, int32_t ly, int32_t lz, int32_t variant,
+                           eup_geometry* g);
+
+/* Voxelises g on the device straight into the handle's bit-packed mask (one warp
+ * per 32 nodes of an x row; no host array, no host-to-device copy of a mask) and
+ * installs it with the checks of eup_set_obstacles.  The mask equals
+ * eup_voxelise's bit for bit. */
+int eup_build_obstacles(eup_handle* h, const eup_geometry* g);
+
+/* The installed mask as obs(1:l,1:m,1:n) (obs may be NULL) and its number of
+ * solid voxels (nobs may be NULL).  The bit-packed mask crosses to the host. */
+int eup_get_obstacles(eup_handle* h, int32_t* obs, int64_t* nobs);
+
+/* Writes the installed mask as an obstacle file (CODE/SRC/build.obs.F90:506-541:
+ * a record with the count, then one (i,j,k) record per solid voxel, i fastest).
+ * The list is compacted and laid out as records on the device and crosses to the
+ * host in one copy.  The count written is the number of records: the reference
+ * writes that count minus 100 for the obstacles it creates (its counter starts
+ * at -100, CODE/SRC/build.obs.F90:68), so reading its file back drops 100 voxels. */
+int eup_write_obstacles(eup_handle* h, const char* path);
+
 /* Copies the 19 haloed host arrays (elem_bytes 4 or 8) into device storage:
  * interior nodes into the lattice (converted to the storage precision), halo
  * nodes into the persistent halo shell.  Replaces the host-to-device copy of
@@ -351,6 +411,10 @@ int eup_init_equilibrium(int32_t l, int32_t m, int32_t n, double u_in, double am
                          int32_t elem_bytes, void* const pops[19]);
 
 /* ---- synthetic geometries (no GPU) ---------------------------------------- */
+
+/* The host voxeliser: obs(1:l,1:m,1:n) of shape g on this lattice (OpenMP).  The
+ * same node tests as eup_build_obstacles, so the two masks are identical. */
+int eup_voxelise(const eup_geometry* g, int32_t l, int32_t m, int32_t n, int32_t* obs);
 
 /* Solid circular cylinder with axis along z: node (i,j,k) is solid when
  * (i-xc)^2 + (j-yc)^2 <= r^2 (1-based node coordinates). */

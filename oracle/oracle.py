@@ -213,3 +213,53 @@ def boundary_solid(p, obs) -> np.ndarray:
 
 def nthreads() -> int:
     return int(lib().orc_nthreads())
+
+
+def created_obstacle(flag2, lx, ly, lz, l, m, n, mpicoords=(0, 0, 0), cylinder_inf=False, test1=False):
+    """Obstacle of CODE/SRC/build.obs.F90 for flag1 = 2 on the local block (l, m, n) at
+    process coordinates mpicoords of a global lx x ly x lz lattice, restated line by line:
+    flag2 = 1 sphere (:207-268), 2 column (:271-367), 3 half column (:370-441), with d2
+    formed in integers and compared in the reference's single-precision reals.  Returns
+    (obs (n, m, l) int32, nobs) where nobs is the reference's counter after the loop: it
+    starts at -100 (:68), so it is the number of solid voxels minus 100."""
+    f32 = np.float32
+    offx, offy, offz = mpicoords[0] * l, mpicoords[1] * m, mpicoords[2] * n
+    k, j, i = np.meshgrid(np.arange(1, n + 1), np.arange(1, m + 1), np.arange(1, l + 1), indexing="ij")
+    if flag2 == 1:
+        icoord, jcoord, kcoord = lx // 4, ly // 2, lz // 2
+        radius = min(ly // 4, lz // 4) if test1 else 20
+        R = f32(radius * 1.0)
+        R2a, R2b = f32((R - f32(2)) * (R - f32(2))), f32((R + f32(2)) * (R + f32(2)))
+        d2i = (icoord - (i + offx)) ** 2 + (jcoord - (j + offy)) ** 2 + (kcoord - (k + offz)) ** 2
+        d2 = d2i.astype(f32)
+        obs = (d2 > R2a) & (d2 < R2b)
+    elif flag2 in (2, 3):
+        if flag2 == 2 and cylinder_inf:
+            radius, icoord, jcoord, kcoord, size_z = 100, lx // 4, ly // 2, 0, lz + 1
+        elif flag2 == 2:
+            radius, icoord, jcoord, kcoord, size_z = min(20, lx // 8), lx // 4, ly // 2, 0, lz
+        else:
+            radius, icoord, jcoord, kcoord, size_z = min(20, lz // 8), lx // 4, ly // 2, 0, 60
+        start_z = kcoord - mpicoords[2] * n
+        stop_z = start_z + size_z
+        R = f32(radius * 1.0)
+        R2a, R2b = f32(0), f32((R + f32(2)) * (R + f32(2)))
+        d2 = ((icoord - (i + offx)) ** 2 + (jcoord - (j + offy)) ** 2).astype(f32)
+        obs = (k >= start_z) & (k < stop_z) & (d2 >= R2a) & (d2 < R2b)
+    else:
+        raise ValueError("flag2 must be 1, 2 or 3")
+    obs = obs.astype(np.int32)
+    return obs, int(obs.sum()) - 100
+
+
+def obstacle_file_bytes(obs, count=None) -> bytes:
+    """The obstacle dump of CODE/SRC/build.obs.F90:506-541 as gfortran writes it: a record
+    holding the count, then one (i, j, k) record per solid voxel, i fastest.  count defaults
+    to the number of solid voxels."""
+    kk, jj, ii = np.nonzero(np.asarray(obs) == 1)  # C order over (n, m, l): i fastest
+    nobs = len(ii) if count is None else count
+    rec = np.empty((len(ii), 5), dtype=np.int32)
+    rec[:, 0] = rec[:, 4] = 12
+    rec[:, 1], rec[:, 2], rec[:, 3] = ii + 1, jj + 1, kk + 1
+    head = np.array([4, nobs, 4], dtype=np.int32)
+    return head.tobytes() + rec.tobytes()

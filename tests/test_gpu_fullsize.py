@@ -62,3 +62,16 @@ def test_fullsize_fp16_tracks_fp32(eup, require_gpu, shell):
     # open inflow/outflow system: the total mass follows the (slightly different) flow
     assert abs(m16[0] - m32[0]) / m32[0] < 2e-4
     assert abs(f16[0] - f32[0]) / abs(f32[0]) < 5e-3
+
+
+def test_fullsize_device_voxeliser(eup, require_gpu, shell):
+    """The production masks built on the device equal the host voxeliser's: the 768x384x384
+    reticular shell (113 M voxels) and the 1024x512x512 ridged shell (268 M voxels)."""
+    import dataclasses
+    from euplectella_hpc_b200 import workloads
+    for wl in (shell, workloads.ridged_shell_channel()):
+        with eup.Solver(dataclasses.replace(wl.cfg, precision=eup.FP16_DEV)) as s:
+            s.build_obstacles(wl.geometry)
+            got, nobs = s.obstacles()
+        assert nobs == int(wl.obs.sum()) > 0, wl.name
+        assert np.array_equal(got, wl.obs), (wl.name, int((got != wl.obs).sum()))
