@@ -26,6 +26,23 @@
          integer(c_int64_t) :: series_capacity
       end type eup_config
 
+      ! voxel shapes of eup_geometry%kind and the variant bits of eup_geometry_reference
+      integer(c_int), parameter :: EUP_GEOM_NONE = 0, EUP_GEOM_REF_SPHERE = 1, EUP_GEOM_REF_COLUMN = 2
+      integer(c_int), parameter :: EUP_GEOM_CYLINDER_Z = 3, EUP_GEOM_RETICULAR_SHELL = 4
+      integer(c_int), parameter :: EUP_GEOM_RIDGED_SHELL = 5
+      integer(c_int), parameter :: EUP_GEOM_VARIANT_CYLINDER_INF = 1, EUP_GEOM_VARIANT_TEST1 = 2
+
+      type, bind(c) :: eup_geometry
+         integer(c_int32_t) :: kind
+         integer(c_int32_t) :: offset(3)      ! mpicoords(d) * (l, m, n), as build_obs
+         integer(c_int32_t) :: center(3), kstop
+         integer(c_int64_t) :: r2_lo, r2_hi
+         real(c_double)     :: xc, yc, zc, radius
+         real(c_double)     :: x0, length, outer_d, strut_d, pitch
+         real(c_double)     :: ridge_h, ridge_t, cap_t, pore_d
+         integer(c_int64_t) :: seed
+      end type eup_geometry
+
       type, bind(c) :: eup_adjoint_config
          integer(c_int32_t) :: nsteps, avg_steps, checkpoints, reserved
       end type eup_adjoint_config
@@ -136,6 +153,39 @@
             real(c_double)                :: objective
             real(c_double)                :: grad_ns(*)
             real(c_double)                :: stats(8)
+         end function
+
+         integer(c_int) function eup_geometry_reference(flag2, lx, ly, lz, variant, g) &
+                                 bind(c, name="eup_geometry_reference")
+            import :: c_int, c_int32_t, eup_geometry
+            integer(c_int32_t), value :: flag2, lx, ly, lz, variant
+            type(eup_geometry)        :: g
+         end function
+
+         integer(c_int) function eup_build_obstacles(h, g) bind(c, name="eup_build_obstacles")
+            import :: c_int, c_ptr, eup_geometry
+            type(c_ptr), value             :: h
+            type(eup_geometry), intent(in) :: g
+         end function
+
+         integer(c_int) function eup_get_obstacles(h, obs, nobs) bind(c, name="eup_get_obstacles")
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: h
+            type(c_ptr), value :: obs               ! c_loc(obs(1,1,1)) or c_null_ptr
+            integer(c_int64_t) :: nobs
+         end function
+
+         integer(c_int) function eup_write_obstacles(h, path) bind(c, name="eup_write_obstacles")
+            import :: c_int, c_ptr, c_char
+            type(c_ptr), value :: h
+            character(kind=c_char), intent(in) :: path(*)   ! 'obs.0000.00000000.bin'//c_null_char
+         end function
+
+         integer(c_int) function eup_voxelise(g, l, m, n, obs) bind(c, name="eup_voxelise")
+            import :: c_int, c_int32_t, c_ptr, eup_geometry
+            type(eup_geometry), intent(in) :: g
+            integer(c_int32_t), value      :: l, m, n
+            type(c_ptr), value             :: obs
          end function
 
          integer(c_int) function eup_read_obs_file(path, l, m, n, obs, nobs) bind(c, name="eup_read_obs_file")

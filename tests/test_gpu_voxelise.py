@@ -126,10 +126,14 @@ def test_build_obstacles_checks_keep_the_previous_mask(eup, require_gpu):
 
 
 def test_slabs_build_their_block(eup, require_gpu):
+    """Each x-slab voxelises its own block of the global shape (offset x0 - 1).  The shell
+    lies inside the middle slab (columns 81..160): a solid next to an exchange face is
+    rejected, as with eup_set_obstacles."""
     from euplectella_hpc_b200.slabs import SlabSolver, slab_obstacles
-    cfg = eup.Config(150, 64, 60, bc=(5, 4, 3, 3, 3, 3), u_inflow=0.05)
-    g = eup.Geometry.reticular_shell(30, 80, 32.5, 30.0, 40, 4, 12, 3)
+    cfg = eup.Config(240, 64, 60, bc=(5, 4, 3, 3, 3, 3), u_inflow=0.05)
+    g = eup.Geometry.reticular_shell(95, 48, 32.5, 30.0, 40, 4, 12, 3)
     full = eup.voxelise(g, cfg.lx, cfg.ly, cfg.lz)
+    assert full[:, :, 92:146].sum() == full.sum() > 0
     for rank in range(3):
         s = SlabSolver(cfg, rank, 3)
         try:
@@ -137,6 +141,13 @@ def test_slabs_build_their_block(eup, require_gpu):
             assert np.array_equal(s.solver.obstacles()[0], slab_obstacles(full, s.x0, s.nx)), rank
         finally:
             s.solver.close()
+    s = SlabSolver(cfg, 1, 2)  # columns 121..240: the face at x = 121 cuts the shell
+    try:
+        with pytest.raises(eup.EupError) as e:
+            s.build_obstacles(g)
+        assert e.value.code == 5
+    finally:
+        s.solver.close()
 
 
 def test_driver_creates_the_reference_column(eup, orc, require_gpu, tmp_path):
