@@ -603,24 +603,47 @@ __global__ void k_probes(Lat<S, R> L, Geo g, int npts, const int32_t* ijk, doubl
 }
 
 // ---- host layout <-> device layout ------------------------------------------------------
+// Host values (T = float or double) into the lattice and the halo shell.  16-bit storage
+// from double converts in double: f = w + D/scale is exact there, so a state downloaded as
+// double and uploaded again keeps every bit of D (through float, deviations below 2^-6
+// lose their low bits to the rounding of f).
 template <typename S, typename R, typename T>
 __global__ void k_scatter(Lat<S, R> L, Geo g, int q, const T* src, int64_t total) {
+    constexpr bool exact16 = DevStore<S>::value && sizeof(T) == 8;
     const int64_t L2 = g.l + 2, M2 = g.m + 2;
     for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(idx % L2), j = (int)((idx / L2) % M2), k = (int)(idx / (L2 * M2));
         const R v = (R)src[idx];
-        if (g.interior(i, j, k)) L.pop[q][g.lin(i, j, k)] = Store<S, R>::store(v, q, L.scale);
-        else L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)] = v;
+        if (g.interior(i, j, k)) {
+            if constexpr (exact16)
+                L.pop[q][g.lin(i, j, k)] =
+                    DevStore<S>::from_d(((double)src[idx] - (double)weight<float>(q)) * (double)L.scale);
+            else
+                L.pop[q][g.lin(i, j, k)] = Store<S, R>::store(v, q, L.scale);
+        } else {
+            L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)] = v;
+        }
     }
 }
 
+// The lattice and halo shell as host values; 16-bit storage to double in double (exact).
 template <typename S, typename R, typename T>
 __global__ void k_gather(Lat<S, R> L, Geo g, int q, T* dst, int64_t total) {
+    constexpr bool exact16 = DevStore<S>::value && sizeof(T) == 8;
     const int64_t L2 = g.l + 2, M2 = g.m + 2;
     for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x)
-        dst[idx] = (T)lat_load(L, g, q, (int)(idx % L2), (int)((idx / L2) % M2), (int)(idx / (L2 * M2)));
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % L2), j = (int)((idx / L2) % M2), k = (int)(idx / (L2 * M2));
+        if constexpr (exact16) {
+            if (g.interior(i, j, k)) {
+                dst[idx] = (double)weight<float>(q) +
+                           (double)DevStore<S>::to_f(L.pop[q][g.lin(i, j, k)]) * (double)L.inv_scale;
+                continue;
+            }
+        }
+        dst[idx] = (T)lat_load(L, g, q, i, j, k);
+    }
 }
 
 // x-face copy of the current lattice (after an upload): one thread per (j,k).

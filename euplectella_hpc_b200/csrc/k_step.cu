@@ -151,45 +151,45 @@ template <> struct Vec2<__nv_bfloat16> {
     static __device__ __forceinline__ __nv_bfloat16 hi(__nv_bfloat162 v) { return __high2bfloat16(v); }
 };
 
-template <typename S, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float> src, Lat<S, float> dst, Geo g,
-                                                                   Phys<float> ph) {
-    using K = KOps<S, float>;
-    using V2 = Vec2<S>;
-    using T2 = typename V2::T;
-    constexpr bool dev = DevStore<S>::value;
-    const int i = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x) + 1;  // first node; i + 1 <= l as l is even
-    const int j = blockIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    if (i > g.l) return;
-    const int l = g.l, lm = (int)g.lm;
-    const int rowlin = l * ((j - 1) + g.m * (k - 1));
-    const bool face_yz = (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-    if (face_yz) {  // warp-uniform: node by node through the halo shell
+// The two nodes of a y/z boundary row (warp-uniform), one by one through the halo shell.
+template <typename S>
+__device__ __forceinline__ void pair_through_shell(const Lat<S, float>& src, const Lat<S, float>& dst, const Geo& g,
+                                                   const Phys<float>& ph, int i, int j, int k, int rowlin) {
 #pragma unroll 1
-        for (int e = 0; e < 2; ++e) {
-            float x[19];
-            gather_node(src, g, i + e, j, k, rowlin, x);
-            K::collide_node(x, ph, src);
-            scatter_node(dst, g, i + e, j, k, rowlin, x);
-        }
-        return;
+    for (int e = 0; e < 2; ++e) {
+        float x[19];
+        gather_node(src, g, i + e, j, k, rowlin, x);
+        KOps<S, float>::collide_node(x, ph, src);
+        scatter_node(dst, g, i + e, j, k, rowlin, x);
     }
-    F2 x[19];
+}
+
+// 16-bit storage: the 19 pulls of the pair (i, i+1) of an interior row as raw words
+// (aligned in the shifted layout whatever cx is).
+template <typename S>
+__device__ __forceinline__ void load_pair_raw(const Lat<S, float>& src, const Geo& g, int i, int rowlin,
+                                              typename Vec2<S>::T (&r)[19]) {
+    using T2 = typename Vec2<S>::T;
+    const int l = g.l, lm = (int)g.lm;
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
         const int cx = (q == 18) ? 0 : cx_of(q), cy = (q == 18) ? 0 : cy_of(q), cz = (q == 18) ? 0 : cz_of(q);
         const S* rp = src.pop[q] + (rowlin - cy * l - cz * lm);
-        if (dev) {  // aligned in the shifted layout whatever cx is
-            x[q] = F2(V2::unpack(*reinterpret_cast<const T2*>(rp + (i - 1 - cx))));
-        } else if (cx == 0) {
-            const float2 v = V2::unpack(*reinterpret_cast<const T2*>(rp + (i - 1)));
-            x[q] = F2(K::val(v.x, q, src), K::val(v.y, q, src));
-        } else {
-            // both shifted loads are in bounds (interior rows; see gather_node)
-            x[q] = F2(K::val(rp[i - 1 - cx], q, src), K::val(rp[i - cx], q, src));
-        }
+        r[q] = *reinterpret_cast<const T2*>(rp + (i - 1 - cx));
     }
+}
+
+// Everything after the pulls of an interior pair: the x-halo values of the first and
+// last node of the row, the collision of both nodes as packed FP32, the x-face copy and
+// the stores.
+template <typename S>
+__device__ __forceinline__ void finish_pair(const Lat<S, float>& src, const Lat<S, float>& dst, const Geo& g,
+                                            const Phys<float>& ph, int i, int j, int k, int rowlin, F2 (&x)[19]) {
+    using K = KOps<S, float>;
+    using V2 = Vec2<S>;
+    using T2 = typename V2::T;
+    constexpr bool dev = DevStore<S>::value;
+    const int l = g.l;
     if (i == 1) {
 #pragma unroll
         for (int q = 0; q < 18; ++q)
@@ -224,6 +224,47 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float>
             op[1] = V2::hi(o);
         }
     }
+}
+
+template <typename S, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float> src, Lat<S, float> dst, Geo g,
+                                                                   Phys<float> ph) {
+    using K = KOps<S, float>;
+    using V2 = Vec2<S>;
+    using T2 = typename V2::T;
+    constexpr bool dev = DevStore<S>::value;
+    const int i = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x) + 1;  // first node; i + 1 <= l as l is even
+    const int j = blockIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > g.l) return;
+    const int l = g.l, lm = (int)g.lm;
+    const int rowlin = l * ((j - 1) + g.m * (k - 1));
+    const bool face_yz = (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
+    if (face_yz) {  // warp-uniform
+        pair_through_shell(src, dst, g, ph, i, j, k, rowlin);
+        return;
+    }
+    F2 x[19];
+    if constexpr (dev) {
+        T2 r[19];
+        load_pair_raw(src, g, i, rowlin, r);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) x[q] = F2(V2::unpack(r[q]));
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const int cx = (q == 18) ? 0 : cx_of(q), cy = (q == 18) ? 0 : cy_of(q), cz = (q == 18) ? 0 : cz_of(q);
+            const S* rp = src.pop[q] + (rowlin - cy * l - cz * lm);
+            if (cx == 0) {
+                const float2 v = V2::unpack(*reinterpret_cast<const T2*>(rp + (i - 1)));
+                x[q] = F2(K::val(v.x, q, src), K::val(v.y, q, src));
+            } else {
+                // both shifted loads are in bounds (interior rows; see gather_node)
+                x[q] = F2(K::val(rp[i - 1 - cx], q, src), K::val(rp[i - cx], q, src));
+            }
+        }
+    }
+    finish_pair(src, dst, g, ph, i, j, k, rowlin, x);
 }
 
 template <typename S, typename R>

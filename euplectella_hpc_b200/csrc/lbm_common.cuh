@@ -313,51 +313,71 @@ template <> struct DevStore<__half> {
     static constexpr bool value = true;
     static __device__ __forceinline__ float to_f(__half s) { return __half2float(s); }
     static __device__ __forceinline__ __half from_f(float d) { return __float2half_rn(d); }
+    static __device__ __forceinline__ __half from_d(double d) { return __double2half(d); }
 };
 template <> struct DevStore<__nv_bfloat16> {
     static constexpr bool value = true;
     static __device__ __forceinline__ float to_f(__nv_bfloat16 s) { return __bfloat162float(s); }
     static __device__ __forceinline__ __nv_bfloat16 from_f(float d) { return __float2bfloat16_rn(d); }
+    static __device__ __forceinline__ __nv_bfloat16 from_d(double d) { return __double2bfloat16(d); }
 };
 
-// One opposite pair (qp, qm) with c_qp . u = v, c_qm = -c_qp; fx = +-1/0 the
-// x component of c_qp (body force along x).  V = float, or F2 for two nodes.
-template <typename V>
-__device__ __forceinline__ void dev_pair(V* D, int qp, int qm, V v, float w, V rm1, V rho, V t, V oS, float omega1,
-                                         V fS, float fx) {
-    const V a = fma_rn(rho, fma_rn(V(4.5f) * v, v, -t), rm1);   // (rho-1) + rho (4.5 v^2 - 1.5 u^2)
-    const V b = V(3.0f) * rho * v;
-    const V ow = oS * V(w);
-    D[qp] = fma_rn(V(omega1), D[qp], fma_rn(ow, a + b, V(fx) * fS));
-    D[qm] = fma_rn(V(omega1), D[qm], fma_rn(ow, a - b, V(-fx) * fS));
+// Reciprocal for the 16-bit path: the hardware approximation (rcp.approx, relative
+// error below 2^-22), per lane, so the one-node and two-node kernels agree bit for bit.
+__device__ __forceinline__ float rcp_dev(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ F2 rcp_dev(F2 x) { return F2(rcp_dev(x.v.x), rcp_dev(x.v.y)); }
+
+// One opposite pair (qp, qm) with c_qp . u = v, c_qm = -c_qp; FX = +-1/0 the x
+// component of c_qp (the body force acts along x).  With c0 = (rho-1) - 1.5 rho u^2,
+//   D'_qp = (1-omega) D_qp + S omega w [c0 + 4.5 rho v^2 + 3 rho v] + S F_qp
+// and D'_qm the same with -v.  V = float, or F2 for two nodes.
+template <int FX, typename V>
+__device__ __forceinline__ void dev_pair(V* D, int qp, int qm, V v, V ow, V c0, V r45, V r3, float omega1, V fS) {
+    const V a = fma_rn(r45 * v, v, c0);
+    const V b = r3 * v;
+    const V dp = FX != 0 ? fma_rn(V(omega1), D[qp], fS) : V(omega1) * D[qp];
+    const V dm = FX != 0 ? fma_rn(V(omega1), D[qm], -fS) : V(omega1) * D[qm];
+    D[qp] = fma_rn(ow, a + b, dp);
+    D[qm] = fma_rn(ow, a - b, dm);
 }
 
 template <typename V>
 __device__ __forceinline__ void collide_dev(V* D, float omega, float omega1, float fgrad, float S, float invS) {
-    V s = D[0];
-#pragma unroll
-    for (int q = 1; q < 19; ++q) s = s + D[q];
+    // rho - 1 and j from partial sums shared between the moments: the +x and -x groups,
+    // the y+ and y- populations without an x component, and the rest
+    const V xp = ((D[0] + D[1]) + (D[2] + D[3])) + D[4];
+    const V xm = ((D[9] + D[10]) + (D[11] + D[12])) + D[13];
+    const V yp = (D[6] + D[7]) + D[8];
+    const V ym = (D[15] + D[16]) + D[17];
+    const V z0 = (D[5] + D[14]) + D[18];
+    const V s = ((xp + xm) + (yp + ym)) + z0;
+    const V jx = xp - xm;
+    const V jy = ((D[2] + D[11]) + yp) - ((D[0] + D[9]) + ym);
+    const V jz = ((D[3] + D[5]) + (D[6] + D[12]) + D[17]) - ((D[1] + D[8]) + (D[10] + D[14]) + D[15]);
     const V rm1 = s * V(invS);
     const V rho = V(1.0f) + rm1;
-    const V jx = (D[0] + D[1] + D[2] + D[3] + D[4]) - (D[9] + D[10] + D[11] + D[12] + D[13]);
-    const V jy = (D[2] + D[6] + D[7] + D[8] + D[11]) - (D[0] + D[9] + D[15] + D[16] + D[17]);
-    const V jz = (D[3] + D[5] + D[6] + D[12] + D[17]) - (D[1] + D[8] + D[10] + D[14] + D[15]);
-    const V ri = V(invS) / rho;
+    const V ri = V(invS) * rcp_dev(rho);
     const V ux = jx * ri, uy = jy * ri, uz = jz * ri;
-    const V t = V(1.5f) * fma_rn(ux, ux, fma_rn(uy, uy, uz * uz));
-    const V oS = V(omega * S);
+    const V r15 = V(1.5f) * rho;
+    const V c0 = fma_rn(-r15, fma_rn(ux, ux, fma_rn(uy, uy, uz * uz)), rm1);  // (rho-1) - 1.5 rho u^2
+    const V r45 = V(4.5f) * rho, r3 = V(3.0f) * rho;
     const V fS = V(S * fgrad) * rho;
-    const float w0 = 1.0f / 3.0f, w1 = 1.0f / 18.0f, w2 = 1.0f / 36.0f;
-    dev_pair<V>(D, 4, 13, ux, w1, rm1, rho, t, oS, omega1, fS, 1.f);        // a05 / a14
-    dev_pair<V>(D, 5, 14, uz, w1, rm1, rho, t, oS, omega1, fS, 0.f);        // a06 / a15
-    dev_pair<V>(D, 7, 16, uy, w1, rm1, rho, t, oS, omega1, fS, 0.f);        // a08 / a17
-    dev_pair<V>(D, 0, 11, ux - uy, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a01 / a12
-    dev_pair<V>(D, 1, 12, ux - uz, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a02 / a13
-    dev_pair<V>(D, 2, 9, ux + uy, w2, rm1, rho, t, oS, omega1, fS, 1.f);    // a03 / a10
-    dev_pair<V>(D, 3, 10, ux + uz, w2, rm1, rho, t, oS, omega1, fS, 1.f);   // a04 / a11
-    dev_pair<V>(D, 6, 15, uy + uz, w2, rm1, rho, t, oS, omega1, fS, 0.f);   // a07 / a16
-    dev_pair<V>(D, 8, 17, uy - uz, w2, rm1, rho, t, oS, omega1, fS, 0.f);   // a09 / a18
-    D[18] = fma_rn(V(omega1), D[18], oS * V(w0) * fma_rn(-rho, t, rm1));   // a19
+    const float oS = omega * S;
+    const V ow1 = V(oS * (1.0f / 18.0f)), ow2 = V(oS * (1.0f / 36.0f)), ow0 = V(oS * (1.0f / 3.0f));
+    dev_pair<1>(D, 4, 13, ux, ow1, c0, r45, r3, omega1, fS);        // a05 / a14
+    dev_pair<0>(D, 5, 14, uz, ow1, c0, r45, r3, omega1, fS);        // a06 / a15
+    dev_pair<0>(D, 7, 16, uy, ow1, c0, r45, r3, omega1, fS);        // a08 / a17
+    dev_pair<1>(D, 0, 11, ux - uy, ow2, c0, r45, r3, omega1, fS);   // a01 / a12
+    dev_pair<1>(D, 1, 12, ux - uz, ow2, c0, r45, r3, omega1, fS);   // a02 / a13
+    dev_pair<1>(D, 2, 9, ux + uy, ow2, c0, r45, r3, omega1, fS);    // a03 / a10
+    dev_pair<1>(D, 3, 10, ux + uz, ow2, c0, r45, r3, omega1, fS);   // a04 / a11
+    dev_pair<0>(D, 6, 15, uy + uz, ow2, c0, r45, r3, omega1, fS);   // a07 / a16
+    dev_pair<0>(D, 8, 17, uy - uz, ow2, c0, r45, r3, omega1, fS);   // a09 / a18
+    D[18] = fma_rn(ow0, c0, V(omega1) * D[18]);                      // a19
 }
 
 // Physical constants of one run, rounded to the arithmetic type the way

@@ -195,7 +195,10 @@ int eup_init_state(eup_handle* h, double u_in, double amp, uint64_t seed, int64_
  * the haloed arrays, elem_bytes 4 or 8, gfortran 4-byte record markers)
  * written from and read into the device state directly, one population at a
  * time through a pinned buffer, with no 19-array host copy: 16-bit storage is
- * expanded to float/double on the way out.  Records over 2 GiB (a population
+ * expanded to float/double on the way out.  A 16-bit state crosses a double file
+ * (elem_bytes 8) bit for bit; in a float file f = w + D/scale is rounded to float,
+ * which drops low bits of deviations below 2^-6 (the same holds for eup_download and
+ * eup_upload with elem_bytes 4 and 8).  Records over 2 GiB (a population
  * beyond 2^29 FP32 nodes) are rejected.  eup_restore_state sets the step
  * counter from the file. */
 int eup_save_state(eup_handle* h, const char* path, int32_t elem_bytes);

@@ -203,30 +203,35 @@ def test_reference_diagnostics_match_oracle(eup, orc, require_gpu, prec):
         np.testing.assert_allclose(g, orc.cv_drag(p, a, b), rtol=1e-12, atol=1e-13)
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp16"])
-def test_device_checkpoint_round_trip(eup, require_gpu, tmp_path, prec):
+@pytest.mark.parametrize("prec,eb", [("fp32", 4), ("fp16", 8), ("fp16", 4)])
+def test_device_checkpoint_round_trip(eup, require_gpu, tmp_path, prec, eb):
     """eup_save_state writes what download + write_raw_state would; eup_restore_state
-    continues the run exactly."""
+    continues the run exactly.  A 16-bit state crosses a double checkpoint bit for bit; a
+    float checkpoint holds f rounded to float (deviations below 2^-6 lose low bits), so the
+    restored run continues from that state, as an upload of the float arrays would."""
     l, m, n = 36, 16, 10
     code = eup.FP32 if prec == "fp32" else eup.FP16_DEV
+    dt = np.float32 if eb == 4 else np.float64
     obs = _cyl(l, m, n)
     cfg = eup.Config(l, m, n, bc=(5, 4, 3, 3, 0, 0), svisc=0.01, u_inflow=0.05, precision=code)
     with eup.Solver(cfg) as s:
         s.set_obstacles(obs)
         s.init_state(0.05, 1e-3, 31, itime=40)
         s.step(6)
-        s.save_state(tmp_path / "save.bin")
-        ref = s.download(np.float32)
+        s.save_state(tmp_path / "save.bin", eb)
+        ref = s.download(dt)
+        if prec == "fp16" and eb == 4:
+            s.upload(ref, itime=46)
         s.step(5)
-        ref_next = s.download(np.float32)
-    got, it = eup.read_raw_state(tmp_path / "save.bin", l, m, n)
+        ref_next = s.download(dt)
+    got, it = eup.read_raw_state(tmp_path / "save.bin", l, m, n, dt)
     assert it == 46 and np.array_equal(got, ref)
     with eup.Solver(cfg) as s:
         s.set_obstacles(obs)
-        s.restore_state(tmp_path / "save.bin")
+        s.restore_state(tmp_path / "save.bin", eb)
         assert s.itime == 46
         s.step(5)
-        assert np.array_equal(s.download(np.float32), ref_next)
+        assert np.array_equal(s.download(dt), ref_next)
 
 
 def test_region_sums_match_oracle(eup, orc, require_gpu):
@@ -304,10 +309,10 @@ def test_deviation_storage_against_fp64(eup, require_gpu, prec):
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16", "bf16"])
 def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
-    """Pipelined (default for 16/32-bit storage) vs one-node-per-thread vs 16-byte and
-    8-byte vectorised stream-collide, CUDA graphs vs plain launches: all paths give
-    the same bits in every storage format."""
-    l, m, n = 256, 20, 12
+    """Two nodes per thread (default for 16/32-bit storage, at several occupancies) vs one
+    node per thread vs 16-byte and 8-byte vectorised stream-collide, CUDA graphs vs plain
+    launches: all paths give the same bits in every storage format."""
+    l, m, n = 256, 20, 13
     code = {"fp32": eup.FP32, "fp64": eup.FP64, "fp16": eup.FP16_DEV, "bf16": eup.BF16_DEV}[prec]
     dt = np.float64 if prec == "fp64" else np.float32
     obs = _cyl(l, m, n)
