@@ -505,29 +505,43 @@ int check_obstacles(eup_handle* h, const char* who, int64_t nsolid, int64_t on_f
 
 // Installs `bits` (m*n*wpr words, owned by the handle from here on; null or
 // nsolid == 0: no solids) in place of the current mask: the list of boundary
-// solids, their link words, and the drag of the current state.
+// solids, their link words, and the drag of the current state.  Every buffer is
+// allocated before the current mask is released, so a failed allocation leaves
+// the handle as it was.
 int install_mask(eup_handle* h, uint32_t* bits, int64_t nsolid) {
     const Geo& g = h->g;
+    if (nsolid <= 0 && bits) { cudaFree(bits); bits = nullptr; }
+    uint8_t* d_flags = nullptr;
+    int32_t* blist = nullptr;
+    uint64_t* blinks = nullptr;
+    if (nsolid > 0) {
+        cudaError_t e = cudaMalloc(&d_flags, g.N);
+        if (e == cudaSuccess) e = cudaMalloc(&blist, sizeof(int32_t) * (size_t)nsolid);
+        if (e == cudaSuccess) e = cudaMalloc(&blinks, sizeof(uint64_t) * (size_t)nsolid);
+        if (e != cudaSuccess) {
+            cudaFree(d_flags);
+            cudaFree(blist);
+            cudaFree(blinks);
+            cudaFree(bits);
+            return cuda_fail(h, e, "install obstacles");
+        }
+    }
     drop_graphs(h);  // the captured steps hold the old mask and list pointers
     if (h->bits) cudaFree(h->bits);
-    if (h->blist) { cudaFree(h->blist); h->blist = nullptr; }
-    if (h->blinks) { cudaFree(h->blinks); h->blinks = nullptr; }
-    h->nblist = 0;
-    h->nsolid = 0;
-    if (nsolid <= 0 && bits) { cudaFree(bits); bits = nullptr; }
+    if (h->blist) cudaFree(h->blist);
+    if (h->blinks) cudaFree(h->blinks);
     h->bits = bits;
+    h->blist = blist;
+    h->blinks = blinks;
+    h->nblist = 0;
+    h->nsolid = nsolid > 0 ? nsolid : 0;
     if (nsolid > 0) {
-        h->nsolid = nsolid;
-        uint8_t* d_flags = nullptr;
-        CK(h, cudaMalloc(&d_flags, g.N));
         launch_flag_boundary_solid(g, make_mask(h), d_flags, h->stream);
-        CK(h, cudaMalloc(&h->blist, sizeof(int32_t) * (size_t)nsolid));
         cudaError_t e;
         const int64_t cnt = compact_flags(d_flags, g.N, h->blist, h->stream, &e);
         cudaFree(d_flags);
         if (e != cudaSuccess) return cuda_fail(h, e, "compact boundary solid list");
-        h->nblist = cnt;
-        CK(h, cudaMalloc(&h->blinks, sizeof(uint64_t) * (size_t)(cnt > 0 ? cnt : 1)));
+        h->nblist = cnt;  // cnt <= nsolid: the boundary solids are solids
         const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
         launch_bsolid_links(g, make_mask(h), bc, h->blist, cnt, h->blinks, h->stream);
     }
