@@ -41,7 +41,7 @@ EXPORTED = [
     "eup_geometry_ridged_shell", "eup_get_region_sums", "eup_init_state", "eup_get_line", "eup_get_plane_means",
     "eup_get_cv_drag", "eup_save_state", "eup_restore_state", "eup_step_boundaries", "eup_step_stream",
     "eup_get_x_planes", "eup_set_x_planes", "eup_geometry_reference", "eup_voxelise", "eup_build_obstacles",
-    "eup_get_obstacles", "eup_write_obstacles",
+    "eup_get_obstacles", "eup_write_obstacles", "eup_step_stream_interior", "eup_step_stream_faces",
 ]
 
 
@@ -163,6 +163,7 @@ def _load():
         "eup_build_obstacles": ([vp, ctypes.POINTER(Geometry)], ctypes.c_int),
         "eup_get_obstacles": ([vp, vp, ctypes.POINTER(i64)], ctypes.c_int),
         "eup_write_obstacles": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "eup_step_stream_interior": ([vp], ctypes.c_int), "eup_step_stream_faces": ([vp], ctypes.c_int),
     }
     # every entry point gets a prototype: an unprototyped call would pass pointers as C ints
     missing = [name for name in EXPORTED if name not in sig]
@@ -377,6 +378,14 @@ class Solver:
     def step_stream(self):
         """Second half of an x-slab step: stream-collide, step counter (asynchronous)."""
         self._ck(lib.eup_step_stream(self._h))
+
+    def step_stream_interior(self):
+        """step_stream's columns 2..l-1, which need no received planes (asynchronous)."""
+        self._ck(lib.eup_step_stream_interior(self._h))
+
+    def step_stream_faces(self):
+        """step_stream's columns 1 and l, after the planes are in, and the step counter."""
+        self._ck(lib.eup_step_stream_faces(self._h))
 
     def get_x_planes(self, side, dev_ptr):
         """Pack the 5 populations leaving through x = 1 (side 0) or x = l (side 1) into device memory."""

@@ -49,6 +49,7 @@ struct eup_handle {
     void* ns = nullptr;           // solid fraction n_s per interior node, arithmetic type
     int64_t launches = 0;  // kernels launched by eup_step / eup_step_profiled
     bool mid_step = false;  // eup_step_boundaries done, eup_step_stream pending
+    bool interior_done = false;  // eup_step_stream_interior done, eup_step_stream_faces pending
     int launches_per_step = 0;
     std::string err;
 };
@@ -189,14 +190,16 @@ void enqueue_boundaries(eup_handle* h) {
 }
 
 template <typename S, typename R>
-void enqueue_stream(eup_handle* h) {
+void enqueue_stream(eup_handle* h, int part) {
     const Phys<R> ph = make_phys<R>(h);
     launch_stream_collide<S, R>(make_lat<S, R>(h, h->cur), make_lat<S, R>(h, h->cur ^ 1), h->g, ph, h->variant,
-                                h->stream);
+                                h->stream, part);
+    h->launches += 1;
+    if (part == kStreamInterior) return;
     h->cur ^= 1;
     h->itime += 1;
     enqueue_drag_only<S, R>(h);  // the force of the state reached, as eup_step leaves it
-    h->launches += 2;
+    h->launches += 1;
 }
 
 template <typename S, typename R>
@@ -343,6 +346,7 @@ int finish_state(eup_handle* h, int64_t itime) {
     h->series_first = itime;
     h->has_state = true;
     h->mid_step = false;
+    h->interior_done = false;
     if (h->pbb) CK(h, cudaMemsetAsync(h->series + 3 * (itime % h->cap), 0, 3 * sizeof(double), h->stream));
     else DISPATCH(h, enqueue_drag_only, h);
     CK(h, cudaGetLastError());
@@ -838,9 +842,33 @@ int eup_step_boundaries(eup_handle* h) {
 int eup_step_stream(eup_handle* h) {
     int rc = check_handle(h);
     if (rc) return rc;
-    if (!h->mid_step) return fail(h, EUP_ERR_INVALID_ARG, "eup_step_stream: eup_step_boundaries is due first");
-    DISPATCH(h, enqueue_stream, h);
+    if (!h->mid_step || h->interior_done)
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_step_stream: eup_step_boundaries (alone) is due first");
+    DISPATCH(h, enqueue_stream, h, (int)kStreamAll);
     CK(h, cudaGetLastError());
+    h->mid_step = false;
+    return EUP_OK;
+}
+
+int eup_step_stream_interior(eup_handle* h) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!h->mid_step || h->interior_done)
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_step_stream_interior: eup_step_boundaries (alone) is due first");
+    DISPATCH(h, enqueue_stream, h, (int)kStreamInterior);
+    CK(h, cudaGetLastError());
+    h->interior_done = true;
+    return EUP_OK;
+}
+
+int eup_step_stream_faces(eup_handle* h) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!h->mid_step || !h->interior_done)
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_step_stream_faces: eup_step_stream_interior is due first");
+    DISPATCH(h, enqueue_stream, h, (int)kStreamFaces);
+    CK(h, cudaGetLastError());
+    h->interior_done = false;
     h->mid_step = false;
     return EUP_OK;
 }

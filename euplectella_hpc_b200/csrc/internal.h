@@ -120,10 +120,14 @@ void launch_unpack_x(const Lat<S, R>& L, const Geo& g, int side, const R* in, cu
 template <typename S, typename R>
 void launch_fill_xface(const Lat<S, R>& L, const Geo& g, cudaStream_t st);
 
-// Fused pull stream + collide (CODE/SRC/movef.F90 + CODE/SRC/col.F90): src -> dst.
+// Fused pull stream + collide (CODE/SRC/movef.F90 + CODE/SRC/col.F90): src -> dst, over
+// every node (kStreamAll), or split into the columns that do not pull from the x halo
+// planes (kStreamInterior) and the two that do (kStreamFaces), so that an x-slab can
+// receive its halo planes while the interior streams.
+enum { kStreamAll = 0, kStreamInterior = 1, kStreamFaces = 2 };
 template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g,
-                           const Phys<R>& ph, int variant, cudaStream_t st);
+                           const Phys<R>& ph, int variant, cudaStream_t st, int part = kStreamAll);
 
 // Reference-form diagnostics (CODE/SRC/prof_*.F90, varm.F90, flux_X/flux_Y.F90):
 // a line of per-node u, w, v, den in R; per-plane means; the FP64 face sums of

@@ -101,18 +101,35 @@ __device__ __forceinline__ void scatter_node(const Lat<S, R>& dst, const Geo& g,
     }
 }
 
-// One thread per node; grid (ceil(l/bx), m, n).
 template <typename S, typename R>
-__global__ void __launch_bounds__(128) k_stream_collide_scalar(Lat<S, R> src, Lat<S, R> dst, Geo g, Phys<R> ph) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    if (i > g.l) return;
+__device__ __forceinline__ void node_step(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g,
+                                          const Phys<R>& ph, int i, int j, int k) {
     const int rowlin = g.l * ((j - 1) + g.m * (k - 1));
     R x[19];
     gather_node(src, g, i, j, k, rowlin, x);
     KOps<S, R>::collide_node(x, ph, src);
     scatter_node(dst, g, i, j, k, rowlin, x);
+}
+
+// One thread per node of the columns i0 .. i0+ni-1; grid (ceil(ni/bx), m, n).
+template <typename S, typename R>
+__global__ void __launch_bounds__(128) k_stream_collide_scalar(Lat<S, R> src, Lat<S, R> dst, Geo g, Phys<R> ph,
+                                                               int i0, int ni) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ni) return;
+    node_step(src, dst, g, ph, i0 + t, (int)blockIdx.y + 1, (int)blockIdx.z + 1);
+}
+
+// The columns i = 1 and i = l (the only ones that pull from the x halo planes): one thread
+// per (side, j, k); sides = 1 when l == 1.
+template <typename S, typename R>
+__global__ void __launch_bounds__(128) k_stream_collide_scalar_faces(Lat<S, R> src, Lat<S, R> dst, Geo g,
+                                                                     Phys<R> ph, int sides) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)sides * g.m * g.n) return;
+    const int side = (int)(t % sides);
+    const int64_t row = t / sides;
+    node_step(src, dst, g, ph, side ? g.l : 1, (int)(row % g.m) + 1, (int)(row / g.m) + 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -226,21 +243,19 @@ __device__ __forceinline__ void finish_pair(const Lat<S, float>& src, const Lat<
     }
 }
 
-template <typename S, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float> src, Lat<S, float> dst, Geo g,
-                                                                   Phys<float> ph) {
+// The pair (i, i+1) of row (j, k).  Rows on the y/z boundary planes go node by node
+// through the halo shell (warp-uniform in the row kernel, where a block is one row).
+template <typename S>
+__device__ __forceinline__ void pair_step(const Lat<S, float>& src, const Lat<S, float>& dst, const Geo& g,
+                                          const Phys<float>& ph, int i, int j, int k) {
     using K = KOps<S, float>;
     using V2 = Vec2<S>;
     using T2 = typename V2::T;
     constexpr bool dev = DevStore<S>::value;
-    const int i = 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x) + 1;  // first node; i + 1 <= l as l is even
-    const int j = blockIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    if (i > g.l) return;
     const int l = g.l, lm = (int)g.lm;
     const int rowlin = l * ((j - 1) + g.m * (k - 1));
     const bool face_yz = (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-    if (face_yz) {  // warp-uniform
+    if (face_yz) {
         pair_through_shell(src, dst, g, ph, i, j, k, rowlin);
         return;
     }
@@ -267,8 +282,29 @@ __global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float>
     finish_pair(src, dst, g, ph, i, j, k, rowlin, x);
 }
 
+// Pairs p0 .. p0+np-1 of every row (pair p: nodes 2p+1, 2p+2); grid (ceil(np/128), m, n).
+template <typename S, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float> src, Lat<S, float> dst, Geo g,
+                                                                   Phys<float> ph, int p0, int np) {
+    const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (t >= np) return;
+    pair_step(src, dst, g, ph, 2 * (p0 + t) + 1, (int)blockIdx.y + 1, (int)blockIdx.z + 1);
+}
+
+// The first and last pair of every row (the only ones that pull from the x halo planes):
+// one thread per (side, j, k); sides = 1 when l == 2.
+template <typename S>
+__global__ void __launch_bounds__(128, 6) k_stream_collide_pair_faces(Lat<S, float> src, Lat<S, float> dst, Geo g,
+                                                                      Phys<float> ph, int sides) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)sides * g.m * g.n) return;
+    const int side = (int)(t % sides);
+    const int64_t row = t / sides;
+    pair_step(src, dst, g, ph, side ? g.l - 1 : 1, (int)(row % g.m) + 1, (int)(row / g.m) + 1);
+}
+
 template <typename S, typename R>
-bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph, int occ,
+bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph, int occ, int part,
                  cudaStream_t st) {
     if constexpr (sizeof(R) != 4) {
         return false;
@@ -284,16 +320,26 @@ bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const
             if ((!dev || cx == 0) && reinterpret_cast<uintptr_t>(dst.pop[q]) % (2 * sizeof(S)) != 0) return false;
         }
         const int bx = 128;
-        dim3 grid((g.l / 2 + bx - 1) / bx, g.m, g.n);
+        if (part == kStreamFaces) {
+            const int sides = g.l == 2 ? 1 : 2;
+            const int64_t threads = (int64_t)sides * g.m * g.n;
+            k_stream_collide_pair_faces<S><<<(unsigned)((threads + bx - 1) / bx), bx, 0, st>>>(src, dst, g, ph, sides);
+            return true;
+        }
+        // all pairs, or all but the first and last of each row
+        const int p0 = part == kStreamInterior ? 1 : 0;
+        const int np = part == kStreamInterior ? g.l / 2 - 2 : g.l / 2;
+        if (np <= 0) return true;
+        dim3 grid((np + bx - 1) / bx, g.m, g.n);
         // resident blocks of 128 threads per SM the register budget is sized for: by default
         // 6 (80 registers) for FP32 storage, 8 (64) for 16-bit storage, whose loads need fewer
         const int minb = occ > 0 ? occ + 3 : (sizeof(S) == 4 ? 6 : 8);
         switch (minb) {
-            case 4: k_stream_collide_pair<S, 4><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
-            case 5: k_stream_collide_pair<S, 5><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
-            case 6: k_stream_collide_pair<S, 6><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
-            case 7: k_stream_collide_pair<S, 7><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
-            default: k_stream_collide_pair<S, 8><<<grid, bx, 0, st>>>(src, dst, g, ph); break;
+            case 4: k_stream_collide_pair<S, 4><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
+            case 5: k_stream_collide_pair<S, 5><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
+            case 6: k_stream_collide_pair<S, 6><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
+            case 7: k_stream_collide_pair<S, 7><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
+            default: k_stream_collide_pair<S, 8><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
         }
         return true;
     }
@@ -444,28 +490,40 @@ bool launch_vec(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const 
 
 template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph,
-                           int variant, cudaStream_t st) {
+                           int variant, cudaStream_t st, int part) {
     // EUP_STEP_VARIANT bit 0: 16-byte vectors, bit 2: 8-byte vectors (when l allows), bit 3: one
     // node per thread, bits 4-6: occupancy target of the two-node kernel (n + 3 blocks per SM);
-    // default: two nodes per thread (FP32 arithmetic, l even).
+    // default: two nodes per thread (FP32 arithmetic, l even).  A split step (interior columns,
+    // then the two x-face columns) uses the two-node or the one-node kernel.
     constexpr int VW = VecWidth<S>::value;
-    if ((variant & 1) && launch_vec<S, R, VW>(src, dst, g, ph, st)) return;
-    if ((variant & 4) && launch_vec<S, R, (VW / 2 > 0 ? VW / 2 : 1)>(src, dst, g, ph, st)) return;
-    if (!(variant & 8) && launch_pair<S, R>(src, dst, g, ph, (variant >> 4) & 7, st)) return;
+    if (part == kStreamAll) {
+        if ((variant & 1) && launch_vec<S, R, VW>(src, dst, g, ph, st)) return;
+        if ((variant & 4) && launch_vec<S, R, (VW / 2 > 0 ? VW / 2 : 1)>(src, dst, g, ph, st)) return;
+    }
+    if (!(variant & 8) && launch_pair<S, R>(src, dst, g, ph, (variant >> 4) & 7, part, st)) return;
     const int bx = 128;
-    dim3 grid((g.l + bx - 1) / bx, g.m, g.n);
-    k_stream_collide_scalar<S, R><<<grid, bx, 0, st>>>(src, dst, g, ph);
+    if (part == kStreamFaces) {
+        const int sides = g.l == 1 ? 1 : 2;
+        const int64_t threads = (int64_t)sides * g.m * g.n;
+        k_stream_collide_scalar_faces<S, R><<<(unsigned)((threads + bx - 1) / bx), bx, 0, st>>>(src, dst, g, ph, sides);
+        return;
+    }
+    const int i0 = part == kStreamInterior ? 2 : 1;
+    const int ni = part == kStreamInterior ? g.l - 2 : g.l;
+    if (ni <= 0) return;
+    dim3 grid((ni + bx - 1) / bx, g.m, g.n);
+    k_stream_collide_scalar<S, R><<<grid, bx, 0, st>>>(src, dst, g, ph, i0, ni);
 }
 
 template void launch_stream_collide<float, float>(const Lat<float, float>&, const Lat<float, float>&,
-                                                  const Geo&, const Phys<float>&, int, cudaStream_t);
+                                                  const Geo&, const Phys<float>&, int, cudaStream_t, int);
 template void launch_stream_collide<double, double>(const Lat<double, double>&, const Lat<double, double>&,
-                                                    const Geo&, const Phys<double>&, int, cudaStream_t);
+                                                    const Geo&, const Phys<double>&, int, cudaStream_t, int);
 template void launch_stream_collide<__half, float>(const Lat<__half, float>&, const Lat<__half, float>&,
-                                                   const Geo&, const Phys<float>&, int, cudaStream_t);
+                                                   const Geo&, const Phys<float>&, int, cudaStream_t, int);
 template void launch_stream_collide<__nv_bfloat16, float>(const Lat<__nv_bfloat16, float>&,
                                                           const Lat<__nv_bfloat16, float>&, const Geo&,
-                                                          const Phys<float>&, int, cudaStream_t);
+                                                          const Phys<float>&, int, cudaStream_t, int);
 
 }  // namespace eup
 

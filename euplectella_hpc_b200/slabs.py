@@ -6,11 +6,12 @@ faces between slabs are flagged EXCHANGE: each step runs
 
     bounce-back + halo planes          eup_step_boundaries   (every slab)
     pack the 5 populations leaving     eup_get_x_planes      (both x faces)
-    send/recv to the neighbours        torch.distributed (NCCL: device buffers
-                                       on the solver's stream; gloo: staged
-                                       through host memory)
+    stream-collide of x = 2..l-1       eup_step_stream_interior
+      meanwhile send/recv to the       torch.distributed (NCCL: device buffers
+      neighbours                       on a high-priority stream, ordered by
+                                       events; gloo: staged through host memory)
     unpack into the x halo             eup_set_x_planes
-    stream-collide                     eup_step_stream
+    stream-collide of x = 1 and l      eup_step_stream_faces
 
 Only 5 of the 19 populations cross a face ((ly+2)(lz+2) values each, the y/z
 halo rows included, so corner pulls see this step's y/z boundary values): the
@@ -124,6 +125,9 @@ class SlabSolver:
         staged = transport is not None and not getattr(transport, "nccl", True)
         self.host = {k: torch.zeros(n, dtype=dt, pin_memory=True) for k in self.buf} if staged else None
         self.stream = torch.cuda.ExternalStream(self.solver.stream())
+        # the exchange runs beside the interior stream-collide; at high priority its kernels
+        # take SMs as the interior blocks retire instead of queueing behind all of them
+        self.xstream = torch.cuda.Stream(device=dev, priority=-1)
 
     # ---- set-up (from the global arrays) ----
     def set_obstacles(self, obs_global: np.ndarray):
@@ -154,12 +158,20 @@ class SlabSolver:
         if self.has_right:
             self.solver.get_x_planes(1, self.buf["send_r"].data_ptr())
 
-    def end(self):
+    def _unpack(self):
         if self.has_left:
             self.solver.set_x_planes(0, self.buf["recv_l"].data_ptr())
         if self.has_right:
             self.solver.set_x_planes(1, self.buf["recv_r"].data_ptr())
+
+    def end(self):
+        self._unpack()
         self.solver.step_stream()
+
+    def end_faces(self):
+        """After step_stream_interior and the exchange: unpack, then the x = 1 and x = l columns."""
+        self._unpack()
+        self.solver.step_stream_faces()
 
     def exchange(self):
         """Move this step's planes to and from the neighbour ranks."""
@@ -179,14 +191,35 @@ class SlabSolver:
                 b[k].copy_(h[k])
             self.torch.cuda.synchronize()
 
-    def step(self, nsteps: int = 1):
-        """nsteps time steps of this slab, exchanging with the neighbour ranks every step."""
+    def exchange_overlapped(self):
+        """NCCL exchange on the high-priority stream while the solver's stream runs the interior
+        stream-collide: the exchange waits for the packed planes, the face columns for the
+        received ones."""
+        torch, b = self.torch, self.buf
+        packed = torch.cuda.Event()
+        packed.record(self.stream)
+        self.solver.step_stream_interior()
+        with torch.cuda.stream(self.xstream):
+            self.xstream.wait_event(packed)
+            self.transport.exchange(b["send_l"], b["send_r"], b["recv_l"], b["recv_r"])
+            arrived = torch.cuda.Event()
+            arrived.record(self.xstream)
+        self.stream.wait_event(arrived)
+
+    def step(self, nsteps: int = 1, overlap: bool = True):
+        """nsteps time steps of this slab, exchanging with the neighbour ranks every step; with
+        NCCL the exchange overlaps the interior stream-collide (overlap=False: in sequence)."""
         if self.world > 1 and self.transport is None:
             raise ValueError("a slab with neighbours needs a transport (or step_in_process)")
+        split = overlap and self.world > 1 and self.host is None
         for _ in range(nsteps):
             self.begin()
-            self.exchange()
-            self.end()
+            if split:
+                self.exchange_overlapped()
+                self.end_faces()
+            else:
+                self.exchange()
+                self.end()
 
     def forces(self) -> np.ndarray:
         """The lattice's momentum-exchange force: the sum over the slabs."""
@@ -198,12 +231,16 @@ class SlabSolver:
         return f.cpu().numpy()
 
 
-def step_in_process(slabs: list[SlabSolver], nsteps: int = 1):
+def step_in_process(slabs: list[SlabSolver], nsteps: int = 1, split: bool = False):
     """Steps slabs that share one process (and possibly one GPU): the plane exchange is a
-    device copy between the slabs' buffers, between the two halves of every slab's step."""
+    device copy between the slabs' buffers, between the two halves of every slab's step
+    (split=True: the interior stream-collide is enqueued before the copy, the face columns
+    after it, as the overlapped NCCL step does)."""
     for _ in range(nsteps):
         for s in slabs:
             s.begin()
+            if split:
+                s.solver.step_stream_interior()
         for s in slabs:
             s.solver.synchronize()
         for r, s in enumerate(slabs):
@@ -213,7 +250,10 @@ def step_in_process(slabs: list[SlabSolver], nsteps: int = 1):
                 s.buf["recv_r"].copy_(slabs[r + 1].buf["send_l"])
         slabs[0].torch.cuda.synchronize()
         for s in slabs:
-            s.end()
+            if split:
+                s.end_faces()
+            else:
+                s.end()
 
 
 def gather_state(slabs: list[SlabSolver], dtype=np.float32) -> np.ndarray:

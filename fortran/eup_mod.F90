@@ -155,6 +155,41 @@
             real(c_double)                :: stats(8)
          end function
 
+         ! x-slab step (one GPU per slab): boundaries, planes out, interior | exchange, planes in, faces
+         integer(c_int) function eup_step_boundaries(h) bind(c, name="eup_step_boundaries")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+         end function
+
+         integer(c_int) function eup_step_stream(h) bind(c, name="eup_step_stream")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+         end function
+
+         integer(c_int) function eup_step_stream_interior(h) bind(c, name="eup_step_stream_interior")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+         end function
+
+         integer(c_int) function eup_step_stream_faces(h) bind(c, name="eup_step_stream_faces")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+         end function
+
+         integer(c_int) function eup_get_x_planes(h, side, dst) bind(c, name="eup_get_x_planes")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: side          ! 0: x = 1 (to the left), 1: x = l (to the right)
+            type(c_ptr), value        :: dst           ! device buffer, 5 (m+2)(n+2) reals
+         end function
+
+         integer(c_int) function eup_set_x_planes(h, side, src) bind(c, name="eup_set_x_planes")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: side
+            type(c_ptr), value        :: src
+         end function
+
          integer(c_int) function eup_geometry_reference(flag2, lx, ly, lz, variant, g) &
                                  bind(c, name="eup_geometry_reference")
             import :: c_int, c_int32_t, eup_geometry

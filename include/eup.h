@@ -347,6 +347,16 @@ int eup_mem_force_noalloc(int32_t l, int32_t m, int32_t n, const int32_t bc[6], 
 int eup_step_boundaries(eup_handle* h);
 int eup_step_stream(eup_handle* h);
 
+/* eup_step_stream in two parts, so that the plane exchange can overlap compute:
+ * eup_step_stream_interior streams and collides every column that does not pull
+ * from the x halo planes (x = 2..l-1) and may be enqueued right after
+ * eup_get_x_planes, before the planes arrive; eup_step_stream_faces, after
+ * eup_set_x_planes, does the columns x = 1 and x = l and advances the step.  Same
+ * bits as eup_step_stream.  No reference counterpart (the reference exchanges with
+ * blocking MPI calls before its step, CODE/SRC/bcond.comm.packed.F90). */
+int eup_step_stream_interior(eup_handle* h);
+int eup_step_stream_faces(eup_handle* h);
+
 /* The five populations that cross an x face, (m+2)(n+2) values each, index
  * (q', j + (m+2) k) for j = 0..m+1, k = 0..n+1, in the arithmetic type (float,
  * or double for FP64), device pointers.  side 0: column x = 1, populations

@@ -31,8 +31,9 @@ def _single(eup, cfg, obs, a, steps, dt):
         return s.download(dt), s.forces()
 
 
+@pytest.mark.parametrize("split", [False, True], ids=["sequential", "interior_then_faces"])
 @pytest.mark.parametrize("prec,world", [("fp32", 3), ("fp64", 2), ("fp16", 4)])
-def test_slabs_in_one_process_equal_single_lattice(eup, require_gpu, prec, world):
+def test_slabs_in_one_process_equal_single_lattice(eup, require_gpu, prec, world, split):
     from euplectella_hpc_b200.slabs import SlabSolver, gather_state, step_in_process
     code, dt = {"fp32": (eup.FP32, np.float32), "fp64": (eup.FP64, np.float64), "fp16": (eup.FP16_DEV, np.float32)}[prec]
     cfg, obs = _case(eup, code)
@@ -44,7 +45,7 @@ def test_slabs_in_one_process_equal_single_lattice(eup, require_gpu, prec, world
         for s in slabs:
             s.set_obstacles(obs)
             s.upload(a)
-        step_in_process(slabs, steps)
+        step_in_process(slabs, steps, split=split)
         got = gather_state(slabs, dt)
         f = sum(s.solver.forces() for s in slabs)
         assert all(s.solver.itime == steps for s in slabs)
@@ -79,6 +80,16 @@ def test_slab_guards(eup, require_gpu):
             s.step(1)                      # an x-slab steps only in halves
         with pytest.raises(eup.EupError):
             s.step_stream()                # the boundaries half comes first
+        with pytest.raises(eup.EupError):
+            s.step_stream_interior()
+        s.step_boundaries()
+        with pytest.raises(eup.EupError):
+            s.step_stream_faces()          # the interior part comes first
+        s.step_stream_interior()
+        with pytest.raises(eup.EupError):
+            s.step_stream()                # the step is half streamed
+        with pytest.raises(eup.EupError):
+            s.step_boundaries()
         bad = np.zeros((N, M, c1.lx), np.int32)
         bad[3, 4, 0] = 1                   # solid next to the rear exchange face
         with pytest.raises(eup.EupError):
@@ -138,3 +149,31 @@ def test_two_ranks_through_torch_distributed(eup, require_gpu, tmp_path):
             got, want = loc[q][1:-1, 1:-1, 1:-1], ref[q][1:-1, 1:-1, x0:x0 + nx]
             assert np.array_equal(got[fl], want[fl]), (r, q)
         np.testing.assert_allclose(np.load(tmp_path / f"force{r}.npy"), f_ref, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("prec,l", [("fp32", 60), ("fp32", 61), ("fp32", 2), ("fp64", 40), ("fp16", 60), ("bf16", 33)])
+def test_split_stream_equals_whole_step(eup, require_gpu, prec, l):
+    """boundaries + interior columns + face columns gives eup_step's bits (two-node kernel for
+    even l, one-node for odd l and FP64; l = 2 has a single pair holding both face columns)."""
+    code, dt = {"fp32": (eup.FP32, np.float32), "fp64": (eup.FP64, np.float64), "fp16": (eup.FP16_DEV, np.float32),
+                "bf16": (eup.BF16_DEV, np.float32)}[prec]
+    bc = (eup.OUTFLOW, eup.INFLOW, eup.FREESLIP, eup.FREESLIP, eup.PERIODIC, eup.PERIODIC)
+    cfg = eup.Config(l, M, N, bc=bc, svisc=0.01, u_inflow=0.05, precision=code)
+    obs = eup.geometry_cylinder_z(l, M, N, l / 3, 9.5, 2.5) if l > 8 else np.zeros((N, M, l), np.int32)
+    a = eup.init_equilibrium(l, M, N, 0.05, 1e-3, 8, dt)
+    out = []
+    for split in (False, True):
+        with eup.Solver(cfg) as s:
+            s.set_obstacles(obs)
+            s.upload(a)
+            for _ in range(12):
+                if split:
+                    s.step_boundaries()
+                    s.step_stream_interior()
+                    s.step_stream_faces()
+                else:
+                    s.step(1)
+            out.append((s.download(dt), s.force_series(0, 13), s.itime))
+    assert out[0][2] == out[1][2] == 12
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
