@@ -188,11 +188,14 @@ __device__ __forceinline__ void load_pair_raw(const Lat<S, float>& src, const Ge
                                               typename Vec2<S>::T (&r)[19]) {
     using T2 = typename Vec2<S>::T;
     const int l = g.l, lm = (int)g.lm;
+    // a base that is the same for the whole row (block) per population, plus one byte offset
+    // per thread shared by all 19 pulls
+    const int64_t toff = (int64_t)(i - 1) * (int64_t)sizeof(S);
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
         const int cx = (q == 18) ? 0 : cx_of(q), cy = (q == 18) ? 0 : cy_of(q), cz = (q == 18) ? 0 : cz_of(q);
-        const S* rp = src.pop[q] + (rowlin - cy * l - cz * lm);
-        r[q] = *reinterpret_cast<const T2*>(rp + (i - 1 - cx));
+        const char* rp = reinterpret_cast<const char*>(src.pop[q] + (rowlin - cy * l - cz * lm - cx));
+        r[q] = *reinterpret_cast<const T2*>(rp + toff);
     }
 }
 
