@@ -181,22 +181,22 @@ __device__ __forceinline__ void pair_through_shell(const Lat<S, float>& src, con
     }
 }
 
-// 16-bit storage: the 19 pulls of the pair (i, i+1) of an interior row as raw words
-// (aligned in the shifted layout whatever cx is).
+// Population q's source pointer moved back by c_q: the pull a_q(x - c_q) of node index x
+// (0-based, x = i-1 + l (j-1 + m (k-1))) is base[q][x].  Set on the host per launch.
 template <typename S>
-__device__ __forceinline__ void load_pair_raw(const Lat<S, float>& src, const Geo& g, int i, int rowlin,
+struct PullBase {
+    const S* p[19];
+};
+
+// 16-bit storage: the 19 pulls of the pair (i, i+1) of an interior row as raw words
+// (aligned in the shifted layout whatever cx is): one index for all of them.
+template <typename S>
+__device__ __forceinline__ void load_pair_raw(const PullBase<S>& pb, int i, int rowlin,
                                               typename Vec2<S>::T (&r)[19]) {
     using T2 = typename Vec2<S>::T;
-    const int l = g.l, lm = (int)g.lm;
-    // a base that is the same for the whole row (block) per population, plus one byte offset
-    // per thread shared by all 19 pulls
-    const int64_t toff = (int64_t)(i - 1) * (int64_t)sizeof(S);
+    const uint32_t x = (uint32_t)(rowlin + i - 1);
 #pragma unroll
-    for (int q = 0; q < 19; ++q) {
-        const int cx = (q == 18) ? 0 : cx_of(q), cy = (q == 18) ? 0 : cy_of(q), cz = (q == 18) ? 0 : cz_of(q);
-        const char* rp = reinterpret_cast<const char*>(src.pop[q] + (rowlin - cy * l - cz * lm - cx));
-        r[q] = *reinterpret_cast<const T2*>(rp + toff);
-    }
+    for (int q = 0; q < 19; ++q) r[q] = *reinterpret_cast<const T2*>(pb.p[q] + x);
 }
 
 // Everything after the pulls of an interior pair: the x-halo values of the first and
@@ -250,7 +250,7 @@ __device__ __forceinline__ void finish_pair(const Lat<S, float>& src, const Lat<
 // through the halo shell (warp-uniform in the row kernel, where a block is one row).
 template <typename S>
 __device__ __forceinline__ void pair_step(const Lat<S, float>& src, const Lat<S, float>& dst, const Geo& g,
-                                          const Phys<float>& ph, int i, int j, int k) {
+                                          const Phys<float>& ph, const PullBase<S>& pb, int i, int j, int k) {
     using K = KOps<S, float>;
     using V2 = Vec2<S>;
     using T2 = typename V2::T;
@@ -265,7 +265,7 @@ __device__ __forceinline__ void pair_step(const Lat<S, float>& src, const Lat<S,
     F2 x[19];
     if constexpr (dev) {
         T2 r[19];
-        load_pair_raw(src, g, i, rowlin, r);
+        load_pair_raw(pb, i, rowlin, r);
 #pragma unroll
         for (int q = 0; q < 19; ++q) x[q] = F2(V2::unpack(r[q]));
     } else {
@@ -288,22 +288,22 @@ __device__ __forceinline__ void pair_step(const Lat<S, float>& src, const Lat<S,
 // Pairs p0 .. p0+np-1 of every row (pair p: nodes 2p+1, 2p+2); grid (ceil(np/128), m, n).
 template <typename S, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_stream_collide_pair(Lat<S, float> src, Lat<S, float> dst, Geo g,
-                                                                   Phys<float> ph, int p0, int np) {
+                                                                   Phys<float> ph, PullBase<S> pb, int p0, int np) {
     const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     if (t >= np) return;
-    pair_step(src, dst, g, ph, 2 * (p0 + t) + 1, (int)blockIdx.y + 1, (int)blockIdx.z + 1);
+    pair_step(src, dst, g, ph, pb, 2 * (p0 + t) + 1, (int)blockIdx.y + 1, (int)blockIdx.z + 1);
 }
 
 // The first and last pair of every row (the only ones that pull from the x halo planes):
 // one thread per (side, j, k); sides = 1 when l == 2.
 template <typename S>
 __global__ void __launch_bounds__(128, 6) k_stream_collide_pair_faces(Lat<S, float> src, Lat<S, float> dst, Geo g,
-                                                                      Phys<float> ph, int sides) {
+                                                                      Phys<float> ph, PullBase<S> pb, int sides) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (int64_t)sides * g.m * g.n) return;
     const int side = (int)(t % sides);
     const int64_t row = t / sides;
-    pair_step(src, dst, g, ph, side ? g.l - 1 : 1, (int)(row % g.m) + 1, (int)(row / g.m) + 1);
+    pair_step(src, dst, g, ph, pb, side ? g.l - 1 : 1, (int)(row % g.m) + 1, (int)(row / g.m) + 1);
 }
 
 template <typename S, typename R>
@@ -323,10 +323,16 @@ bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const
             if ((!dev || cx == 0) && reinterpret_cast<uintptr_t>(dst.pop[q]) % (2 * sizeof(S)) != 0) return false;
         }
         const int bx = 128;
+        PullBase<S> pb;
+        for (int q = 0; q < Q; ++q) {
+            const int64_t c = (q == 18) ? 0 : (int64_t)cy_of(q) * g.l + (int64_t)cz_of(q) * g.lm + cx_of(q);
+            pb.p[q] = src.pop[q] - c;  // only ever indexed at x >= c: the pull lies in the population
+        }
         if (part == kStreamFaces) {
             const int sides = g.l == 2 ? 1 : 2;
             const int64_t threads = (int64_t)sides * g.m * g.n;
-            k_stream_collide_pair_faces<S><<<(unsigned)((threads + bx - 1) / bx), bx, 0, st>>>(src, dst, g, ph, sides);
+            k_stream_collide_pair_faces<S><<<(unsigned)((threads + bx - 1) / bx), bx, 0, st>>>(src, dst, g, ph, pb,
+                                                                                              sides);
             return true;
         }
         // all pairs, or all but the first and last of each row
@@ -338,11 +344,11 @@ bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const
         // 6 (80 registers) for FP32 storage, 8 (64) for 16-bit storage, whose loads need fewer
         const int minb = occ > 0 ? occ + 3 : (sizeof(S) == 4 ? 6 : 8);
         switch (minb) {
-            case 4: k_stream_collide_pair<S, 4><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
-            case 5: k_stream_collide_pair<S, 5><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
-            case 6: k_stream_collide_pair<S, 6><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
-            case 7: k_stream_collide_pair<S, 7><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
-            default: k_stream_collide_pair<S, 8><<<grid, bx, 0, st>>>(src, dst, g, ph, p0, np); break;
+            case 4: k_stream_collide_pair<S, 4><<<grid, bx, 0, st>>>(src, dst, g, ph, pb, p0, np); break;
+            case 5: k_stream_collide_pair<S, 5><<<grid, bx, 0, st>>>(src, dst, g, ph, pb, p0, np); break;
+            case 6: k_stream_collide_pair<S, 6><<<grid, bx, 0, st>>>(src, dst, g, ph, pb, p0, np); break;
+            case 7: k_stream_collide_pair<S, 7><<<grid, bx, 0, st>>>(src, dst, g, ph, pb, p0, np); break;
+            default: k_stream_collide_pair<S, 8><<<grid, bx, 0, st>>>(src, dst, g, ph, pb, p0, np); break;
         }
         return true;
     }
