@@ -175,3 +175,31 @@ def test_driver_creates_the_reference_column(eup, orc, require_gpu, tmp_path):
     keep[1:-1, 1:-1, 1:-1] = obs == 0
     for q in range(19):
         assert np.array_equal(got[q][keep], ref[q][keep]), q
+
+
+def test_driver_production_column(eup, orc, require_gpu, tmp_path):
+    """The obstacle of the reference's production inputs (CODE/RUN/bgk.*.input: flag1 = 2,
+    flag2 = 2, built with -DCYLINDER_INF): the radius-100 column over every z layer, created on
+    the device by the reference program on a 420x210x4 channel and stepped like the oracle."""
+    lx, ly, lz = 420, 210, 4
+    a = eup.init_equilibrium(lx, ly, lz, 0.05, 1e-3, 29, np.float32)
+    eup.write_raw_state(tmp_path / "restore.00.00.00.bin", a, 0)
+    (tmp_path / "bgk.input").write_text(
+        f"&parameters\n lx = {lx}\n ly = {ly}\n lz = {lz}\n proc_x = 1\n proc_y = 1\n proc_z = 1\n"
+        " svisc=0.02\n u0=0.05\n itfin=10\n ivtim=1000\n isignal=10\n itsave=10\n icheck=10\n"
+        " tstep=10\n irestart=1\n flag1=2\n flag2=2\n flag3=2\n init_v=0        /\n")
+    r = subprocess.run([DRIVER, "--preset", "cylinder_inf"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout
+    obs, _ = orc.created_obstacle(2, lx, ly, lz, lx, ly, lz, cylinder_inf=True)
+    assert obs[-1].sum() == obs[0].sum() > 0 and not obs[:, :, -1].any()  # every layer, clear of i = l
+    assert (tmp_path / "obs.0000.00000000.bin").read_bytes() == orc.obstacle_file_bytes(obs)
+    p = orc.params(lx, ly, lz, [5, 4, 0, 0, 0, 0], svisc=0.02, u_inflow=0.05)
+    ref = a.copy()
+    orc.run(p, ref, obs, 10)
+    got, it = eup.read_raw_state(tmp_path / "save.00.00.00.00000010.bin", lx, ly, lz)
+    assert it == 10
+    keep = np.ones(got.shape[1:], bool)
+    keep[1:-1, 1:-1, 1:-1] = obs == 0
+    for q in range(19):
+        assert np.array_equal(got[q][keep], ref[q][keep]), q
