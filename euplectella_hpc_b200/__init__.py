@@ -42,6 +42,7 @@ EXPORTED = [
     "eup_get_cv_drag", "eup_save_state", "eup_restore_state", "eup_step_boundaries", "eup_step_stream",
     "eup_get_x_planes", "eup_set_x_planes", "eup_geometry_reference", "eup_voxelise", "eup_build_obstacles",
     "eup_get_obstacles", "eup_write_obstacles", "eup_step_stream_interior", "eup_step_stream_faces",
+    "eup_init_reference",
 ]
 
 
@@ -164,6 +165,8 @@ def _load():
         "eup_get_obstacles": ([vp, vp, ctypes.POINTER(i64)], ctypes.c_int),
         "eup_write_obstacles": ([vp, ctypes.c_char_p], ctypes.c_int),
         "eup_step_stream_interior": ([vp], ctypes.c_int), "eup_step_stream_faces": ([vp], ctypes.c_int),
+        "eup_init_reference": ([i32, i32, i32, i32, ctypes.c_int32 * 3, ctypes.c_int32 * 3, i32, dbl, i32, P19],
+                               ctypes.c_int),
     }
     # every entry point gets a prototype: an unprototyped call would pass pointers as C ints
     missing = [name for name in EXPORTED if name not in sig]
@@ -474,6 +477,16 @@ def init_equilibrium(l, m, n, u_in, amp, seed, dtype=np.float32) -> np.ndarray:
     """Synthetic initial state: equilibrium at rho=1, u = inlet + seeded perturbation, halos included."""
     out = np.empty((19, n + 2, m + 2, l + 2), dtype=dtype)
     _check(lib.eup_init_equilibrium(l, m, n, float(u_in), float(amp), int(seed), _elem(out), _ptrs(out)))
+    return out
+
+
+def init_reference(opt, l, m, n, glob=None, start=(0, 0, 0), periodic=False, u0=0.0, dtype=np.float32) -> np.ndarray:
+    """The reference's initial state init(opt) (CODE/SRC/init.F90, options 0..3) for a block
+    l x m x n at start of a glob = (lx, ly, lz) lattice, halos included."""
+    out = np.empty((19, n + 2, m + 2, l + 2), dtype=dtype)
+    g = (ctypes.c_int32 * 3)(*(glob if glob is not None else (l, m, n)))
+    _check(lib.eup_init_reference(int(opt), l, m, n, g, (ctypes.c_int32 * 3)(*start), int(bool(periodic)),
+                                  float(u0), _elem(out), _ptrs(out)))
     return out
 
 

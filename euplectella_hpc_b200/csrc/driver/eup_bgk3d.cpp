@@ -22,7 +22,9 @@
 //   bgk.perf           loop time and MLUPS (CODE/SRC/finalize.F90:58-124)
 //
 //   eup_bgk3d [--preset cylinder_inf|freeslip|driven|couette|check2d|channel | --bc f,r,ri,le,u,d]
-//             [--precision fp32|fp64|fp16|bf16] [--device N] [--drag-length D] [--cv-drag] [--input bgk.input]
+//             [--precision fp32|fp64|fp16|bf16] [--device N] [--drag-length D] [--cv-drag] [--periodic-init]
+//             [--input bgk.input]
+// init_v = 0..3 builds the initial state of CODE/SRC/init.F90 (--periodic-init: its -DPERIODIC coordinates).
 #include <chrono>
 #include <cctype>
 #include <cmath>
@@ -120,6 +122,7 @@ int main(int argc, char** argv) {
     std::string input = "bgk.input", preset = "cylinder_inf", prec = "fp32", bcarg;
     int device = 0;
     bool cv_drag = false;
+    bool periodic_init = false;  // the reference's -DPERIODIC coordinates in init
     double drag_length = 0.0;
     for (int a = 1; a < argc; ++a) {
         const std::string s = argv[a];
@@ -131,6 +134,7 @@ int main(int argc, char** argv) {
         else if (s == "--device") device = std::atoi(next().c_str());
         else if (s == "--drag-length") drag_length = std::atof(next().c_str());
         else if (s == "--cv-drag") cv_drag = true;
+        else if (s == "--periodic-init") periodic_init = true;
         else return die("unknown option " + s);
     }
     std::string err;
@@ -215,8 +219,11 @@ int main(int argc, char** argv) {
         if (eup_read_raw_state("restore.00.00.00.bin", lx, ly, lz, eb, pops, &itstart) != EUP_OK)
             return die("restore file", nullptr);
     } else {
-        if (init_v != 0) return die("only init_v = 0 (rest state) or irestart = 1 are offered");
-        if (eup_init_equilibrium(lx, ly, lz, 0.0, 0.0, 0, eb, pops) != EUP_OK) return die("init", nullptr);
+        // CODE/SRC/init.F90 with the namelist's init_v, after build_bcond has settled u0
+        const int32_t glob[3] = {lx, ly, lz}, start[3] = {0, 0, 0};
+        if (eup_init_reference((int32_t)init_v, lx, ly, lz, glob, start, periodic_init ? 1 : 0, cfg.u0, eb, pops) !=
+            EUP_OK)
+            return die("init", nullptr);
     }
     if (eup_upload(h, pops, eb, itstart) != EUP_OK) return die("eup_upload", h);
 

@@ -154,6 +154,73 @@ int eup_write_raw_state(const char* path, int32_t l, int32_t m, int32_t n, int32
     return EUP_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// One coordinate of CODE/SRC/init.F90:110-133 for index c (0 .. size+1) of a block
+// starting at `start` in a lattice of `size` nodes, scaled by `scale` (x is scaled by lz in
+// the reference).  Default build: evaluated in default REAL (single precision) whatever
+// mykind is; -DPERIODIC: (c + start - 1/2)/size formed in quad precision and rounded to
+// mykind, which is one correctly rounded division of exact operands in T.
+template <typename T>
+T init_coord(int c, int start, int size, int scale, bool periodic) {
+    if (periodic) return (T)((T)(c + start) - (T)0.5) / (T)size;
+    const float a = (float)(c + start) - 0.5f - 0.5f * (float)size;
+    return (T)(a / (0.5f * (float)scale));
+}
+
+template <typename T>
+void init_reference_t(int opt, int32_t l, int32_t m, int32_t n, const int32_t glob[3], const int32_t start[3],
+                      bool periodic, double u0, void* const pops[19]) {
+    const T pi = (T)3.141592653589793238462643383279f;  // a default-REAL parameter (:61)
+    const T tenth = (T)0.1f, two = (T)2, u0t = (T)u0;
+    const int64_t L2 = l + 2, M2 = m + 2;
+    T* dst[19];
+    for (int q = 0; q < 19; ++q) dst[q] = static_cast<T*>(pops[q]);
+#pragma omp parallel for schedule(static)
+    for (int32_t k = 0; k <= n + 1; ++k) {
+        const T z = init_coord<T>(k, start[2], glob[2], glob[2], periodic);
+        for (int32_t j = 0; j <= m + 1; ++j)
+            for (int32_t i = 0; i <= l + 1; ++i) {
+                const T x = init_coord<T>(i, start[0], glob[0], periodic ? glob[0] : glob[2], periodic);
+                T xj = 0, yj = 0, zj = 0;
+                if (opt == 1) {
+                    xj = tenth * ((T)1 - z * z);  // Poiseuille (:148-152)
+                } else if (opt == 2) {
+                    xj = u0t * std::sin(two * pi * z);  // decaying flow (:154-161)
+                } else if (opt == 3) {            // Kida vortices (:163-171)
+                    xj = tenth * std::sin(two * pi * x) * std::cos(two * pi * z);
+                    zj = -(tenth * std::cos(two * pi * x) * std::sin(two * pi * z));
+                }
+                T f[19];
+                eup::equilibrium<T>(xj, yj, zj, f);
+                const int64_t L = i + L2 * (j + M2 * (int64_t)k);
+                for (int q = 0; q < 19; ++q) dst[q][L] = f[q];
+            }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int eup_init_reference(int32_t opt, int32_t l, int32_t m, int32_t n, const int32_t global[3], const int32_t start[3],
+                       int32_t periodic, double u0, int32_t elem_bytes, void* const pops[19]) {
+    if (!pops || !global || !start || (elem_bytes != 4 && elem_bytes != 8) || l < 1 || m < 1 || n < 1 ||
+        global[0] < 1 || global[1] < 1 || global[2] < 1)
+        return herr(EUP_ERR_INVALID_ARG, "eup_init_reference: bad argument");
+    for (int q = 0; q < 19; ++q)
+        if (!pops[q]) return herr(EUP_ERR_INVALID_ARG, "eup_init_reference: null population array");
+    if (opt == 4 || opt == 5)
+        return herr(EUP_ERR_UNSUPPORTED, "eup_init_reference: the reference stops on init option " +
+                                              std::to_string(opt) + " (\"still to port\")");
+    if (opt < 0 || opt > 5) return herr(EUP_ERR_INVALID_ARG, "eup_init_reference: option out of range [0,5]");
+    if (elem_bytes == 4) init_reference_t<float>(opt, l, m, n, global, start, periodic != 0, u0, pops);
+    else init_reference_t<double>(opt, l, m, n, global, start, periodic != 0, u0, pops);
+    return EUP_OK;
+}
+
 int eup_init_equilibrium(int32_t l, int32_t m, int32_t n, double u_in, double amp, uint64_t seed, int32_t elem_bytes,
                          void* const pops[19]) {
     if (!pops || (elem_bytes != 4 && elem_bytes != 8) || l < 1 || m < 1 || n < 1)

@@ -190,6 +190,17 @@
             type(c_ptr), value        :: src
          end function
 
+         integer(c_int) function eup_init_reference(opt, l, m, n, glob, start, periodic, u0, elem_bytes, &
+                                                     pops) bind(c, name="eup_init_reference")
+            import :: c_int, c_int32_t, c_double, c_ptr
+            integer(c_int32_t), value   :: opt, l, m, n   ! opt = init_v
+            integer(c_int32_t)          :: glob(3), start(3)  ! (lx,ly,lz), mpicoords*(l,m,n)
+            integer(c_int32_t), value   :: periodic       ! 1 for the -DPERIODIC coordinates
+            real(c_double), value       :: u0
+            integer(c_int32_t), value   :: elem_bytes
+            type(c_ptr), intent(in)     :: pops(19)       ! c_loc(a01(0,0,0)) ... c_loc(a19(0,0,0))
+         end function
+
          integer(c_int) function eup_geometry_reference(flag2, lx, ly, lz, variant, g) &
                                  bind(c, name="eup_geometry_reference")
             import :: c_int, c_int32_t, eup_geometry

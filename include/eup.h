@@ -415,6 +415,20 @@ int eup_read_raw_state(const char* path, int32_t l, int32_t m, int32_t n, int32_
 int eup_write_raw_state(const char* path, int32_t l, int32_t m, int32_t n, int32_t elem_bytes,
                         const void* const pops[19], int64_t itime);
 
+/* The initial states of CODE/SRC/init.F90:42-236 (init(opt), called with the
+ * namelist's init_v): the equilibrium at rho = 1 of 0 rest, 1 Poiseuille
+ * u_x = 0.1 (1 - z^2), 2 decaying shear u_x = u0 sin(2 pi z), 3 Kida vortices
+ * u = 0.1 (sin 2pi x cos 2pi z, 0, -cos 2pi x sin 2pi z), over the haloed arrays,
+ * with the reference's coordinates and constants (single-precision literals,
+ * x scaled by lz; periodic != 0 selects the -DPERIODIC coordinates (k - 1/2)/lz).
+ * global = (lx, ly, lz) of the whole lattice; start = mpicoords * (l, m, n) places
+ * this block in it.  u0 is the one the reference holds after build_bcond (0 with an
+ * inlet or a lid).  Options 4 and 5 stop the reference ("still to port") and return
+ * EUP_ERR_UNSUPPORTED. */
+int eup_init_reference(int32_t opt, int32_t l, int32_t m, int32_t n, const int32_t global[3],
+                       const int32_t start[3], int32_t periodic, double u0, int32_t elem_bytes,
+                       void* const pops[19]);
+
 /* Equilibrium state of CODE/SRC/init.F90:194-232 with rho = 1 and
  * u = (u_in + amp*xi_x, amp*xi_y, amp*xi_z), xi uniform in [-1,1) from
  * splitmix64(seed + 3 L + c) (L haloed linear index, c the component), halos

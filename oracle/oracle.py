@@ -62,6 +62,11 @@ def lib():
             getattr(L, f"orc_{pfx}_init_perturbed").argtypes = [
                 ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                 ctypes.c_uint64, PP]
+            I3 = ctypes.c_int32 * 3
+            getattr(L, f"orc_{pfx}_init_reference").argtypes = [
+                ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, I3, I3, ctypes.c_int32,
+                ctypes.c_double, PP]
+            getattr(L, f"orc_{pfx}_init_reference").restype = ctypes.c_int
             getattr(L, f"orc_{pfx}_mem_force").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_void_p, ctypes.c_void_p]
             getattr(L, f"orc_{pfx}_monitor").argtypes = [ctypes.POINTER(Params), PP, ctypes.c_void_p, ctypes.c_void_p]
             getattr(L, f"orc_{pfx}_macro").argtypes = [ctypes.POINTER(Params), PP] + [ctypes.c_void_p] * 4
@@ -119,6 +124,18 @@ def new_state(l, m, n, dtype=np.float32) -> np.ndarray:
 def init_perturbed(l, m, n, u_in, amp, seed, dtype=np.float32) -> np.ndarray:
     a = new_state(l, m, n, dtype)
     getattr(lib(), f"orc_{_pfx(a)}_init_perturbed")(l, m, n, u_in, amp, seed, _ptrs(a))
+    return a
+
+
+def init_reference(opt, l, m, n, glob=None, start=(0, 0, 0), periodic=False, u0=0.0, dtype=np.float32):
+    """init(opt) of CODE/SRC/init.F90 (options 0..3) on a block of a glob lattice."""
+    a = new_state(l, m, n, dtype)
+    g = (ctypes.c_int32 * 3)(*(glob if glob is not None else (l, m, n)))
+    st = (ctypes.c_int32 * 3)(*start)
+    rc = getattr(lib(), f"orc_{_pfx(a)}_init_reference")(opt, l, m, n, g, st, int(bool(periodic)), float(u0),
+                                                           _ptrs(a))
+    if rc != 0:
+        raise ValueError(f"init option {opt} not restated")
     return a
 
 

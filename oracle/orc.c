@@ -5,6 +5,7 @@
  */
 #include "orc.h"
 
+#include <math.h>
 #include <stdlib.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -30,15 +31,23 @@ int32_t orc_nthreads(void)
 
 #define REAL float
 #define P f
+#define RSIN sinf
+#define RCOS cosf
 #include "orc_impl.h"
 #undef REAL
 #undef P
+#undef RSIN
+#undef RCOS
 
 #define REAL double
 #define P d
+#define RSIN sin
+#define RCOS cos
 #include "orc_impl.h"
 #undef REAL
 #undef P
+#undef RSIN
+#undef RCOS
 
 /* D3Q19 velocities in the reference's order a01..a18 (CODE/SRC/bgk3d.F90:30-49). */
 static const int CX[18] = {1, 1, 1, 1, 1, 0, 0, 0, 0, -1, -1, -1, -1, -1, 0, 0, 0, 0};

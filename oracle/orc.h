@@ -54,6 +54,9 @@ typedef struct orc_params {
                       const int32_t* obs, int32_t nsteps);                                \
     void orc_##P##_init_perturbed(int32_t l, int32_t m, int32_t n, double u_in,           \
                                   double amp, uint64_t seed, REAL* const a[19]);          \
+    int orc_##P##_init_reference(int32_t opt, int32_t l, int32_t m, int32_t n,            \
+                                 const int32_t glob[3], const int32_t start[3],           \
+                                 int32_t periodic, double u0, REAL* const a[19]);         \
     void orc_##P##_mem_force(const orc_params* p, REAL* const a[19], const int32_t* obs,  \
                              double out[3]);                                              \
     void orc_##P##_monitor(const orc_params* p, REAL* const a[19], const int32_t* obs,    \

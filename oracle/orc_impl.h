@@ -497,6 +497,53 @@ int FN(run)(const orc_params* p, REAL* const a[19], REAL* const b[19], const int
  * splitmix64(seed + 3*L + c), L the haloed linear index; populations set to
  * the equilibrium of CODE/SRC/init.F90:194-232 with crho = 1, halos included.
  */
+/* The equilibrium of CODE/SRC/init.F90:194-232 at rho = 1 and velocity (xj, yj, zj),
+ * stored at haloed index L of the 19 arrays. */
+static void FN(equilibrium_at)(REAL xj, REAL yj, REAL zj, REAL* const a[19], int64_t L)
+{
+    const REAL crho = (REAL)1.0;
+    const REAL cvsq = xj * xj + yj * yj + zj * zj;
+    const REAL T = (REAL)3.0;
+    const REAL cx01 = RF * (xj - yj) + QF * (T * (xj - yj) * (xj - yj) - cvsq);
+    const REAL cx02 = RF * (xj - zj) + QF * (T * (xj - zj) * (xj - zj) - cvsq);
+    const REAL cx03 = RF * (xj + yj) + QF * (T * (xj + yj) * (xj + yj) - cvsq);
+    const REAL cx04 = RF * (xj + zj) + QF * (T * (xj + zj) * (xj + zj) - cvsq);
+    const REAL cx05 = RF * (xj) + QF * (T * (xj) * (xj) - cvsq);
+    const REAL cx06 = RF * (zj) + QF * (T * (zj) * (zj) - cvsq);
+    const REAL cx07 = RF * (yj + zj) + QF * (T * (yj + zj) * (yj + zj) - cvsq);
+    const REAL cx08 = RF * (yj) + QF * (T * (yj) * (yj) - cvsq);
+    const REAL cx09 = RF * (yj - zj) + QF * (T * (yj - zj) * (yj - zj) - cvsq);
+    const REAL cx10 = RF * (-xj - yj) + QF * (T * (xj + yj) * (xj + yj) - cvsq);
+    const REAL cx11 = RF * (-xj - zj) + QF * (T * (xj + zj) * (xj + zj) - cvsq);
+    const REAL cx12 = RF * (-xj + yj) + QF * (T * (xj - yj) * (xj - yj) - cvsq);
+    const REAL cx13 = RF * (-xj + zj) + QF * (T * (xj - zj) * (xj - zj) - cvsq);
+    const REAL cx14 = RF * (-xj) + QF * (T * (xj) * (xj) - cvsq);
+    const REAL cx15 = RF * (-zj) + QF * (T * (zj) * (zj) - cvsq);
+    const REAL cx16 = RF * (-yj - zj) + QF * (T * (yj + zj) * (yj + zj) - cvsq);
+    const REAL cx17 = RF * (-yj) + QF * (T * (yj) * (yj) - cvsq);
+    const REAL cx18 = RF * (-yj + zj) + QF * (T * (yj - zj) * (yj - zj) - cvsq);
+    const REAL cx19 = RF * ((REAL)0.0) + QF * (T * ((REAL)0.0) * ((REAL)0.0) - cvsq);
+    a[0][L] = crho * P2 * ((REAL)1.0 + cx01);
+    a[1][L] = crho * P2 * ((REAL)1.0 + cx02);
+    a[2][L] = crho * P2 * ((REAL)1.0 + cx03);
+    a[3][L] = crho * P2 * ((REAL)1.0 + cx04);
+    a[4][L] = crho * P1 * ((REAL)1.0 + cx05);
+    a[5][L] = crho * P1 * ((REAL)1.0 + cx06);
+    a[6][L] = crho * P2 * ((REAL)1.0 + cx07);
+    a[7][L] = crho * P1 * ((REAL)1.0 + cx08);
+    a[8][L] = crho * P2 * ((REAL)1.0 + cx09);
+    a[9][L] = crho * P2 * ((REAL)1.0 + cx10);
+    a[10][L] = crho * P2 * ((REAL)1.0 + cx11);
+    a[11][L] = crho * P2 * ((REAL)1.0 + cx12);
+    a[12][L] = crho * P2 * ((REAL)1.0 + cx13);
+    a[13][L] = crho * P1 * ((REAL)1.0 + cx14);
+    a[14][L] = crho * P1 * ((REAL)1.0 + cx15);
+    a[15][L] = crho * P2 * ((REAL)1.0 + cx16);
+    a[16][L] = crho * P1 * ((REAL)1.0 + cx17);
+    a[17][L] = crho * P2 * ((REAL)1.0 + cx18);
+    a[18][L] = crho * P0 * ((REAL)1.0 + cx19);
+}
+
 void FN(init_perturbed)(int32_t l_, int32_t m_, int32_t n_, double u_in, double amp,
                         uint64_t seed, REAL* const a[19])
 {
@@ -512,48 +559,52 @@ void FN(init_perturbed)(int32_t l_, int32_t m_, int32_t n_, double u_in, double 
         const REAL xj = (REAL)(u_in + amp * xi[0]);
         const REAL yj = (REAL)(amp * xi[1]);
         const REAL zj = (REAL)(amp * xi[2]);
-        const REAL crho = (REAL)1.0;
-        const REAL cvsq = xj * xj + yj * yj + zj * zj;
-        const REAL T = (REAL)3.0;
-        const REAL cx01 = RF * (xj - yj) + QF * (T * (xj - yj) * (xj - yj) - cvsq);
-        const REAL cx02 = RF * (xj - zj) + QF * (T * (xj - zj) * (xj - zj) - cvsq);
-        const REAL cx03 = RF * (xj + yj) + QF * (T * (xj + yj) * (xj + yj) - cvsq);
-        const REAL cx04 = RF * (xj + zj) + QF * (T * (xj + zj) * (xj + zj) - cvsq);
-        const REAL cx05 = RF * (xj) + QF * (T * (xj) * (xj) - cvsq);
-        const REAL cx06 = RF * (zj) + QF * (T * (zj) * (zj) - cvsq);
-        const REAL cx07 = RF * (yj + zj) + QF * (T * (yj + zj) * (yj + zj) - cvsq);
-        const REAL cx08 = RF * (yj) + QF * (T * (yj) * (yj) - cvsq);
-        const REAL cx09 = RF * (yj - zj) + QF * (T * (yj - zj) * (yj - zj) - cvsq);
-        const REAL cx10 = RF * (-xj - yj) + QF * (T * (xj + yj) * (xj + yj) - cvsq);
-        const REAL cx11 = RF * (-xj - zj) + QF * (T * (xj + zj) * (xj + zj) - cvsq);
-        const REAL cx12 = RF * (-xj + yj) + QF * (T * (xj - yj) * (xj - yj) - cvsq);
-        const REAL cx13 = RF * (-xj + zj) + QF * (T * (xj - zj) * (xj - zj) - cvsq);
-        const REAL cx14 = RF * (-xj) + QF * (T * (xj) * (xj) - cvsq);
-        const REAL cx15 = RF * (-zj) + QF * (T * (zj) * (zj) - cvsq);
-        const REAL cx16 = RF * (-yj - zj) + QF * (T * (yj + zj) * (yj + zj) - cvsq);
-        const REAL cx17 = RF * (-yj) + QF * (T * (yj) * (yj) - cvsq);
-        const REAL cx18 = RF * (-yj + zj) + QF * (T * (yj - zj) * (yj - zj) - cvsq);
-        const REAL cx19 = RF * ((REAL)0.0) + QF * (T * ((REAL)0.0) * ((REAL)0.0) - cvsq);
-        a[0][L] = crho * P2 * ((REAL)1.0 + cx01);
-        a[1][L] = crho * P2 * ((REAL)1.0 + cx02);
-        a[2][L] = crho * P2 * ((REAL)1.0 + cx03);
-        a[3][L] = crho * P2 * ((REAL)1.0 + cx04);
-        a[4][L] = crho * P1 * ((REAL)1.0 + cx05);
-        a[5][L] = crho * P1 * ((REAL)1.0 + cx06);
-        a[6][L] = crho * P2 * ((REAL)1.0 + cx07);
-        a[7][L] = crho * P1 * ((REAL)1.0 + cx08);
-        a[8][L] = crho * P2 * ((REAL)1.0 + cx09);
-        a[9][L] = crho * P2 * ((REAL)1.0 + cx10);
-        a[10][L] = crho * P2 * ((REAL)1.0 + cx11);
-        a[11][L] = crho * P2 * ((REAL)1.0 + cx12);
-        a[12][L] = crho * P2 * ((REAL)1.0 + cx13);
-        a[13][L] = crho * P1 * ((REAL)1.0 + cx14);
-        a[14][L] = crho * P1 * ((REAL)1.0 + cx15);
-        a[15][L] = crho * P2 * ((REAL)1.0 + cx16);
-        a[16][L] = crho * P1 * ((REAL)1.0 + cx17);
-        a[17][L] = crho * P2 * ((REAL)1.0 + cx18);
-        a[18][L] = crho * P0 * ((REAL)1.0 + cx19);
+        FN(equilibrium_at)(xj, yj, zj, a, L);
     }
+}
+
+/*
+ * The initial states of CODE/SRC/init.F90:42-236, init(opt), for a block of l x m x n
+ * nodes starting at start[] (mpicoords * size) in a glob[0] x glob[1] x glob[2] lattice.
+ * Coordinates, :110-133: the default build forms them in default REAL (single precision,
+ * whatever mykind is), x scaled by nn; -DPERIODIC forms (c + start - 0.5_qp)/size in quad
+ * precision and rounds it to mykind -- one division of exact operands in REAL gives the
+ * same value.  pi (:61) is a default-REAL parameter, and so are the literals 0.1.
+ * Options 4 and 5 stop the reference (:174-188); this returns -1 for them.
+ */
+int FN(init_reference)(int32_t opt, int32_t l_, int32_t m_, int32_t n_, const int32_t glob[3],
+                       const int32_t start[3], int32_t periodic, double u0, REAL* const a[19])
+{
+    if (opt < 0 || opt > 3) return -1;
+    const int64_t L2 = l_ + 2, M2 = m_ + 2;
+    const int ll = glob[0], nn = glob[2];
+    const REAL pi = (REAL)3.141592653589793238462643383279f;
+    const REAL u0m = (REAL)u0;  /* u0 held as real(mykind) */
+    for (int k = 0; k <= n_ + 1; ++k) {
+        REAL z;
+        if (periodic) z = ((REAL)(k + start[2]) - (REAL)0.5) / (REAL)nn;
+        else z = (REAL)(((float)(k + start[2]) - 0.5f - 0.5f * (float)nn) / (0.5f * (float)nn));
+        for (int j = 0; j <= m_ + 1; ++j) {
+            for (int i = 0; i <= l_ + 1; ++i) {
+                REAL x;
+                if (periodic) x = ((REAL)(i + start[0]) - (REAL)0.5) / (REAL)ll;
+                else x = (REAL)(((float)(i + start[0]) - 0.5f - 0.5f * (float)ll) / (0.5f * (float)nn));
+                REAL xj = (REAL)0.0, yj = (REAL)0.0, zj = (REAL)0.0;
+                if (opt == 1) {                                   /* poiseuille, :148-152 */
+                    xj = (REAL)0.1f * ((REAL)1 - z * z);
+                }
+                if (opt == 2) {                                   /* decaying flow, :154-161 */
+                    xj = u0m * RSIN((REAL)2 * pi * z);
+                }
+                if (opt == 3) {                                   /* kida vortices, :163-171 */
+                    xj = (REAL)0.1f * RSIN((REAL)2 * pi * x) * RCOS((REAL)2 * pi * z);
+                    zj = -((REAL)0.1f * RCOS((REAL)2 * pi * x) * RSIN((REAL)2 * pi * z));
+                }
+                FN(equilibrium_at)(xj, yj, zj, a, (int64_t)i + L2 * ((int64_t)j + M2 * (int64_t)k));
+            }
+        }
+    }
+    return 0;
 }
 
 /*

@@ -70,3 +70,24 @@ def test_driver_runs_reference_inputs(eup, orc, require_gpu, tmp_path):
     probe = (tmp_path / "probe_g.0000.dat").read_text().split("\n")[0]
     assert probe.startswith("     110") and "E" in probe
     assert "Mlups" in (tmp_path / "bgk.perf").read_text()
+
+
+@pytest.mark.parametrize("init_v,periodic", [(1, False), (3, True)])
+def test_driver_reference_initial_states(eup, orc, require_gpu, tmp_path, init_v, periodic):
+    """init_v = 1 (Poiseuille) and 3 (Kida vortices, -DPERIODIC coordinates) built by the
+    program through eup_init_reference, stepped on a fully periodic box like the oracle."""
+    l, m, n = 32, 12, 16
+    (tmp_path / "bgk.input").write_text(
+        f"&parameters\n lx = {l}\n ly = {m}\n lz = {n}\n proc_x = 1\n proc_y = 1\n proc_z = 1\n"
+        " svisc=0.02\n u0=0.0\n itfin=10\n ivtim=1000\n isignal=10\n itsave=10\n icheck=10\n"
+        f" tstep=10\n irestart=0\n flag1=0\n flag2=2\n flag3=0\n init_v={init_v}        /\n")
+    args = [DRIVER, "--bc", "0,0,0,0,0,0"] + (["--periodic-init"] if periodic else [])
+    r = subprocess.run(args, cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr + r.stdout
+    a = orc.init_reference(init_v, l, m, n, periodic=periodic)
+    p = orc.params(l, m, n, [0, 0, 0, 0, 0, 0], svisc=0.02)
+    orc.run(p, a, None, 10)
+    got, it = eup.read_raw_state(tmp_path / "save.00.00.00.00000010.bin", l, m, n)
+    assert it == 10
+    for q in range(19):
+        assert np.array_equal(got[q], a[q]), q
