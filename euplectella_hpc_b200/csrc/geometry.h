@@ -52,7 +52,7 @@ EUP_HD inline double atan_unit(double t) {
     }
     const double t2 = t * t;
     double s = 0.0;
-#ifdef __CUDACC__
+#ifdef __CUDA_ARCH__
 #pragma unroll
 #endif
     for (int k = 13; k >= 0; --k) s = 1.0 / (double)(2 * k + 1) - t2 * s;
