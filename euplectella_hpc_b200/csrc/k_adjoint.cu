@@ -323,9 +323,12 @@ __device__ __forceinline__ R pull_pre(const Lat<R, R>& L, const Geo& g, int q, i
 
 // Forward partial-bounce-back step; the FP64 force of the step goes to
 // series[(itime + 1) % cap] and the device step counter advances.
-template <typename R>
-__global__ void __launch_bounds__(256) k_pbb_step(Lat<R, R> src, Lat<R, R> dst, Geo g, Phys<R> ph, const R* ns,
-                                                  Reduce red, double* series, int64_t cap, int64_t* d_itime) {
+// MINB: resident blocks per SM the registers are sized for (FP32: 4, at 64 registers;
+// FP64 keeps its accumulators in 128).
+template <typename R, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pbb_step(Lat<R, R> src, Lat<R, R> dst, Geo g, Phys<R> ph,
+                                                        const R* ns, Reduce red, double* series, int64_t cap,
+                                                        int64_t* d_itime) {
     double f[3] = {0.0, 0.0, 0.0};
     for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.N;
          lin += (int64_t)gridDim.x * blockDim.x) {
@@ -485,7 +488,8 @@ unsigned capped_grid(int64_t work, int tpb) {
 template <typename R>
 void launch_pbb_step(const Lat<R, R>& src, const Lat<R, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
                      const Reduce& red, double* series, int64_t cap, int64_t* d_itime, cudaStream_t st) {
-    k_pbb_step<R><<<capped_grid(g.N, 256), 256, 0, st>>>(src, dst, g, ph, ns, red, series, cap, d_itime);
+    k_pbb_step<R, sizeof(R) == 4 ? 4 : 1><<<capped_grid(g.N, 256), 256, 0, st>>>(src, dst, g, ph, ns, red, series,
+                                                                                   cap, d_itime);
 }
 
 template <typename R>
