@@ -241,6 +241,167 @@
             type(c_ptr), value        :: obs
             integer(c_int64_t)        :: nobs
          end function
+
+         ! ---- the remaining entry points of include/eup.h ----
+         integer(c_int32_t) function eup_abi_version() bind(c, name="eup_abi_version")
+            import :: c_int32_t
+         end function
+
+         integer(c_int32_t) function eup_device_count() bind(c, name="eup_device_count")
+            import :: c_int32_t
+         end function
+
+         integer(c_int) function eup_synchronize(h) bind(c, name="eup_synchronize")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+         end function
+
+         integer(c_int) function eup_get_stream(h, stream) bind(c, name="eup_get_stream")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            type(c_ptr)        :: stream            ! the handle's cudaStream_t
+         end function
+
+         integer(c_int) function eup_get_itime(h, itime) bind(c, name="eup_get_itime")
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int64_t) :: itime
+         end function
+
+         integer(c_int) function eup_get_launch_count(h, launches) bind(c, name="eup_get_launch_count")
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int64_t) :: launches
+         end function
+
+         integer(c_int) function eup_get_force_series(h, first, cnt, fxyz) bind(c, name="eup_get_force_series")
+            import :: c_int, c_ptr, c_int64_t, c_int32_t, c_double
+            type(c_ptr), value        :: h
+            integer(c_int64_t), value :: first
+            integer(c_int32_t), value :: cnt
+            real(c_double)            :: fxyz(3, *)
+         end function
+
+         integer(c_int) function eup_get_links(h, links) bind(c, name="eup_get_links")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            type(c_ptr), value :: links             ! c_loc of integer(c_int32_t) links(l,m,n)
+         end function
+
+         integer(c_int) function eup_get_boundary_solid(h, list, cap, count) bind(c, name="eup_get_boundary_solid")
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value        :: h
+            type(c_ptr), value        :: list       ! integer(c_int64_t) list(cap), or c_null_ptr
+            integer(c_int64_t), value :: cap
+            integer(c_int64_t)        :: count
+         end function
+
+         integer(c_int) function eup_get_line(h, axis, c1, c2, out) bind(c, name="eup_get_line")
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: axis, c1, c2   ! prof_i/j/k: 0, 1, 2
+            real(c_double)            :: out(4, *)      ! u, w, v, den per node
+         end function
+
+         integer(c_int) function eup_get_plane_means(h, axis, out) bind(c, name="eup_get_plane_means")
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: axis
+            real(c_double)            :: out(4, *)
+         end function
+
+         integer(c_int) function eup_get_cv_drag(h, box, out) bind(c, name="eup_get_cv_drag")
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int32_t) :: box(6)            ! i1, i2, j1, j2, k1, k2
+            real(c_double)     :: out(2)            ! fluxX, fluxY
+         end function
+
+         integer(c_int) function eup_save_state(h, path, elem_bytes) bind(c, name="eup_save_state")
+            import :: c_int, c_ptr, c_char, c_int32_t
+            type(c_ptr), value                 :: h
+            character(kind=c_char), intent(in) :: path(*)
+            integer(c_int32_t), value          :: elem_bytes
+         end function
+
+         integer(c_int) function eup_restore_state(h, path, elem_bytes) bind(c, name="eup_restore_state")
+            import :: c_int, c_ptr, c_char, c_int32_t
+            type(c_ptr), value                 :: h
+            character(kind=c_char), intent(in) :: path(*)
+            integer(c_int32_t), value          :: elem_bytes
+         end function
+
+         integer(c_int) function eup_write_obs_file(path, l, m, n, obs) bind(c, name="eup_write_obs_file")
+            import :: c_int, c_char, c_int32_t, c_ptr
+            character(kind=c_char), intent(in) :: path(*)
+            integer(c_int32_t), value :: l, m, n
+            type(c_ptr), value        :: obs
+         end function
+
+         integer(c_int) function eup_read_raw_state(path, l, m, n, elem_bytes, pops, itime) &
+                                 bind(c, name="eup_read_raw_state")
+            import :: c_int, c_char, c_int32_t, c_int64_t, c_ptr
+            character(kind=c_char), intent(in) :: path(*)
+            integer(c_int32_t), value :: l, m, n, elem_bytes
+            type(c_ptr), intent(in)   :: pops(19)
+            integer(c_int64_t)        :: itime
+         end function
+
+         integer(c_int) function eup_write_raw_state(path, l, m, n, elem_bytes, pops, itime) &
+                                 bind(c, name="eup_write_raw_state")
+            import :: c_int, c_char, c_int32_t, c_int64_t, c_ptr
+            character(kind=c_char), intent(in) :: path(*)
+            integer(c_int32_t), value  :: l, m, n, elem_bytes
+            type(c_ptr), intent(in)    :: pops(19)
+            integer(c_int64_t), value  :: itime
+         end function
+
+         integer(c_int) function eup_init_equilibrium(l, m, n, u_in, amp, seed, elem_bytes, pops) &
+                                 bind(c, name="eup_init_equilibrium")
+            import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr
+            integer(c_int32_t), value :: l, m, n
+            real(c_double), value     :: u_in, amp
+            integer(c_int64_t), value :: seed
+            integer(c_int32_t), value :: elem_bytes
+            type(c_ptr), intent(in)   :: pops(19)
+         end function
+
+         integer(c_int) function eup_mem_force_noalloc(l, m, n, bc, pops, elem_bytes, obs, force, stream) &
+                                 bind(c, name="eup_mem_force_noalloc")
+            import :: c_int, c_int32_t, c_ptr
+            integer(c_int32_t), value :: l, m, n
+            integer(c_int32_t)        :: bc(6)
+            type(c_ptr), intent(in)   :: pops(19)   ! device pointers (host_data use_device)
+            integer(c_int32_t), value :: elem_bytes
+            type(c_ptr), value        :: obs, force, stream
+         end function
+
+         integer(c_int) function eup_geometry_cylinder_z(l, m, n, xc, yc, r, obs) bind(c, name="eup_geometry_cylinder_z")
+            import :: c_int, c_int32_t, c_double, c_ptr
+            integer(c_int32_t), value :: l, m, n
+            real(c_double), value     :: xc, yc, r
+            type(c_ptr), value        :: obs
+         end function
+
+         integer(c_int) function eup_geometry_reticular_shell(l, m, n, x0, length, yc, zc, outer_d, strut_d, pitch, &
+                                                               seed, obs) bind(c, name="eup_geometry_reticular_shell")
+            import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr
+            integer(c_int32_t), value :: l, m, n
+            real(c_double), value     :: x0, length, yc, zc, outer_d, strut_d, pitch
+            integer(c_int64_t), value :: seed
+            type(c_ptr), value        :: obs
+         end function
+
+         integer(c_int) function eup_geometry_ridged_shell(l, m, n, x0, length, yc, zc, outer_d, strut_d, pitch, &
+                                                            ridge_h, ridge_t, cap_t, pore_d, smooth_w, seed, ns, &
+                                                            dns_dh) bind(c, name="eup_geometry_ridged_shell")
+            import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr
+            integer(c_int32_t), value :: l, m, n
+            real(c_double), value     :: x0, length, yc, zc, outer_d, strut_d, pitch
+            real(c_double), value     :: ridge_h, ridge_t, cap_t, pore_d, smooth_w
+            integer(c_int64_t), value :: seed
+            type(c_ptr), value        :: ns, dns_dh
+         end function
       end interface
 
       end module eup_mod

@@ -135,3 +135,13 @@ def test_geometry_ridged_shell(eup):
     hm = eup.geometry_ridged_shell(*args, 4.0 - 1e-5, 3.0, 4.0, 5.0, 1.0, 7)
     fd = (hp - hm) / 2e-5
     assert np.abs(fd - d).max() < 1e-5 * max(1.0, np.abs(d).max())
+
+
+def test_fortran_module_binds_every_entry_point():
+    """fortran/eup_mod.F90 declares a bind(c) interface, once, for every function of include/eup.h
+    (it is not compiled here: there is no Fortran compiler), in free-form lines of at most 132
+    characters."""
+    src = open(os.path.join(ROOT, "fortran", "eup_mod.F90")).read()
+    bound = re.findall(r'bind\(c,\s*name="(eup_[a-z0-9_]+)"\)', src)
+    assert sorted(bound) == header_functions()
+    assert max(len(line) for line in src.splitlines()) <= 132
