@@ -109,11 +109,12 @@ const char* eup_last_error(const eup_handle* h);
 /* ---- state ---------------------------------------------------------------- */
 
 /* Installs the solid mask obs(1:l,1:m,1:n) (1 = solid): builds the bit-packed
- * mask, the list of solid voxels adjacent to fluid or halo, and the bounding
- * box.  Replaces CODE/SRC/build.obs.F90:33-194 as consumed by
- * CODE/SRC/bcond.obs.F90:47-77.  Solid voxels on the outflow plane i = l are
- * rejected (EUP_ERR_UNSUPPORTED): there the reference's result depends on the
- * iteration order of its bounce-back loop. */
+ * mask, the list of solid voxels adjacent to fluid or halo (which takes the place
+ * of the reference's bounding box) and their neighbour classification.  Replaces
+ * CODE/SRC/build.obs.F90:33-194 as consumed by CODE/SRC/bcond.obs.F90:47-77.
+ * Solid voxels on the outflow plane i = l are rejected (EUP_ERR_UNSUPPORTED):
+ * there the reference's result depends on the iteration order of its
+ * bounce-back loop.  On any failure the previous mask stays installed. */
 int eup_set_obstacles(eup_handle* h, const int32_t* obs);
 
 /* ---- obstacles built on the device ------------------------------------------ */
