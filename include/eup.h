@@ -114,7 +114,8 @@ const char* eup_last_error(const eup_handle* h);
  * CODE/SRC/build.obs.F90:33-194 as consumed by CODE/SRC/bcond.obs.F90:47-77.
  * Solid voxels on the outflow plane i = l are rejected (EUP_ERR_UNSUPPORTED):
  * there the reference's result depends on the iteration order of its
- * bounce-back loop.  On any failure the previous mask stays installed. */
+ * bounce-back loop.  A rejected mask, or one whose buffers cannot be
+ * allocated, leaves the previous mask installed. */
 int eup_set_obstacles(eup_handle* h, const int32_t* obs);
 
 /* ---- obstacles built on the device ------------------------------------------ */
