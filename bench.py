@@ -18,9 +18,18 @@ One JSON line is printed by rank 0:
            + 19 writes of S-byte populations per node) over its mean launch
            time from CUDA events, against the measured HBM copy bandwidth;
   cpu_baseline - the CPU oracle (restatement of the reference's serial step,
-           OpenMP over all host cores) on the same workload.
-`--impl reference` times only the CPU oracle (the reference arm).
-Multi-GPU (torchrun): one independent lattice per GPU (replicas, weak scaling).
+           OpenMP over all host cores) on the same workload;
+  precision_forms - (one GPU) the same workload with populations stored as
+           FP16 and BF16 deviations: step time, MLUPS, ratio to the FP32 line,
+           stream-collide roofline at 76 B/node; and the velocity / C_d error of
+           both against an FP64 run on the 256x128x64 cylinder channel;
+  adjoint - (one GPU) the 192x96x96 partial-bounce-back channel, 4000 steps:
+           checkpointed adjoint time over forward time, FP32 against FP64 gradient.
+`--impl reference` times only the CPU oracle (the reference arm); it builds its
+input (obstacle mask, seeded initial state) with the oracle alone.
+Multi-GPU (torchrun): by default the channel grows with N and is cut into
+x-slabs, one per GPU, with the NCCL plane exchange every step (weak scaling);
+`--decomp replicas` runs one independent lattice per GPU instead.
 """
 from __future__ import annotations
 
@@ -40,6 +49,53 @@ sys.path.insert(0, ROOT)
 
 PRECISIONS = {"fp32": (0, 4, "f32"), "fp64": (1, 8, "f64"), "fp16": (2, 2, "f16-dev/f32"), "bf16": (3, 2, "bf16-dev/f32")}
 
+# The two benchmark workloads as plain numbers.  The eup arm builds them through
+# euplectella_hpc_b200.workloads; the reference arm from these numbers with the oracle
+# alone (a CPU test holds the two descriptions equal, mask and initial state included).
+#   bc: reference face flags (front, rear, right, left, up, down); svisc = u_in * d / re.
+SPECS = {
+    "shell": {"name": "reticular_shell_768x384x384_re2000", "lattice": (768, 384, 384), "bc": (5, 4, 3, 3, 3, 3),
+              "u_in": 0.05, "re": 2000.0, "d": 96.0, "seed": 2024,
+              "body": {"kind": "shell", "x0": 192.0, "length": 256.0, "yc": 192.5, "zc": 192.5, "outer_d": 96.0,
+                       "strut_d": 4.0, "pitch": 16.0, "seed": 2024}},
+    "cylinder": {"name": "cylinder_256x128x64_re100", "lattice": (256, 128, 64), "bc": (5, 4, 3, 3, 0, 0),
+                 "u_in": 0.05, "re": 100.0, "d": 20.0, "seed": 1234,
+                 "body": {"kind": "cylinder_z", "xc": 64.0, "yc": 64.0, "r": 10.0}},
+}
+PERTURBATION = 1e-4
+
+
+def spec_svisc(spec):
+    return spec["u_in"] * spec["d"] / spec["re"]
+
+
+def config_dict(spec, precision, solid_voxels, world=1):
+    """The `config` of the JSON line, the same for both arms."""
+    lx, ly, lz = spec["lattice"]
+    sbytes = PRECISIONS[precision][1]
+    if world > 1:
+        return {"workload": f"{spec['name']} x{world} in series", "lattice": [lx * world, ly, lz],
+                "nodes": lx * ly * lz * world, "precision": precision, "solid_voxels": solid_voxels * world,
+                "bc": list(spec["bc"]), "svisc": spec_svisc(spec), "l2_flush": "inputs larger than L2",
+                "parallelism": f"x-slabs x{world}, NCCL plane exchange every step"}
+    return {"workload": spec["name"], "lattice": [lx, ly, lz], "nodes": lx * ly * lz, "precision": precision,
+            "solid_voxels": solid_voxels, "bc": list(spec["bc"]), "svisc": spec_svisc(spec),
+            "l2_flush": f"inputs larger than L2 (lattice {2 * 19 * sbytes * lx * ly * lz / 1e9:.2f} GB >> 126 MB)"}
+
+
+def reference_input(spec, dtype):
+    """Obstacle mask and seeded initial state of a workload, built by the oracle only."""
+    from oracle import oracle as O
+    lx, ly, lz = spec["lattice"]
+    b = spec["body"]
+    if b["kind"] == "shell":
+        obs = O.voxelise_shell(lx, ly, lz, b["x0"], b["length"], b["yc"], b["zc"], b["outer_d"], b["strut_d"],
+                               b["pitch"], b["seed"])
+    else:
+        obs = O.voxelise_cylinder_z(lx, ly, lz, b["xc"], b["yc"], b["r"])
+    state = O.init_perturbed(lx, ly, lz, spec["u_in"], PERTURBATION, spec["seed"], dtype)
+    return obs, state
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -52,6 +108,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="one GPU: skip the FP16/BF16 and adjoint measurements after the FP32 line")
     ap.add_argument("--decomp", choices=["slabs", "replicas"], default="slabs",
                     help="N > 1: x-slabs of one channel with the plane exchange every step (default), or "
                          "independent replicas")
@@ -153,34 +211,42 @@ def cpu_baseline(wl, state, seconds, prec_name):
 
 
 def run_reference(args):
+    """The reference arm: the CPU oracle (C restatement of the reference's serial step, the
+    Fortran reference having no compiler here) on the host cores, on the eup arm's workload,
+    with its input built by the oracle alone (no GPU library is loaded)."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    wl = make_workload(args.workload, PRECISIONS[args.precision][0])
-    state = wl.initial_state(np.float64 if args.precision == "fp64" else np.float32)
     from oracle import oracle as O
-    c = wl.cfg
-    p = O.params(c.lx, c.ly, c.lz, c.bc, svisc=c.svisc, u0=c.u0, u_inflow=c.u_inflow, u00=c.u00)
+    spec = SPECS[args.workload]
+    dt = np.float64 if args.precision == "fp64" else np.float32
+    obs, state = reference_input(spec, dt)
+    lx, ly, lz = spec["lattice"]
+    nodes = lx * ly * lz
+    p = O.params(lx, ly, lz, spec["bc"], svisc=spec_svisc(spec), u_inflow=spec["u_in"])
     b = np.empty_like(state)
     t0 = time.perf_counter()
-    O.run(p, state, wl.obs, 1, b)  # first warm-up step, also sizes the sample
+    O.run(p, state, obs, 1, b)  # first warm-up step, also sizes the sample
     t1 = time.perf_counter() - t0
     budget = 150.0
     warm = max(0, min(args.warmup - 1, int(0.1 * budget / max(t1, 1e-6))))
-    O.run(p, state, wl.obs, warm, b)
+    O.run(p, state, obs, warm, b)
     steps = int(max(1, min(args.steps, (0.9 * budget) / max(t1, 1e-6))))
     t0 = time.perf_counter()
-    O.run(p, state, wl.obs, steps, b)
+    O.run(p, state, obs, steps, b)
     dt_s = time.perf_counter() - t0
-    v = wl.nodes * steps / dt_s / 1e6
-    sample = (f"{steps} of {args.steps} requested time steps (each the full {wl.nodes}-node lattice), "
-              f"{1 + warm} warm-up; CPU oracle (C restatement of the serial reference step; the Fortran "
-              f"reference has no compiler here), OpenMP {O.nthreads()} threads")
+    v = nodes * steps / dt_s / 1e6
+    what = f"the {nodes}-node lattice" if world == 1 else f"one {lx}x{ly}x{lz} x-slab (with its body) of the {world}-slab channel"
+    sample = (f"{steps} of {args.steps} requested time steps of {what}, {1 + warm} warm-up; CPU oracle "
+              f"(C restatement of the serial reference step; the Fortran reference has no compiler here), "
+              f"{'float' if dt == np.float32 else 'double'}, OpenMP {O.nthreads()} threads; input built by the "
+              f"oracle (no GPU library loaded)")
     line = {"impl": "reference", "metric": "MLUPS", "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
             "steps": steps, "warmup": 1 + warm, "ms_per_step": dt_s * 1e3 / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": PRECISIONS[args.precision][2], "data": "synthetic",
-            "config": {"workload": wl.name, "lattice": [c.lx, c.ly, c.lz], "nodes": wl.nodes},
+            "config": config_dict(spec, args.precision, int(obs.sum()), world),
             "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": O.nthreads(), "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -247,7 +313,6 @@ def run_eup(args):
         t_ms = float(t.item())
     value = world * wl.nodes * args.steps / (t_ms / 1e3) / 1e6
     f_last = solver.forces()
-    cd = solver.cd_series(solver.itime, 1)[0]
 
     # roofline of the dominant kernel (stream-collide)
     k_ms = ms[2] / args.steps
@@ -292,22 +357,138 @@ def run_eup(args):
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         cpu = cpu_baseline(wl, hnp, args.cpu_seconds, args.precision)
 
+    itime = solver.itime
+    solver.close()
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras["precision_forms"] = precision_forms(args, wl, value, t_ms / args.steps, k_ms, local)
+        extras["adjoint"] = adjoint_cost(local)
+
     if rank == 0:
+        config = config_dict(SPECS[args.workload], args.precision, int(wl.obs.sum()))
+        if world > 1:
+            config["workload"] = f"{wl.name} x{world} replicas"
+            config["nodes"] = wl.nodes * world
         line = {"metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": dtype_name, "data": "synthetic",
-                "config": {"workload": wl.name, "lattice": [c.lx, c.ly, c.lz], "nodes": wl.nodes,
-                           "precision": args.precision, "solid_voxels": int(wl.obs.sum()),
-                           "bc": list(c.bc), "svisc": c.svisc, "l2_flush": "inputs larger than L2 (lattice "
-                           f"{2 * 19 * sbytes * wl.nodes / 1e9:.1f} GB >> 126 MB)",
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "vs_baseline": None, "dtype": dtype_name, "data": "synthetic", "config": config,
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
-                "drag": {"fx": f_last[0], "cd": cd, "itime": solver.itime}}
+                # force on the body after the timed steps from an impulsive start: a check that the
+                # state stayed finite, not a drag coefficient of the developed flow
+                "state_check": {"fx_after_timed_steps": f_last[0], "itime": itime}}
+        line.update(extras)
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def _timed_steps(solver, steps, torch):
+    """Device ms of `steps` time steps (CUDA events on the solver's stream) and the stream-collide
+    ms per step from a profiled pass over the same number of steps."""
+    st = torch.cuda.ExternalStream(solver.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    solver.step(steps)
+    e1.record(st)
+    e1.synchronize()
+    ms = solver.step_profiled(steps)
+    return e0.elapsed_time(e1) / steps, ms[2] / steps
+
+
+def precision_forms(args, wl, fp32_mlups, fp32_step_ms, fp32_kernel_ms, device):
+    """FP16 and BF16 deviation storage on the bench workload (same box, same process as the FP32
+    line), and their accuracy against an FP64 run of the same kernel on the 256x128x64 cylinder
+    channel (velocity relative L2 over the fluid after 2000 steps, C_d averaged over the last 500)."""
+    import dataclasses as dc
+
+    import torch
+    import euplectella_hpc_b200 as E
+    from euplectella_hpc_b200 import workloads
+    from euplectella_hpc_b200.studies import velocity
+
+    steps = max(100, min(args.steps, 300))
+    peak, _ = measured_peak()
+    out = {"steps": steps, "warmup": max(args.warmup, 3), "fp32_step_ms": fp32_step_ms,
+           "fp32_stream_collide_ms": fp32_kernel_ms}
+    for name, code in (("fp16", E.FP16_DEV), ("bf16", E.BF16_DEV)):
+        cfg = dc.replace(wl.cfg, precision=code, device=device)
+        with E.Solver(cfg) as s:
+            s.set_obstacles(wl.obs)
+            s.init_state(0.05, 1e-4, wl.seed)
+            s.step_profiled(max(args.warmup, 3))
+            step_ms, k_ms = _timed_steps(s, steps, torch)
+        mlups = wl.nodes / (step_ms / 1e3) / 1e6
+        ach = 2 * 19 * 2 * wl.nodes / (k_ms / 1e3) / 1e9
+        out[name] = {"step_ms": step_ms, "mlups": mlups, "over_fp32_mlups": mlups / fp32_mlups,
+                     "stream_collide_ms": k_ms, "stream_collide_over_fp32": fp32_kernel_ms / k_ms,
+                     "roofline": {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                  "bytes_per_node": 76}}
+    # accuracy on the cylinder channel against FP64
+    cyl = workloads.cylinder_channel()
+    fluid = cyl.obs == 0
+    a0 = cyl.initial_state(np.float64)
+    runs = {}
+    for name, code in (("fp64", E.FP64), ("fp16", E.FP16_DEV), ("bf16", E.BF16_DEV), ("fp32", E.FP32)):
+        with E.Solver(dc.replace(cyl.cfg, precision=code, device=device)) as s:
+            s.set_obstacles(cyl.obs)
+            s.upload(a0)
+            s.step(2000)
+            runs[name] = (velocity(s.download(np.float64))[:, fluid], s.cd_series(1501, 500).mean())
+    u64, cd64 = runs["fp64"]
+    acc = {"workload": cyl.name, "steps": 2000, "cd_window": "steps 1501-2000", "cd_mean_fp64": cd64}
+    for name in ("fp32", "fp16", "bf16"):
+        u, cd = runs[name]
+        acc[name] = {"velocity_rel_l2": float(np.linalg.norm(u - u64) / np.linalg.norm(u64)),
+                     "cd_rel_err": abs(cd - cd64) / abs(cd64)}
+    out["accuracy_vs_fp64"] = acc
+    return out
+
+
+def adjoint_cost(device):
+    """The 192x96x96 partial-bounce-back channel (Re 100, 4000 steps, objective mean C_d over the
+    last 1000): adjoint with recomputation from checkpoints over the forward run, against the
+    partial-bounce-back forward and against the plain halfway-bounce-back FP32 step on the same
+    lattice (body = n_s > 1/2); FP32 against FP64 gradient."""
+    import dataclasses as dc
+
+    import torch
+    import euplectella_hpc_b200 as E
+    from euplectella_hpc_b200 import workloads
+
+    T, A = 4000, 1000
+    out = {"workload": "pbb_cylinder_192x96x96_re100", "steps": T, "avg_steps": A}
+    grads = {}
+    for name, code, dt in (("fp32", E.FP32, np.float32), ("fp64", E.FP64, np.float64)):
+        wl = workloads.pbb_cylinder_channel(steps=T, avg_steps=A, precision=code)
+        cfg = dc.replace(wl.cfg, device=device)
+        a = wl.initial_state(dt)
+        with E.Solver(cfg) as s:
+            s.set_solid_fraction(wl.ns)
+            s.upload(a)
+            fwd_ms = _timed_steps(s, T, torch)[0] * T
+        with E.Solver(cfg) as s:
+            s.set_solid_fraction(wl.ns)
+            s.upload(a)
+            J, g, st = s.adjoint(T, A, 64)
+        grads[name] = g
+        adj_ms = st["forward_ms"] + st["reverse_ms"]
+        row = {"objective": J, "pbb_forward_ms": fwd_ms, "adjoint_ms": adj_ms,
+               "adjoint_forward_sweep_ms": st["forward_ms"], "adjoint_reverse_ms": st["reverse_ms"],
+               "adjoint_over_pbb_forward": adj_ms / fwd_ms, "recomputed_steps": st["recomputed_steps"],
+               "stored_states": st["checkpoints"], "stored_state_bytes": st["state_bytes"]}
+        if name == "fp32":
+            with E.Solver(cfg) as s:
+                s.set_obstacles((wl.ns > 0.5).astype(np.int32))
+                s.upload(a)
+                plain_ms = _timed_steps(s, T, torch)[0] * T
+            row["plain_forward_ms"] = plain_ms
+            row["adjoint_over_plain_forward"] = adj_ms / plain_ms
+        out[name] = row
+    out["grad_fp32_vs_fp64_rel_l2"] = float(np.linalg.norm(grads["fp32"] - grads["fp64"]) /
+                                            np.linalg.norm(grads["fp64"]))
+    return out
 
 
 def run_slabs(args):
@@ -398,20 +579,17 @@ def run_slabs(args):
                        "all-reduced force) + eup_download"}
     f = slab.forces()
     if rank == 0:
-        c = wl.cfg
         line = {"metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": dtype_name, "data": "synthetic",
-                "config": {"workload": f"{wl.name} x{world} in series", "lattice": [c.lx * world, c.ly, c.lz],
-                           "nodes": nodes * world, "precision": args.precision, "bc": list(gcfg.bc),
-                           "svisc": c.svisc, "l2_flush": "inputs larger than L2",
-                           "parallelism": f"x-slabs x{world}, NCCL plane exchange every step"},
+                "config": config_dict(SPECS[args.workload], args.precision, int(wl.obs.sum()), world),
+                "parallelism": f"x-slabs x{world}, NCCL plane exchange every step",
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": (tpn * nodes if tpn is not None else None),
                              "kernel": "k_stream_collide_pair (+ plane unpack and force of the step)",
                              "kernel_ms": k_ms, "peak_source": peak_src},
                 "e2e": e2e, "cpu_baseline": None, "clocks": clk, "gpu_launches": launches,
-                "drag": {"fx": float(f[0]), "itime": s.itime}}
+                "state_check": {"fx_after_timed_steps": float(f[0]), "itime": s.itime}}
         print(json.dumps(line), flush=True)
     s.close()
     dist.barrier()

@@ -39,6 +39,7 @@ struct eup_handle {
     double* series = nullptr;
     int64_t cap = 0;
     double* dscratch = nullptr;  // 64 doubles
+    unsigned int* d_bad = nullptr;  // upload check: bit q set when population q had a non-finite value
     void* staging = nullptr;
     size_t staging_bytes = 0;
     int64_t itime = 0, series_first = 0;
@@ -293,7 +294,8 @@ void fill_xface_dispatch(eup_handle* h) {
 
 template <typename S, typename R, typename T>
 void enqueue_upload_q(eup_handle* h, int q) {
-    launch_scatter<S, R, T>(make_lat<S, R>(h, h->cur), h->g, q, static_cast<const T*>(h->staging), h->stream);
+    launch_scatter<S, R, T>(make_lat<S, R>(h, h->cur), h->g, q, static_cast<const T*>(h->staging), h->d_bad,
+                            h->stream);
 }
 template <typename S, typename R, typename T>
 void enqueue_download_q(eup_handle* h, int q) {
@@ -362,6 +364,27 @@ int ensure_staging(eup_handle* h, size_t bytes) {
     CK(h, cudaMalloc(&h->staging, bytes));
     h->staging_bytes = bytes;
     return EUP_OK;
+}
+
+// Start / end of a state transfer into the device: the scatter sets bit q of d_bad for a
+// population that held a value that is not finite.  A rejected state leaves the handle
+// without a state (the lattice holds part of it).
+int begin_upload_check(eup_handle* h) {
+    CK(h, cudaMemsetAsync(h->d_bad, 0, sizeof(unsigned int), h->stream));
+    return EUP_OK;
+}
+int end_upload_check(eup_handle* h, const char* who) {
+    unsigned int bad = 0;
+    CK(h, cudaMemcpyAsync(&bad, h->d_bad, sizeof(bad), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (bad == 0) return EUP_OK;
+    h->has_state = false;
+    std::string qs;
+    for (int q = 0; q < Q; ++q)
+        if (bad & (1u << q)) qs += (qs.empty() ? "" : ",") + std::to_string(q + 1);
+    return fail(h, EUP_ERR_INVALID_ARG,
+                std::string(who) + ": non-finite value (NaN or Inf) in population(s) a" + qs +
+                    "; the state was rejected and the handle holds no state");
 }
 
 bool has_exchange_face(const eup_handle* h) {
@@ -458,6 +481,8 @@ int eup_create(const eup_config* cfg, eup_handle** out) {
     cudaMemsetAsync(h->series, 0, sizeof(double) * 3 * h->cap, h->stream);
     if ((e = cudaMalloc(&h->dscratch, sizeof(double) * 64)) != cudaSuccess)
         return cleanup_fail(cuda_fail(h, e, "cudaMalloc(scratch)"));
+    if ((e = cudaMalloc(&h->d_bad, sizeof(unsigned int))) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMalloc(upload check)"));
     const size_t xface_bytes = (size_t)2 * 18 * h->g.m * h->g.n * h->rbytes;
     if ((e = cudaMalloc(&h->xface, xface_bytes)) != cudaSuccess)
         return cleanup_fail(cuda_fail(h, e, "cudaMalloc(x-face copy)"));
@@ -476,7 +501,7 @@ int eup_destroy(eup_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
     void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->blinks, h->partials, h->counter,
-                    h->series, h->dscratch, h->staging, h->xface, h->d_itime, h->ns};
+                    h->series, h->dscratch, h->staging, h->xface, h->d_itime, h->ns, h->d_bad};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -699,10 +724,12 @@ int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, in
     const Geo& g = h->g;
     const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * elem_bytes;
     if ((rc = ensure_staging(h, bytes))) return rc;
+    if ((rc = begin_upload_check(h))) return rc;
     for (int q = 0; q < Q; ++q) {
         CK(h, cudaMemcpyAsync(h->staging, pops[q], bytes, cudaMemcpyHostToDevice, h->stream));
         DISPATCH(h, upload_q, h, q, elem_bytes);
     }
+    if ((rc = end_upload_check(h, "eup_upload"))) return rc;
     return finish_state(h, itime);
 }
 
@@ -714,11 +741,13 @@ int eup_init_state(eup_handle* h, double u_in, double amp, uint64_t seed, int64_
     const int eb = (h->prec == EUP_FP64) ? 8 : 4;  // what eup_init_equilibrium would hand to eup_upload
     const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * eb;
     if ((rc = ensure_staging(h, bytes))) return rc;
+    if ((rc = begin_upload_check(h))) return rc;
     for (int q = 0; q < Q; ++q) {
         if (eb == 8) launch_init_population<double>(static_cast<double*>(h->staging), g, q, u_in, amp, seed, h->stream);
         else launch_init_population<float>(static_cast<float*>(h->staging), g, q, u_in, amp, seed, h->stream);
         DISPATCH(h, upload_q, h, q, eb);
     }
+    if ((rc = end_upload_check(h, "eup_init_state"))) return rc;
     return finish_state(h, itime);
 }
 
@@ -768,10 +797,10 @@ int eup_restore_state(eup_handle* h, const char* path, int32_t elem_bytes) {
         std::fclose(f);
         return cuda_fail(h, e, "cudaMallocHost");
     }
-    int out = EUP_OK;
+    int out = begin_upload_check(h);
     int32_t it = 0;
     std::string why;
-    if (!eup_internal_read_record(f, &it, 4, &why)) out = fail(h, EUP_ERR_IO, "eup_restore_state: itime: " + why);
+    if (out == EUP_OK && !eup_internal_read_record(f, &it, 4, &why)) out = fail(h, EUP_ERR_IO, "eup_restore_state: itime: " + why);
     for (int q = 0; q < Q && out == EUP_OK; ++q) {
         if (!eup_internal_read_record(f, pinned, (int64_t)bytes, &why)) {
             out = fail(h, EUP_ERR_IO, "eup_restore_state: population " + std::to_string(q + 1) + ": " + why);
@@ -787,6 +816,7 @@ int eup_restore_state(eup_handle* h, const char* path, int32_t elem_bytes) {
     std::fclose(f);
     cudaFreeHost(pinned);
     if (out != EUP_OK) return out;
+    if ((out = end_upload_check(h, "eup_restore_state"))) return out;
     return finish_state(h, it);
 }
 
@@ -972,6 +1002,11 @@ int eup_get_force_series(eup_handle* h, int64_t first_step, int32_t count, doubl
         CK(h, cudaMemcpy(fxyz + 3 * (int64_t)c, h->series + 3 * pos, sizeof(double) * 3 * run, cudaMemcpyDeviceToHost));
         c += run;
     }
+    for (int64_t t = 0; t < 3 * (int64_t)count; ++t)
+        if (!std::isfinite(fxyz[t]))
+            return fail(h, EUP_ERR_DIVERGED,
+                        "eup_get_force_series: non-finite FP64 force at step " + std::to_string(first_step + t / 3) +
+                            " (run diverged)");
     return EUP_OK;
 }
 

@@ -160,9 +160,10 @@ template <typename S, typename R>
 void launch_probes(const Lat<S, R>& L, const Geo& g, int npts, const int32_t* ijk, double* out,
                    cudaStream_t st);
 
-// Scatter one haloed host-layout array (T) into lattice population q + shell.
+// Scatter one haloed host-layout array (T) into lattice population q + shell; a
+// value that is not finite sets bit q of *bad (device pointer).
 template <typename S, typename R, typename T>
-void launch_scatter(const Lat<S, R>& L, const Geo& g, int q, const T* staging, cudaStream_t st);
+void launch_scatter(const Lat<S, R>& L, const Geo& g, int q, const T* staging, unsigned int* bad, cudaStream_t st);
 template <typename S, typename R, typename T>
 void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStream_t st);
 

@@ -606,14 +606,16 @@ __global__ void k_probes(Lat<S, R> L, Geo g, int npts, const int32_t* ijk, doubl
 // Host values (T = float or double) into the lattice and the halo shell.  16-bit storage
 // from double converts in double: f = w + D/scale is exact there, so a state downloaded as
 // double and uploaded again keeps every bit of D (through float, deviations below 2^-6
-// lose their low bits to the rounding of f).
+// lose their low bits to the rounding of f).  A host value that is not finite sets bit q
+// of *bad (the caller rejects the state).
 template <typename S, typename R, typename T>
-__global__ void k_scatter(Lat<S, R> L, Geo g, int q, const T* src, int64_t total) {
+__global__ void k_scatter(Lat<S, R> L, Geo g, int q, const T* src, int64_t total, unsigned int* bad) {
     constexpr bool exact16 = DevStore<S>::value && sizeof(T) == 8;
     const int64_t L2 = g.l + 2, M2 = g.m + 2;
     for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(idx % L2), j = (int)((idx / L2) % M2), k = (int)(idx / (L2 * M2));
+        if (!isfinite(src[idx])) atomicOr(bad, 1u << q);
         const R v = (R)src[idx];
         if (g.interior(i, j, k)) {
             if constexpr (exact16)
@@ -833,9 +835,9 @@ void launch_probes(const Lat<S, R>& L, const Geo& g, int npts, const int32_t* ij
 }
 
 template <typename S, typename R, typename T>
-void launch_scatter(const Lat<S, R>& L, const Geo& g, int q, const T* staging, cudaStream_t st) {
+void launch_scatter(const Lat<S, R>& L, const Geo& g, int q, const T* staging, unsigned int* bad, cudaStream_t st) {
     const int64_t total = (int64_t)(g.l + 2) * (g.m + 2) * (g.n + 2);
-    k_scatter<S, R, T><<<grid_for(total, kTpb), kTpb, 0, st>>>(L, g, q, staging, total);
+    k_scatter<S, R, T><<<grid_for(total, kTpb), kTpb, 0, st>>>(L, g, q, staging, total, bad);
 }
 
 template <typename S, typename R, typename T>
@@ -863,9 +865,9 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
     template void launch_probes<S, R>(const Lat<S, R>&, const Geo&, int, const int32_t*, double*,      \
                                       cudaStream_t);                                                   \
     template void launch_scatter<S, R, float>(const Lat<S, R>&, const Geo&, int, const float*,         \
-                                              cudaStream_t);                                           \
+                                              unsigned int*, cudaStream_t);                            \
     template void launch_scatter<S, R, double>(const Lat<S, R>&, const Geo&, int, const double*,       \
-                                               cudaStream_t);                                          \
+                                               unsigned int*, cudaStream_t);                           \
     template void launch_gather<S, R, float>(const Lat<S, R>&, const Geo&, int, float*, cudaStream_t); \
     template void launch_gather<S, R, double>(const Lat<S, R>&, const Geo&, int, double*, cudaStream_t);
 

@@ -9,10 +9,13 @@
 // stall every stream on the device.  This
 // entry point reads the caller's device arrays in the reference's haloed
 // layout and writes the force to the caller's device memory; its only scratch
-// is the file-scope array below, fixed in size at load time.
+// is the file-scope array below, of fixed size.  The CUDA runtime loads the
+// library's device code lazily (CUDA_MODULE_LOADING=LAZY is the default), so
+// the array is created on a device by the first call there: a caller with a
+// fixed device-memory budget makes one call (any small lattice) before its own
+// allocator takes that budget.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/eup.h"
@@ -23,8 +26,8 @@ void eup_internal_set_error(const std::string& msg);
 namespace {
 
 // One FP64 partial force per z-plane plus the completion counter.  Every GPU
-// that loads the library holds this array (about 96 KiB) until the process
-// exits.  All calls share it, so calls that overlap on the GPU (different
+// on which the entry point has been called holds this array (about 96 KiB)
+// until the process exits.  All calls share it, so calls that overlap on the GPU (different
 // streams, or different host threads on one device) race on it.
 constexpr int kNoAllocMaxPlanes = 4096;
 struct NoAllocScratch {
@@ -39,25 +42,15 @@ struct Pops19 {
     const T* p[19];
 };
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-NoAllocScratch* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch on the current device, looked up once per
-// device.  In host code the symbol is only a host-side stand-in.
+// Device address of the scratch on the current device.  In host code the
+// symbol is only a host-side stand-in; the address is looked up on every call
+// (cheap next to the launch), so it stays right after a device reset or a
+// runtime shutdown and re-initialisation reloads the module elsewhere.
 cudaError_t scratch_for_current_device(NoAllocScratch** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = static_cast<NoAllocScratch*>(p);
-    }
-    *out = g_scratch_addr[dev];
+    *out = static_cast<NoAllocScratch*>(p);
     return cudaSuccess;
 }
 

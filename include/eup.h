@@ -182,7 +182,10 @@ int eup_write_obstacles(eup_handle* h, const char* path);
  * interior nodes into the lattice (converted to the storage precision), halo
  * nodes into the persistent halo shell.  Replaces the host-to-device copy of
  * CODE/SRC/bgk3d.F90:113 / CODE/SRC/initialize.F90:164-175; also the
- * restart path (CODE/SRC/restore_raw.F90:43-63).  Sets the step counter. */
+ * restart path (CODE/SRC/restore_raw.F90:43-63).  Sets the step counter.
+ * A value that is not finite (NaN, Inf) anywhere in the 19 arrays is
+ * EUP_ERR_INVALID_ARG naming the populations; the handle then holds no state
+ * (eup_restore_state and eup_init_state check the same way). */
 int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, int64_t itime);
 
 /* The seeded equilibrium state of eup_init_equilibrium generated on the
@@ -248,7 +251,9 @@ int eup_get_itime(eup_handle* h, int64_t* itime);
 /* Momentum-exchange force on the solid for the current state, FP64:
  * F = sum over fluid nodes x and directions q with solid neighbour x + c_q
  * (wrapped across periodic axes) of 2 c_q f_q(x), post-collision.  No
- * reference counterpart (the reference's drag is CODE/SRC/drag.F90:33-79). */
+ * reference counterpart (the reference's drag is CODE/SRC/drag.F90:33-79).
+ * EUP_ERR_DIVERGED when a component is not finite (the values are still
+ * written), the same for eup_get_force_series and eup_get_cd_series. */
 int eup_get_forces(eup_handle* h, double fxyz[3]);
 
 /* Force history: entries for steps first_step .. first_step+count-1 (step t =
@@ -325,9 +330,13 @@ int eup_get_boundary_solid(eup_handle* h, int64_t* list, int64_t cap, int64_t* c
  *   bc[6]     reference face flags (axes with both faces periodic wrap);
  *   force     device pointer receiving 3 doubles;
  *   stream    cudaStream_t to run on (NULL: the legacy default stream).
- * Asynchronous on `stream`.  The first call on each device looks up the
- * scratch address (cudaGetSymbolAddress); make it before any stream capture.
- * All calls share the scratch: calls that overlap on the GPU race. */
+ * Asynchronous on `stream`.  Every call looks up the scratch address on the
+ * current device (cudaGetSymbolAddress), so it stays valid across a device
+ * reset.  The CUDA runtime loads device code lazily by default, so the
+ * scratch comes into being on a device at the first call there: a caller with
+ * a fixed device-memory budget makes one call before its allocator takes the
+ * budget, and makes that first call before any stream capture.  All calls
+ * share the scratch: calls that overlap on the GPU race. */
 int eup_mem_force_noalloc(int32_t l, int32_t m, int32_t n, const int32_t bc[6], const void* const pops[19],
                           int32_t elem_bytes, const int32_t* obs, double* force, void* stream);
 

@@ -79,6 +79,11 @@ def lib():
         L.orc_links.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p]
         L.orc_boundary_solid.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p]
         L.orc_boundary_solid.restype = ctypes.c_int64
+        dbl = ctypes.c_double
+        L.orc_voxelise_shell.argtypes = [ctypes.c_int32] * 3 + [dbl] * 7 + [ctypes.c_uint64, ctypes.c_void_p]
+        L.orc_voxelise_shell.restype = ctypes.c_int64
+        L.orc_voxelise_cylinder_z.argtypes = [ctypes.c_int32] * 3 + [dbl] * 3 + [ctypes.c_void_p]
+        L.orc_voxelise_cylinder_z.restype = ctypes.c_int64
         L.orc_splitmix64.argtypes = [ctypes.c_uint64]
         L.orc_splitmix64.restype = ctypes.c_uint64
         L.orc_nthreads.restype = ctypes.c_int32
@@ -226,6 +231,21 @@ def boundary_solid(p, obs) -> np.ndarray:
     out = np.zeros(max(cnt, 1), dtype=np.int64)
     lib().orc_boundary_solid(ctypes.byref(p), _obs_ptr(obs), out.ctypes.data)
     return out[:cnt]
+
+
+def voxelise_shell(l, m, n, x0, length, yc, zc, outer_d, strut_d, pitch, seed) -> np.ndarray:
+    """The reticular shell of the benchmark workloads as obs (n, m, l) (oracle/orc_geom.c)."""
+    obs = np.empty((n, m, l), dtype=np.int32)
+    lib().orc_voxelise_shell(l, m, n, float(x0), float(length), float(yc), float(zc), float(outer_d),
+                             float(strut_d), float(pitch), int(seed), obs.ctypes.data)
+    return obs
+
+
+def voxelise_cylinder_z(l, m, n, xc, yc, r) -> np.ndarray:
+    """Solid circular cylinder along z, (i - xc)^2 + (j - yc)^2 <= r^2, as obs (n, m, l)."""
+    obs = np.empty((n, m, l), dtype=np.int32)
+    lib().orc_voxelise_cylinder_z(l, m, n, float(xc), float(yc), float(r), obs.ctypes.data)
+    return obs
 
 
 def nthreads() -> int:

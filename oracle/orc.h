@@ -73,6 +73,12 @@ typedef struct orc_params {
 ORC_DECLARE(f, float)
 ORC_DECLARE(d, double)
 
+/* The synthetic bodies of the benchmark workloads (orc_geom.c): obs (n, m, l),
+ * 1 = solid, bit-identical to the product's voxelisers; return the solid count. */
+int64_t orc_voxelise_shell(int32_t l, int32_t m, int32_t n, double x0, double length, double yc, double zc,
+                           double outer_d, double strut_d, double pitch, uint64_t seed, int32_t* obs);
+int64_t orc_voxelise_cylinder_z(int32_t l, int32_t m, int32_t n, double xc, double yc, double r, int32_t* obs);
+
 /* Precision-independent helpers. */
 void orc_links(const orc_params* p, const int32_t* obs, uint32_t* links);
 int64_t orc_boundary_solid(const orc_params* p, const int32_t* obs, int64_t* list);

@@ -52,6 +52,36 @@ def test_noalloc_force_matches_handle(eup, require_gpu, prec):
     del pops
 
 
+def test_noalloc_on_a_caller_stream(eup, require_gpu):
+    """The counter reset and the kernel run in order on a non-default stream of the caller."""
+    import torch
+
+    l, m, n = 64, 24, 10
+    bc = (eup.OUTFLOW, eup.INFLOW, eup.FREESLIP, eup.FREESLIP, eup.PERIODIC, eup.PERIODIC)
+    obs = eup.geometry_cylinder_z(l, m, n, 20, 12.5, 5)
+    cfg = eup.Config(l, m, n, bc=bc, svisc=0.01, u_inflow=0.05)
+    with eup.Solver(cfg) as s:
+        s.set_obstacles(obs)
+        s.upload(eup.init_equilibrium(l, m, n, 0.05, 1e-3, 12, np.float32))
+        s.step(20)
+        f_ref = s.forces()
+        state = s.download(np.float32)
+    dev = torch.device("cuda", 0)
+    side = torch.cuda.Stream(dev)
+    with torch.cuda.stream(side):
+        pops = torch.from_numpy(state).to(dev)
+        d_obs = torch.from_numpy(obs).to(dev)
+        out = torch.full((3,), float("nan"), dtype=torch.float64, device=dev)
+        ptrs = [pops[q].data_ptr() for q in range(19)]
+        for _ in range(2):
+            out.fill_(float("nan"))
+            rc = _call(eup, l, m, n, bc, ptrs, 4, d_obs.data_ptr(), out.data_ptr(), side.cuda_stream)
+            assert rc == 0, eup.lib.eup_last_error(None)
+            got = out.cpu().numpy()  # ordered after the kernel on the same stream
+            np.testing.assert_allclose(got, f_ref, rtol=1e-12, atol=1e-14)
+    side.synchronize()
+
+
 def test_noalloc_rejects_oversized_lattice(eup):
     dummy = [1] * 19
     rc = _call(eup, 8, 8, 4097, (0,) * 6, dummy, 4, 1, 1, None)
