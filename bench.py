@@ -477,7 +477,8 @@ def adjoint_cost(device):
         row = {"objective": J, "pbb_forward_ms": fwd_ms, "adjoint_ms": adj_ms,
                "adjoint_forward_sweep_ms": st["forward_ms"], "adjoint_reverse_ms": st["reverse_ms"],
                "adjoint_over_pbb_forward": adj_ms / fwd_ms, "recomputed_steps": st["recomputed_steps"],
-               "stored_states": st["checkpoints"], "stored_state_bytes": st["state_bytes"]}
+               "stored_states": st["checkpoints"], "repetitions": st["repetitions"],
+               "stored_state_bytes": st["state_bytes"]}
         if name == "fp32":
             with E.Solver(cfg) as s:
                 s.set_obstacles((wl.ns > 0.5).astype(np.int32))

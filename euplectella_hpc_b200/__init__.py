@@ -459,7 +459,7 @@ class Solver:
         grad = np.zeros((self.cfg.lz, self.cfg.ly, self.cfg.lx), dtype=np.float64)
         st = np.zeros(8, dtype=np.float64)
         self._ck(lib.eup_adjoint_run(self._h, ctypes.byref(cfg), ctypes.byref(obj), grad.ctypes.data, st.ctypes.data))
-        keys = ["forward_ms", "reverse_ms", "recomputed_steps", "checkpoints", "segment_steps", "state_bytes",
+        keys = ["forward_ms", "reverse_ms", "recomputed_steps", "checkpoints", "repetitions", "state_bytes",
                 "nsteps", "avg_steps"]
         return obj.value, grad, dict(zip(keys, st.tolist()))
 

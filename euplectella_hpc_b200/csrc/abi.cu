@@ -48,6 +48,8 @@ struct eup_handle {
     int variant = 0;  // EUP_STEP_VARIANT: bit 0/2 16/8-byte vector stream-collide, bit 1 no CUDA graphs
     bool pbb = false;             // partial-bounce-back model active (solid fraction set)
     void* ns = nullptr;           // solid fraction n_s per interior node, arithmetic type
+    int32_t* ns_list = nullptr;   // interior linear indices with n_s > 0, ascending
+    int64_t ns_count = 0;
     int64_t launches = 0;  // kernels launched by eup_step / eup_step_profiled
     bool mid_step = false;  // eup_step_boundaries done, eup_step_stream pending
     bool interior_done = false;  // eup_step_stream_interior done, eup_step_stream_faces pending
@@ -159,7 +161,8 @@ int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
             if (pe) pe->mark(4 * s + 1, h->stream);
             n += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
             if (pe) pe->mark(4 * s + 2, h->stream);
-            launch_pbb_step<R>(src, dst, h->g, ph, static_cast<const R*>(h->ns), make_reduce(h), h->series, h->cap,
+            launch_pbb_step<R>(src, dst, h->g, ph, static_cast<const R*>(h->ns), h->ns_list, h->ns_count,
+                               make_reduce(h), h->series, h->cap,
                                h->d_itime, h->stream);
             if (pe) pe->mark(4 * s + 3, h->stream);
             return n + 1;
@@ -391,6 +394,19 @@ bool has_exchange_face(const eup_handle* h) {
     return h->cfg.bc[EUP_FRONT] == EUP_BC_EXCHANGE || h->cfg.bc[EUP_REAR] == EUP_BC_EXCHANGE;
 }
 
+// After a synchronisation: a bounded wait of the staged stream-collide kernel that ran out
+// left a step incomplete.
+int check_kernel_waits(eup_handle* h, const char* who) {
+    unsigned int n = 0;
+    CK(h, staged_wait_timeouts(&n));
+    if (n != 0)
+        return fail(h, EUP_ERR_CUDA,
+                    std::string(who) + ": " + std::to_string(n) +
+                        " bulk copies of the staged stream-collide kernel did not complete within 2 s; "
+                        "the steps since are incomplete");
+    return EUP_OK;
+}
+
 int check_handle(eup_handle* h) {
     if (!h) return fail(nullptr, EUP_ERR_INVALID_ARG, "null handle");
     cudaError_t e = cudaSetDevice(h->cfg.device);
@@ -460,6 +476,8 @@ int eup_create(const eup_config* cfg, eup_handle** out) {
     };
     cudaError_t e = cudaSetDevice(cfg->device);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(h, e, "cudaSetDevice"));
+    if ((e = prepare_stream_collide()) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "stream-collide kernel attributes"));
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return cleanup_fail(cuda_fail(h, e, "cudaStreamCreate"));
     const size_t lat_bytes = (size_t)Q * h->Nq * h->sbytes;
@@ -501,7 +519,7 @@ int eup_destroy(eup_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
     void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->blinks, h->partials, h->counter,
-                    h->series, h->dscratch, h->staging, h->xface, h->d_itime, h->ns, h->d_bad};
+                    h->series, h->dscratch, h->staging, h->xface, h->d_itime, h->ns, h->d_bad, h->ns_list};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -960,7 +978,7 @@ int eup_synchronize(eup_handle* h) {
     int rc = check_handle(h);
     if (rc) return rc;
     CK(h, cudaStreamSynchronize(h->stream));
-    return EUP_OK;
+    return check_kernel_waits(h, "eup_synchronize");
 }
 
 int eup_get_launch_count(eup_handle* h, int64_t* launches) {
@@ -995,6 +1013,7 @@ int eup_get_force_series(eup_handle* h, int64_t first_step, int32_t count, doubl
                         std::to_string(first_step + count - 1) + " outside the recorded range " +
                         std::to_string(lo) + ".." + std::to_string(h->itime));
     CK(h, cudaStreamSynchronize(h->stream));
+    if ((rc = check_kernel_waits(h, "eup_get_force_series"))) return rc;
     for (int32_t c = 0; c < count;) {
         const int64_t t = first_step + c;
         const int64_t pos = t % h->cap;
@@ -1203,17 +1222,101 @@ Lat<R, R> lat_at(const eup_handle* h, R* base, R* shell = nullptr) {
     return L;
 }
 
-// Forward sweep with checkpoints, reverse sweep recomputing each segment once.
-// Schedule: K = ceil(T / slots) steps per segment, ceil(T / K) checkpoints
-// (states 0, K, 2K, ...) plus a K-state segment buffer: every forward step is
-// recomputed at most once (binomial checkpointing at repetition number 2).
+// ---- binomial checkpointing ---------------------------------------------------------
+// Reversing n steps from a stored state with c snapshot slots (the stored state's own
+// included) needs at least t(n, c) = r n - C(c + r, r - 1) forward steps, r the smallest
+// repetition number with C(c + r, c) >= n (t = 0 for n <= 1, n(n-1)/2 for c = 1):
+// A. Griewank, "Achieving logarithmic growth of temporal and spatial complexity in reverse
+// automatic differentiation", Optim. Methods Softw. 1 (1992); A. Griewank and A. Walther,
+// ACM TOMS 26 (2000), "revolve".  The schedule below splits each range at the step that
+// minimises m + t(m, c) + t(n - m, c - 1) (scanned with the closed form), which attains
+// t(n, c).
+
+// C(a, b), saturating far above any step count
+int64_t binom_sat(int64_t a, int64_t b) {
+    if (b < 0 || b > a) return 0;
+    if (b > a - b) b = a - b;
+    const int64_t cap = (int64_t)1 << 50;
+    int64_t v = 1;
+    for (int64_t i = 1; i <= b; ++i) {
+        v = v * (a - b + i) / i;  // exact: the product of i consecutive integers divides by i!
+        if (v > cap) return cap;
+    }
+    return v;
+}
+
+int64_t revolve_cost(int64_t n, int64_t c) {
+    if (n <= 1) return 0;
+    if (c <= 1) return n * (n - 1) / 2;
+    int64_t r = 0;
+    while (binom_sat(c + r, c) < n) ++r;
+    return r * n - binom_sat(c + r, r - 1);
+}
+
+// smallest r with C(c + r, c) >= n
+int revolve_repetition(int64_t n, int64_t c) {
+    if (n <= 1) return 0;
+    if (c <= 1) return (int)(n - 1);
+    int r = 0;
+    while (binom_sat(c + r, c) < n) ++r;
+    return r;
+}
+
+enum : int { kActAdvance = 0, kActSnapshot = 1, kActRestore = 2, kActAdjoint = 3 };
+struct RevAct {
+    int kind, arg;  // advance: steps; snapshot/restore: slot; adjoint: the step t reversed (from state t-1)
+};
+
+// Reverse steps a+1 .. b with the working state at a (also held in slot_a) and `free` slots.
+void revolve_schedule(int a, int b, int slot_a, std::vector<int>& free, std::vector<RevAct>& acts) {
+    const int n = b - a;
+    if (n == 1) {
+        acts.push_back({kActAdjoint, b});
+        return;
+    }
+    if (free.empty()) {  // no slot left: recompute from a for every step
+        for (int t = b; t > a; --t) {
+            if (t != b) acts.push_back({kActRestore, slot_a});
+            if (t - 1 - a > 0) acts.push_back({kActAdvance, t - 1 - a});
+            acts.push_back({kActAdjoint, t});
+        }
+        return;
+    }
+    const int64_t c = (int64_t)free.size() + 1;
+    int best_m = 1;
+    int64_t best = -1;
+    for (int m = 1; m < n; ++m) {
+        const int64_t v = m + revolve_cost(m, c) + revolve_cost(n - m, c - 1);
+        if (best < 0 || v < best) {
+            best = v;
+            best_m = m;
+        }
+    }
+    const int k = free.back();
+    free.pop_back();
+    acts.push_back({kActAdvance, best_m});
+    acts.push_back({kActSnapshot, k});
+    revolve_schedule(a + best_m, b, k, free, acts);
+    free.push_back(k);
+    acts.push_back({kActRestore, slot_a});
+    revolve_schedule(a, a + best_m, slot_a, free, acts);
+}
+
+// T partial-bounce-back steps forward, then the adjoint back, with `slots` stored states
+// (binomial checkpointing).  The plain forward sweep on the handle's own lattices records
+// every step's force and, as it passes them, copies the states the schedule stores on its
+// first descent (state 0 included) into their slots and state T-1 into the working
+// buffer; the rest of the schedule then runs on two working buffers: restores, forward
+// steps without force, stores, and adjoint steps in the order T, T-1, ..., 1.  Before each
+// forward or adjoint step the halo blocks run on the working state (its halo follows from
+// it: configurations whose halo holds older values are refused), writing a working halo
+// shell that starts as a copy of the handle's (its never-written slots are constant).
 template <typename R>
 int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, double* grad_out, double* stats) {
     const Geo& g = h->g;
     const int T = ac->nsteps, A = ac->avg_steps;
-    const int slots = ac->checkpoints > 0 ? ac->checkpoints : 64;
-    const int K = (T + slots - 1) / slots;
-    const int nseg = (T + K - 1) / K;
+    int slots = ac->checkpoints > 0 ? ac->checkpoints : 64;
+    if (slots > T) slots = T;
     const int bc[6] = {h->cfg.bc[0], h->cfg.bc[1], h->cfg.bc[2], h->cfg.bc[3], h->cfg.bc[4], h->cfg.bc[5]};
     const double norm = 0.5 * h->cfg.cd_rho0 * h->cfg.cd_uref * h->cfg.cd_uref * h->cfg.cd_length * h->cfg.cd_span;
     const double gamma = 1.0 / ((double)A * norm);
@@ -1239,23 +1342,38 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     td.out_jk = d_ojk.p; td.out_start = d_ostart.p; td.out_slot = d_oslot.p; td.out_q = d_oq.p;
     td.nout = (int64_t)tab.out_jk.size();
 
+    // the schedule, and the states its first descent stores
+    std::vector<RevAct> acts;
+    {
+        std::vector<int> free;
+        for (int k = slots - 1; k >= 1; --k) free.push_back(k);
+        acts.push_back({kActSnapshot, 0});
+        revolve_schedule(0, T, 0, free, acts);
+    }
+    std::vector<int> store_at((size_t)T, -1);  // forward-sweep state -> slot
+    size_t first_adj = 0;
+    {
+        int state = 0;
+        for (; first_adj < acts.size() && acts[first_adj].kind != kActAdjoint; ++first_adj) {
+            if (acts[first_adj].kind == kActAdvance) state += acts[first_adj].arg;
+            else if (acts[first_adj].kind == kActSnapshot) store_at[(size_t)state] = acts[first_adj].arg;
+        }
+        if (state != T - 1) return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: internal schedule error");
+    }
+
     const size_t state = (size_t)Q * h->Nq;
     const size_t shell = (size_t)Q * g.G;
-    DevBuf<R> ckpt, seg, seg_shell, lam, gmu, shell_save;
-    DevBuf<double> grad, scratch_series;
-    DevBuf<int64_t> scratch_itime;
-    CK(h, ckpt.alloc(state * nseg));
-    CK(h, seg.alloc(state * K));
-    CK(h, seg_shell.alloc(shell * K));
+    DevBuf<R> snap, work, lam, gmu, wshell;
+    DevBuf<double> grad;
+    CK(h, snap.alloc(state * slots));
+    CK(h, work.alloc(state * 2));
     CK(h, lam.alloc(state * 2));
-    CK(h, gmu.alloc((size_t)Q * g.G));
-    CK(h, shell_save.alloc((size_t)Q * g.G));
+    CK(h, gmu.alloc(shell));
+    CK(h, wshell.alloc(shell));
     CK(h, grad.alloc(g.N));
-    CK(h, scratch_series.alloc(3 * 2));
-    CK(h, scratch_itime.alloc(1));
     CK(h, cudaMemsetAsync(grad.p, 0, sizeof(double) * g.N, st));
     CK(h, cudaMemsetAsync(lam.p, 0, sizeof(R) * state * 2, st));
-    CK(h, cudaMemsetAsync(scratch_itime.p, 0, sizeof(int64_t), st));
+    CK(h, cudaMemsetAsync(work.p, 0, sizeof(R) * state * 2, st));
     const Reduce red = make_reduce(h);
 
     cudaEvent_t ev[3];
@@ -1264,15 +1382,18 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     const int64_t t0 = h->itime;
     CK(h, cudaEventRecord(ev[0], st));
     for (int s = 0; s < T; ++s) {
-        if (s % K == 0)
-            CK(h, cudaMemcpyAsync(ckpt.p + state * (s / K), h->lat[h->cur], sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
+        if (store_at[(size_t)s] >= 0)
+            CK(h, cudaMemcpyAsync(snap.p + state * store_at[(size_t)s], h->lat[h->cur], sizeof(R) * state,
+                                  cudaMemcpyDeviceToDevice, st));
+        if (s == T - 1)
+            CK(h, cudaMemcpyAsync(work.p, h->lat[h->cur], sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
         const Lat<R, R> src = make_lat<R, R>(h, h->cur), dst = make_lat<R, R>(h, h->cur ^ 1);
         launch_bc<R, R>(src, g, bc, ph, st);
-        launch_pbb_step<R>(src, dst, g, ph, ns, red, h->series, h->cap, h->d_itime, st);
+        launch_pbb_step<R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, h->series, h->cap, h->d_itime, st);
         h->cur ^= 1;
         h->itime += 1;
     }
-    CK(h, cudaMemcpyAsync(shell_save.p, h->ghost, sizeof(R) * Q * g.G, cudaMemcpyDeviceToDevice, st));
+    CK(h, cudaMemcpyAsync(wshell.p, h->ghost, sizeof(R) * shell, cudaMemcpyDeviceToDevice, st));
     CK(h, cudaEventRecord(ev[1], st));
     CK(h, cudaGetLastError());
     // objective: mean C_d over the last A steps (steps T-A+1 .. T)
@@ -1287,40 +1408,39 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     J *= gamma;
     if (!std::isfinite(J)) return fail(h, EUP_ERR_DIVERGED, "eup_adjoint_run: forward run diverged");
 
-    // ---- reverse sweep ----
-    // Every segment state keeps its own halo shell: the halo blocks of the step
-    // leaving it write there during recomputation and the adjoint step reads it.
-    // Slots no block writes hold their initial values, copied in once here.
-    for (int t = 0; t < K; ++t)
-        CK(h, cudaMemcpyAsync(seg_shell.p + shell * t, h->ghost, sizeof(R) * shell, cudaMemcpyDeviceToDevice, st));
-    int cur_lam = 0;  // lam[cur_lam] = adjoint of the state after the step being reversed
+    // ---- reverse sweep: the rest of the schedule on the working buffers ----
+    int w = 0;              // work[w] holds the working state (state T-1 now)
+    int cur_lam = 0;        // lam[cur_lam] = adjoint of the state after the step being reversed
     int64_t recomputed = 0;
-    for (int c = nseg - 1; c >= 0; --c) {
-        const int a = c * K, b = std::min(a + K, T);
-        // recompute states a .. b-1 into the segment buffer, with the halo of each
-        CK(h, cudaMemcpyAsync(seg.p, ckpt.p + state * c, sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
-        launch_fill_xface<R, R>(lat_at<R>(h, seg.p), g, st);
-        for (int s = a; s < b; ++s) {
-            const Lat<R, R> src = lat_at<R>(h, seg.p + state * (s - a), seg_shell.p + shell * (s - a));
-            launch_bc<R, R>(src, g, bc, ph, st);
-            if (s + 1 < b) {  // the step's x-face copy feeds the next halo blocks
-                const Lat<R, R> dst = lat_at<R>(h, seg.p + state * (s + 1 - a));
-                launch_pbb_step<R>(src, dst, g, ph, ns, red, scratch_series.p, 2, scratch_itime.p, st);
+    R* const wb[2] = {work.p, work.p + state};
+    launch_fill_xface<R, R>(lat_at<R>(h, wb[w], wshell.p), g, st);
+    for (size_t a = first_adj; a < acts.size(); ++a) {
+        const RevAct act = acts[a];
+        if (act.kind == kActAdvance) {
+            for (int s = 0; s < act.arg; ++s) {
+                const Lat<R, R> src = lat_at<R>(h, wb[w], wshell.p), dst = lat_at<R>(h, wb[w ^ 1], wshell.p);
+                launch_bc<R, R>(src, g, bc, ph, st);
+                launch_pbb_step<R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
+                w ^= 1;
                 ++recomputed;
             }
-        }
-        // adjoint steps b .. a+1: state s-1 -> s
-        for (int s = b; s > a; --s) {
-            const Lat<R, R> f = lat_at<R>(h, seg.p + state * (s - 1 - a), seg_shell.p + shell * (s - 1 - a));
+        } else if (act.kind == kActSnapshot) {
+            CK(h, cudaMemcpyAsync(snap.p + state * act.arg, wb[w], sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
+        } else if (act.kind == kActRestore) {
+            CK(h, cudaMemcpyAsync(wb[w], snap.p + state * act.arg, sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
+            launch_fill_xface<R, R>(lat_at<R>(h, wb[w], wshell.p), g, st);
+        } else {  // adjoint of step t from state t-1
+            const int t = act.arg;
+            const Lat<R, R> f = lat_at<R>(h, wb[w], wshell.p);
+            launch_bc<R, R>(f, g, bc, ph, st);  // the halo of step t, from state t-1
             const Lat<R, R> lin_ = lat_at<R>(h, lam.p + state * cur_lam), lout = lat_at<R>(h, lam.p + state * (cur_lam ^ 1));
-            const R gam = (s > T - A) ? (R)gamma : R(0);
+            const R gam = (t > T - A) ? (R)gamma : R(0);
             launch_pbb_adjoint<R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st);
             cur_lam ^= 1;
         }
     }
     CK(h, cudaEventRecord(ev[2], st));
-    // restore the halo shell and x-face copy of the handle's current state
-    CK(h, cudaMemcpyAsync(h->ghost, shell_save.p, sizeof(R) * Q * g.G, cudaMemcpyDeviceToDevice, st));
+    // the x-face copy of the handle's current state (the working states wrote over it)
     launch_fill_xface<R, R>(make_lat<R, R>(h, h->cur), g, st);
     CK(h, cudaGetLastError());
     CK(h, cudaMemcpyAsync(grad_out, grad.p, sizeof(double) * g.N, cudaMemcpyDeviceToHost, st));
@@ -1334,9 +1454,9 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
         stats[0] = fwd_ms;
         stats[1] = rev_ms;
         stats[2] = (double)recomputed;
-        stats[3] = nseg;
-        stats[4] = K;
-        stats[5] = (double)(sizeof(R) * (state * (nseg + K + 2) + shell * K));
+        stats[3] = slots;
+        stats[4] = revolve_repetition(T, slots);
+        stats[5] = (double)(sizeof(R) * (state * ((size_t)slots + 4) + shell * 2));
         stats[6] = T;
         stats[7] = A;
     }
@@ -1354,7 +1474,10 @@ int eup_set_solid_fraction(eup_handle* h, const double* ns) {
     drop_graphs(h);
     if (!ns) {
         if (h->ns) cudaFree(h->ns);
+        if (h->ns_list) cudaFree(h->ns_list);
         h->ns = nullptr;
+        h->ns_list = nullptr;
+        h->ns_count = 0;
         h->pbb = false;
         return EUP_OK;
     }
@@ -1369,7 +1492,18 @@ int eup_set_solid_fraction(eup_handle* h, const double* ns) {
     for (int64_t t = 0; t < N; ++t)
         if (!(ns[t] >= 0.0 && ns[t] <= 1.0))
             return fail(h, EUP_ERR_INVALID_ARG, "eup_set_solid_fraction: n_s outside [0,1] at index " + std::to_string(t));
+    // the voxels the solid takes momentum from (n_s > 0 in the arithmetic type)
+    std::vector<int32_t> list;
+    for (int64_t t = 0; t < N; ++t)
+        if ((h->prec == EUP_FP64 ? ns[t] : (double)(float)ns[t]) > 0.0) list.push_back((int32_t)t);
     if (!h->ns) CK(h, cudaMalloc(&h->ns, h->rbytes * N));
+    if (h->ns_list) cudaFree(h->ns_list);
+    h->ns_list = nullptr;
+    h->ns_count = 0;
+    CK(h, cudaMalloc(&h->ns_list, sizeof(int32_t) * (list.empty() ? 1 : list.size())));
+    if (!list.empty())
+        CK(h, cudaMemcpy(h->ns_list, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice));
+    h->ns_count = (int64_t)list.size();
     if (h->prec == EUP_FP64) {
         CK(h, cudaMemcpy(h->ns, ns, sizeof(double) * N, cudaMemcpyHostToDevice));
     } else {

@@ -125,6 +125,11 @@ void launch_fill_xface(const Lat<S, R>& L, const Geo& g, cudaStream_t st);
 // planes (kStreamInterior) and the two that do (kStreamFaces), so that an x-slab can
 // receive its halo planes while the interior streams.
 enum { kStreamAll = 0, kStreamInterior = 1, kStreamFaces = 2 };
+// Kernel attributes the stream-collide launches need (once per device, outside graph capture).
+cudaError_t prepare_stream_collide();
+// Number of bounded waits of the staged stream-collide kernel that ran out on this device
+// (each stopped its CTA's stores: the step's result is then incomplete).
+cudaError_t staged_wait_timeouts(unsigned int* count);
 template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g,
                            const Phys<R>& ph, int variant, cudaStream_t st, int part = kStreamAll);
@@ -216,9 +221,13 @@ struct HaloAdjointDevice {
 // Returns EUP_OK or EUP_ERR_UNSUPPORTED (err says why).
 int build_halo_adjoint_tables(const Geo& g, const int bc[6], HaloAdjointTables* out, std::string* err);
 
+// One partial-bounce-back step src -> dst; with `series` the FP64 force of the step (over the
+// ns_count voxels of ns_list, those with n_s > 0) goes to series[(itime + 1) % cap] and the
+// device step counter advances; series == nullptr skips it (recomputation in the adjoint).
 template <typename R>
 void launch_pbb_step(const Lat<R, R>& src, const Lat<R, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
-                     const Reduce& red, double* series, int64_t cap, int64_t* d_itime, cudaStream_t st);
+                     const int32_t* ns_list, int64_t ns_count, const Reduce& red, double* series, int64_t cap,
+                     int64_t* d_itime, cudaStream_t st);
 template <typename R>
 void launch_pbb_adjoint(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
                         const Lat<R, R>& lam_out, R* gmu, double* grad, R gamma, const HaloAdjointDevice& t,

@@ -321,44 +321,115 @@ __device__ __forceinline__ R pull_pre(const Lat<R, R>& L, const Geo& g, int q, i
     return lat_load(L, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
 }
 
-// Forward partial-bounce-back step; the FP64 force of the step goes to
-// series[(itime + 1) % cap] and the device step counter advances.
-// MINB: resident blocks per SM the registers are sized for (FP32: 4, at 64 registers;
-// FP64 keeps its accumulators in 128).
-template <typename R, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_pbb_step(Lat<R, R> src, Lat<R, R> dst, Geo g, Phys<R> ph,
-                                                        const R* ns, Reduce red, double* series, int64_t cap,
-                                                        int64_t* d_itime) {
-    double f[3] = {0.0, 0.0, 0.0};
+// Forward partial-bounce-back step, one node per thread (FP64 storage, odd l).  The force
+// of the step is k_pbb_force's.
+template <typename R>
+__global__ void __launch_bounds__(256) k_pbb_step(Lat<R, R> src, Lat<R, R> dst, Geo g, Phys<R> ph, const R* ns) {
     for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.N;
          lin += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(lin % g.l) + 1, j = (int)((lin / g.l) % g.m) + 1, k = (int)(lin / g.lm) + 1;
         const bool face = (i == 1) | (i == g.l) | (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-        R pre[19], x[19];
+        R x[19];
 #pragma unroll
-        for (int q = 0; q < 18; ++q) pre[q] = pull_pre(src, g, q, i, j, k, lin, face);
-        pre[18] = src.pop[18][lin];
+        for (int q = 0; q < 18; ++q) x[q] = pull_pre(src, g, q, i, j, k, lin, face);
+        x[18] = src.pop[18][lin];
+        collide<R>(x, ph.omega, ph.omega1, ph.fgrad);
         const R s = ns[lin];
+        if (s != R(0)) {  // f* = (1 - n_s) BGK(f) + n_s f_opp; n_s = 0 leaves the BGK value
+            const R s1 = R(1) - s;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const int qo = opp_of(q);
+                const R pre_o = qo == 18 ? src.pop[18][lin] : pull_pre(src, g, qo, i, j, k, lin, face);
+                x[q] = s1 * x[q] + s * pre_o;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            dst.pop[q][lin] = x[q];
+            if (q < 18 && i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = x[q];
+            if (q < 18 && i == g.l) dst.xface[xface_idx(g, 1, q, j, k)] = x[q];
+        }
+    }
+}
+
+// Pulled population q of the pair (i, i+1), i odd, of row (j, k) (rowlin = linear index of
+// x = 1 on the row): rows on the y/z boundary planes node by node through the halo shell,
+// elsewhere two shifted loads (one 8-byte load when cx = 0) with the x-halo values of the
+// row's first and last node from the shell.
+__device__ __forceinline__ F2 pull_pair_f32(const Lat<float, float>& L, const Geo& g, int q, int i, int j, int k,
+                                            int rowlin, bool face) {
+    const int cx = q == 18 ? 0 : cx_of(q), cy = q == 18 ? 0 : cy_of(q), cz = q == 18 ? 0 : cz_of(q);
+    if (face) return F2(lat_load(L, g, q, i - cx, j - cy, k - cz), lat_load(L, g, q, i + 1 - cx, j - cy, k - cz));
+    const float* rp = L.pop[q] + (rowlin - cy * g.l - cz * (int)g.lm);
+    if (cx == 0) return F2(*reinterpret_cast<const float2*>(rp + (i - 1)));
+    // both loads stay inside the population for interior rows (see the stream-collide kernel)
+    float a = rp[i - 1 - cx], b = rp[i - cx];
+    if (cx == 1 && i == 1) a = L.ghost[(int64_t)q * g.G + g.gidx(0, j - cy, k - cz)];
+    if (cx == -1 && i + 1 == g.l) b = L.ghost[(int64_t)q * g.G + g.gidx(g.l + 1, j - cy, k - cz)];
+    return F2(a, b);
+}
+
+// Forward partial-bounce-back step, FP32, two nodes per thread (l even): the BGK collision
+// runs once on F2 values (packed FP32, each lane rounded as the one-node kernel, so the
+// bits are the same), and only pairs with n_s != 0 on either node pull the opposite
+// populations again for the mixing.  grid (ceil(np/128), m, n), pairs p0 .. p0+np-1.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pbb_pair(Lat<float, float> src, Lat<float, float> dst, Geo g,
+                                                        Phys<float> ph, const float* ns, int np) {
+    const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (t >= np) return;
+    const int i = 2 * t + 1, j = (int)blockIdx.y + 1, k = (int)blockIdx.z + 1;
+    const int rowlin = g.l * ((j - 1) + g.m * (k - 1));
+    const bool face = (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
+    F2 x[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) x[q] = pull_pair_f32(src, g, q, i, j, k, rowlin, face);
+    collide<F2>(x, F2(ph.omega), F2(ph.omega1), F2(ph.fgrad));
+    const float2 sv = *reinterpret_cast<const float2*>(ns + rowlin + (i - 1));
+    if (sv.x != 0.0f || sv.y != 0.0f) {
+        const F2 s(sv), s1 = F2(1.0f) - s;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) x[q] = s1 * x[q] + s * pull_pair_f32(src, g, opp_of(q), i, j, k, rowlin, face);
+    }
+    if (i == 1) {
+#pragma unroll
+        for (int q = 0; q < 18; ++q) dst.xface[xface_idx(g, 0, q, j, k)] = x[q].v.x;
+    }
+    if (i + 1 == g.l) {
+#pragma unroll
+        for (int q = 0; q < 18; ++q) dst.xface[xface_idx(g, 1, q, j, k)] = x[q].v.y;
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) *reinterpret_cast<float2*>(dst.pop[q] + rowlin + (i - 1)) = x[q].v;
+}
+
+// Momentum the solid takes in the step, F = sum over voxels with n_s > 0 of 2 n_s j(x), j
+// the momentum of the pulled (pre-collision) populations, in FP64 over the list of those
+// voxels; written to series[(itime + 1) % cap] and the device step counter advanced (one
+// block at least, so an empty list records a zero force).
+template <typename R>
+__global__ void __launch_bounds__(256) k_pbb_force(Lat<R, R> src, Geo g, const R* ns, const int32_t* list,
+                                                   int64_t nlist, Reduce red, double* series, int64_t cap,
+                                                   int64_t* d_itime) {
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nlist;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t lin = list[t];
+        const int i = (int)(lin % g.l) + 1, j = (int)((lin / g.l) % g.m) + 1, k = (int)(lin / g.lm) + 1;
+        const bool face = (i == 1) | (i == g.l) | (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
         double jx = 0.0, jy = 0.0, jz = 0.0;
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            x[q] = pre[q];
-            jx += cx_of(q) * (double)pre[q];
-            jy += cy_of(q) * (double)pre[q];
-            jz += cz_of(q) * (double)pre[q];
+            const double v = (double)(q == 18 ? src.pop[18][lin] : pull_pre(src, g, q, i, j, k, lin, face));
+            jx += (q == 18 ? 0 : cx_of(q)) * v;
+            jy += (q == 18 ? 0 : cy_of(q)) * v;
+            jz += (q == 18 ? 0 : cz_of(q)) * v;
         }
-        f[0] += 2.0 * (double)s * jx;
-        f[1] += 2.0 * (double)s * jy;
-        f[2] += 2.0 * (double)s * jz;
-        collide<R>(x, ph.omega, ph.omega1, ph.fgrad);
-        const R s1 = R(1) - s;
-#pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            const R v = s1 * x[q] + s * pre[opp_of(q)];
-            dst.pop[q][lin] = v;
-            if (q < 18 && i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = v;
-            if (q < 18 && i == g.l) dst.xface[xface_idx(g, 1, q, j, k)] = v;
-        }
+        const double s = (double)ns[lin];
+        f[0] += 2.0 * s * jx;
+        f[1] += 2.0 * s * jy;
+        f[2] += 2.0 * s * jz;
     }
     block_reduce_store<3>(f, red, nullptr, series, cap, d_itime, 1, 1);
 }
@@ -366,21 +437,23 @@ __global__ void __launch_bounds__(256, MINB) k_pbb_step(Lat<R, R> src, Lat<R, R>
 // Adjoint of one step: state f (entering the step, its halo shell holding the
 // halo values of that step), lam_in = adjoint of the state the step produced;
 // writes the adjoint of f (lam_out, pushed), the halo part of it (gmu, per
-// halo slot), and accumulates dJ/dn_s.  One pass over the 19 directions: the
-// BGK post-collision value needed by dJ/dn_s is re-evaluated from rho and u.
-template <typename R>
-__global__ void __launch_bounds__(256, 2) k_pbb_adjoint(Lat<R, R> f, Geo g, Phys<R> ph, const R* ns, Lat<R, R> lam_in,
+// halo slot), and accumulates dJ/dn_s.  The pulled populations stay in registers;
+// lam_in is read in two passes over the 19 directions (the sums of the BGK
+// Jacobian's transpose first, then the pushed values, whose second read of the
+// node's 19 words comes from the cache), so one node fits in few registers and
+// many nodes are in flight per SM.  The BGK post-collision value needed by dJ/dn_s
+// is re-evaluated from rho and u.
+template <typename R, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pbb_adjoint(Lat<R, R> f, Geo g, Phys<R> ph, const R* ns, Lat<R, R> lam_in,
                                                      Lat<R, R> lam_out, R* gmu, double* grad, R gamma) {
     for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.N;
          lin += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(lin % g.l) + 1, j = (int)((lin / g.l) % g.m) + 1, k = (int)(lin / g.lm) + 1;
         const bool face = (i == 1) | (i == g.l) | (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-        R pre[19], lam[19];
+        R pre[19];
 #pragma unroll
         for (int q = 0; q < 18; ++q) pre[q] = pull_pre(f, g, q, i, j, k, lin, face);
         pre[18] = f.pop[18][lin];
-#pragma unroll
-        for (int q = 0; q < 19; ++q) lam[q] = lam_in.pop[q][lin];
         const R s = ns[lin], s1 = R(1) - s;
         R rho = R(0), jx = R(0), jy = R(0), jz = R(0);
 #pragma unroll
@@ -397,27 +470,29 @@ __global__ void __launch_bounds__(256, 2) k_pbb_adjoint(Lat<R, R> f, Geo g, Phys
         R A = R(0), Bx = R(0), By = R(0), Bz = R(0), Fx = R(0);
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
+            const R lam = lam_in.pop[q][lin];
             const R w = weight<R>(q);
             const R cu = R(cx_of(q)) * ux + R(cy_of(q)) * uy + R(cz_of(q)) * uz;
             const R feq = w * rho * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq);
             const R bgk = ph.omega1 * pre[q] + ph.omega * feq + frho * R(cx_of(q));
-            gs += lam[q] * (pre[opp_of(q)] - bgk);
-            const R nw = s1 * lam[q] * w;
+            gs += lam * (pre[opp_of(q)] - bgk);
+            const R nw = s1 * lam * w;
             A += nw * (R(1) - R(4.5) * cu * cu + R(1.5) * usq);
             const R b9 = nw * R(9) * cu;
             Bx += nw * R(3) * (R(cx_of(q)) - ux) + b9 * R(cx_of(q));
             By += nw * R(3) * (R(cy_of(q)) - uy) + b9 * R(cy_of(q));
             Bz += nw * R(3) * (R(cz_of(q)) - uz) + b9 * R(cz_of(q));
-            Fx += s1 * lam[q] * R(cx_of(q));
+            Fx += s1 * lam * R(cx_of(q));
         }
         grad[lin] += (double)gs;
         const R common = ph.omega * A + ph.fgrad * Fx;
         const R g2 = gamma * R(2) * s;
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            const R mu = ph.omega1 * s1 * lam[q] + common +
+            const R lam = lam_in.pop[q][lin], lam_o = lam_in.pop[opp_of(q)][lin];
+            const R mu = ph.omega1 * s1 * lam + common +
                          ph.omega * (R(cx_of(q)) * Bx + R(cy_of(q)) * By + R(cz_of(q)) * Bz) +
-                         s * lam[opp_of(q)] + g2 * R(cx_of(q));
+                         s * lam_o + g2 * R(cx_of(q));
             if (!face) {  // f_q(x) was pulled from the interior node x - c_q
                 lam_out.pop[q][lin - cx_of(q) - (int64_t)cy_of(q) * g.l - (int64_t)cz_of(q) * g.lm] = mu;
             } else {
@@ -487,16 +562,34 @@ unsigned capped_grid(int64_t work, int tpb) {
 
 template <typename R>
 void launch_pbb_step(const Lat<R, R>& src, const Lat<R, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
-                     const Reduce& red, double* series, int64_t cap, int64_t* d_itime, cudaStream_t st) {
-    k_pbb_step<R, sizeof(R) == 4 ? 4 : 1><<<capped_grid(g.N, 256), 256, 0, st>>>(src, dst, g, ph, ns, red, series,
-                                                                                   cap, d_itime);
+                     const int32_t* ns_list, int64_t ns_count, const Reduce& red, double* series, int64_t cap,
+                     int64_t* d_itime, cudaStream_t st) {
+    if (series) {  // the force first: it reads the source lattice the step leaves unchanged
+        k_pbb_force<R><<<capped_grid(ns_count, 256), 256, 0, st>>>(src, g, ns, ns_list, ns_count, red, series, cap,
+                                                                    d_itime);
+    }
+    if constexpr (sizeof(R) == 4) {
+        bool aligned = true;
+        for (int q = 0; q < Q; ++q)
+            aligned = aligned && reinterpret_cast<uintptr_t>(src.pop[q]) % 8 == 0 &&
+                      reinterpret_cast<uintptr_t>(dst.pop[q]) % 8 == 0;
+        if (g.l % 2 == 0 && aligned && reinterpret_cast<uintptr_t>(ns) % 8 == 0) {
+            const int np = g.l / 2;
+            dim3 grid((np + 127) / 128, g.m, g.n);
+            k_pbb_pair<5><<<grid, 128, 0, st>>>(src, dst, g, ph, ns, np);
+            return;
+        }
+    }
+    k_pbb_step<R><<<capped_grid(g.N, 256), 256, 0, st>>>(src, dst, g, ph, ns);
 }
 
 template <typename R>
 void launch_pbb_adjoint(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
                         const Lat<R, R>& lam_out, R* gmu, double* grad, R gamma, const HaloAdjointDevice& t,
                         cudaStream_t st) {
-    k_pbb_adjoint<R><<<capped_grid(g.N, 256), 256, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma);
+    // resident blocks of 256 per SM the registers are sized for: FP32 3 (80 registers), FP64 2
+    k_pbb_adjoint<R, sizeof(R) == 4 ? 3 : 2><<<capped_grid(g.N, 256), 256, 0, st>>>(f, g, ph, ns, lam_in, lam_out,
+                                                                                      gmu, grad, gamma);
     if (t.ncopy > 0)
         k_adj_copy<R><<<(unsigned)((t.ncopy + 255) / 256), 256, 0, st>>>(g, t.copy_key, t.copy_start, t.copy_slot,
                                                                           t.ncopy, gmu, lam_out);
@@ -506,11 +599,11 @@ void launch_pbb_adjoint(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, con
 }
 
 template void launch_pbb_step<float>(const Lat<float, float>&, const Lat<float, float>&, const Geo&,
-                                     const Phys<float>&, const float*, const Reduce&, double*, int64_t, int64_t*,
-                                     cudaStream_t);
+                                     const Phys<float>&, const float*, const int32_t*, int64_t, const Reduce&,
+                                     double*, int64_t, int64_t*, cudaStream_t);
 template void launch_pbb_step<double>(const Lat<double, double>&, const Lat<double, double>&, const Geo&,
-                                      const Phys<double>&, const double*, const Reduce&, double*, int64_t,
-                                      int64_t*, cudaStream_t);
+                                      const Phys<double>&, const double*, const int32_t*, int64_t, const Reduce&,
+                                      double*, int64_t, int64_t*, cudaStream_t);
 template void launch_pbb_adjoint<float>(const Lat<float, float>&, const Geo&, const Phys<float>&, const float*,
                                         const Lat<float, float>&, const Lat<float, float>&, float*, double*, float,
                                         const HaloAdjointDevice&, cudaStream_t);

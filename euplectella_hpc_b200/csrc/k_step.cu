@@ -188,6 +188,11 @@ struct PullBase {
     const S* p[19];
 };
 
+// lattice velocity components with the rest population (q = 18) as zero
+__host__ __device__ constexpr int cx_of_or0(int q) { return q == 18 ? 0 : cx_of(q); }
+__host__ __device__ constexpr int cy_of_or0(int q) { return q == 18 ? 0 : cy_of(q); }
+__host__ __device__ constexpr int cz_of_or0(int q) { return q == 18 ? 0 : cz_of(q); }
+
 // 16-bit storage: the 19 pulls of the pair (i, i+1) of an interior row as raw words
 // (aligned in the shifted layout whatever cx is): one index for all of them.
 template <typename S>
@@ -355,6 +360,244 @@ bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const
 }
 
 // ---------------------------------------------------------------------------
+// Staged pair kernel (16-bit storage, l a multiple of 8).  The pulls of the interior rows
+// (2 <= j <= m-1, 2 <= k <= n-1) come into shared memory by bulk asynchronous copies
+// instead of per-thread loads.  In the x-shifted layout the pulls of population q for a
+// run of consecutive nodes x0 .. x0+len-1 of one plane's interior rows are the run
+// pb.p[q][x0 .. x0+len-1]: contiguous and, with x0 and len multiples of 8, 16-byte
+// aligned.  A tile is kTileNodes such nodes (19 bulk copies).
+//
+// Persistent CTAs, warp-specialised: one producer warp and kConsumerWarps consumer warps
+// (one pair of nodes per consumer thread and tile) share a ring of S stages, each with a
+// "full" mbarrier (armed by the producer with the tile's byte count, completed by the
+// copies) and an "empty" mbarrier (one arrival per consumer warp once the warp has read
+// its words of the stage).  Consumers never wait for one another: a warp reads its 19
+// words, releases the stage, then collides and stores while later tiles stream in.  The
+// collision and stores are the register-pull kernel's (finish_pair: same arithmetic, same
+// bits).  Rows on the y/z boundary planes, which pull through the halo shell, follow the
+// tiles in the same launch, node by node.
+//
+// Every wait is bounded (2 s of the global timer).  A wait that runs out counts itself in
+// g_staged_timeouts and stops its CTA: the consumers stop storing, the producer stops
+// issuing and waits (bounded) for the copies it has in flight before the CTA returns.
+// ---------------------------------------------------------------------------
+__device__ unsigned int g_staged_timeouts;
+
+constexpr int kStagedMaxStages = 4;
+constexpr int kConsumerWarps = 8;
+constexpr int kTileNodes = 64 * kConsumerWarps;       // 512 nodes, 256 pairs
+constexpr int kStagedThreads = 32 * (kConsumerWarps + 1);
+constexpr uint64_t kStagedWaitNs = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arm(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// true when the phase with this parity completed, false after kStagedWaitNs
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_test(bar, parity))
+        if (global_ns() - t0 > kStagedWaitNs) return false;
+    return true;
+}
+// bytes (a multiple of 16) from global src (16-byte aligned) to shared dst (16-byte aligned),
+// completion counted on bar
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+struct StagedPlan {
+    int plane_nodes;      // l * (m - 2): the interior rows of one plane
+    int tiles_per_plane;  // ceil(plane_nodes / kTileNodes)
+    int ntiles;           // tiles_per_plane * (n - 2)
+    int nface;            // rows on the y/z boundary planes
+    int stages;
+    float inv_l;          // 1/l (rows of a node offset, corrected to exact)
+};
+
+// Row (j, k) of face row index f: the planes k = 1 and k = n (all j), then j = 1 and j = m
+// of the planes k = 2 .. n-1.
+__device__ __forceinline__ void face_row(const Geo& g, int f, int* j, int* k) {
+    const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
+    if (f < nz * g.m) {
+        *k = f < g.m ? 1 : g.n;
+        *j = f % g.m + 1;
+    } else {
+        const int r = f - nz * g.m;
+        *k = 2 + r / ny;
+        *j = (r % ny == 0) ? 1 : g.m;
+    }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kStagedThreads, 3) k_stream_collide_staged(Lat<S, float> src, Lat<S, float> dst,
+                                                                              Geo g, Phys<float> ph, PullBase<S> pb,
+                                                                              StagedPlan sp) {
+    using V2 = Vec2<S>;
+    using T2 = typename V2::T;
+    constexpr uint32_t kRunBytes = kTileNodes * sizeof(S);   // one population's run in a full tile
+    constexpr uint32_t kStageBytes = 19 * kRunBytes;
+    extern __shared__ __align__(128) unsigned char stage_mem[];
+    __shared__ uint64_t full[kStagedMaxStages], empty[kStagedMaxStages];
+    __shared__ int abort_flag;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int l = g.l, m = g.m;
+    if (tid == 0) {
+        for (int s = 0; s < sp.stages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kConsumerWarps);
+        }
+        mbar_init_fence();
+        abort_flag = 0;
+    }
+    __syncthreads();
+
+    // tile t: nodes x0 .. x0+len-1 (a multiple of 8 of them) of plane k's interior rows,
+    // starting `off` nodes after the plane's row j = 2
+    auto tile = [&](int t, int* k, int* off) {
+        *k = 2 + t / sp.tiles_per_plane;
+        *off = (t % sp.tiles_per_plane) * kTileNodes;
+        return min(kTileNodes, sp.plane_nodes - *off);
+    };
+    const int first = blockIdx.x, stride = gridDim.x;
+    if (warp == kConsumerWarps) {
+        // producer: lane 0 arms each stage and issues its 19 copies once the consumers
+        // have released it
+        if (lane == 0) {
+            int it = 0;
+            for (int t = first; t < sp.ntiles; t += stride, ++it) {
+                const int slot = it % sp.stages;
+                if (it >= sp.stages && !mbar_wait_bounded(&empty[slot], (uint32_t)(it / sp.stages - 1) & 1u)) {
+                    abort_flag = 1;
+                    break;
+                }
+                if (abort_flag) break;
+                int k, off;
+                const int len = tile(t, &k, &off);
+                const uint32_t bytes = (uint32_t)len * (uint32_t)sizeof(S);
+                const uint32_t x0 = (uint32_t)l * (uint32_t)(1 + m * (k - 1)) + (uint32_t)off;
+                unsigned char* base = stage_mem + (size_t)slot * kStageBytes;
+                mbar_arm(&full[slot], 19u * bytes);
+#pragma unroll 1
+                for (int q = 0; q < 19; ++q) bulk_copy_g2s(base + q * kRunBytes, pb.p[q] + x0, bytes, &full[slot]);
+            }
+            // whatever is still in flight lands before the CTA's shared memory is released
+            const int issued = it;
+            for (int u = max(0, issued - sp.stages); u < issued; ++u)
+                mbar_wait_bounded(&full[u % sp.stages], (uint32_t)(u / sp.stages) & 1u);
+        }
+    } else {
+        int it = 0;
+        const int c = tid;  // consumer thread: pair c of every tile
+        for (int t = first; t < sp.ntiles; t += stride, ++it) {
+            const int slot = it % sp.stages;
+            if (!mbar_wait_bounded(&full[slot], (uint32_t)(it / sp.stages) & 1u)) {
+                abort_flag = 1;
+                break;
+            }
+            int k, off;
+            const int len = tile(t, &k, &off);
+            const unsigned char* base = stage_mem + (size_t)slot * kStageBytes;
+            const bool active = 2 * c < len;
+            F2 x[19];
+            if (active) {
+#pragma unroll
+                for (int q = 0; q < 19; ++q)
+                    x[q] = F2(V2::unpack(reinterpret_cast<const T2*>(base + q * kRunBytes)[c]));
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[slot]);
+            if (abort_flag) break;
+            if (active) {
+                // node offset within the plane's interior rows -> row and column
+                const int xr = off + 2 * c;
+                int jr = __float2int_rz((float)xr * sp.inv_l);
+                int ir = xr - jr * l;
+                if (ir < 0) { --jr; ir += l; }
+                if (ir >= l) { ++jr; ir -= l; }
+                const int j = 2 + jr;
+                finish_pair(src, dst, g, ph, ir + 1, j, k, l * ((j - 1) + m * (k - 1)), x);
+            }
+        }
+    }
+    __syncthreads();
+    if (abort_flag) {
+        if (tid == 0) atomicAdd(&g_staged_timeouts, 1u);
+        return;
+    }
+    // rows on the y/z boundary planes: every pull through the halo shell
+    const int half_l = l / 2;
+    for (int f = blockIdx.x; f < sp.nface; f += stride) {
+        int j, k;
+        face_row(g, f, &j, &k);
+        for (int p = tid; p < half_l; p += kStagedThreads) pair_step(src, dst, g, ph, pb, 2 * p + 1, j, k);
+    }
+}
+
+constexpr int kStagedSmemLimit = 200 * 1024;   // dynamic shared memory the staged kernels opt into
+constexpr int kSmemPerSM = 228 * 1024;
+
+template <typename S>
+bool launch_staged(const Lat<S, float>& src, const Lat<S, float>& dst, const Geo& g, const Phys<float>& ph,
+                   cudaStream_t st) {
+    if (g.l % 8 != 0 || g.l < 8) return false;
+    StagedPlan sp;
+    const int64_t plane_nodes = (int64_t)g.l * (g.m - 2);
+    sp.plane_nodes = plane_nodes > 0 ? (int)plane_nodes : 0;
+    sp.tiles_per_plane = (sp.plane_nodes + kTileNodes - 1) / kTileNodes;
+    sp.ntiles = (g.n >= 3 && sp.plane_nodes > 0) ? sp.tiles_per_plane * (g.n - 2) : 0;
+    const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
+    sp.nface = nz * g.m + (g.n > 2 ? (g.n - 2) * ny : 0);
+    sp.inv_l = 1.0f / (float)g.l;
+    const int stage_bytes = 19 * kTileNodes * (int)sizeof(S);
+    // three CTAs per SM, each with as many stages as fit (at most four)
+    sp.stages = kStagedMaxStages;
+    while (sp.stages > 2 && 3 * (stage_bytes * sp.stages + 1024) > kSmemPerSM) --sp.stages;
+    // every run starts on a 16-byte boundary: the pull bases (a tile starts at a multiple of 8)
+    PullBase<S> pb;
+    for (int q = 0; q < Q; ++q) {
+        pb.p[q] = src.pop[q] - (cy_of_or0(q) * (int64_t)g.l + cz_of_or0(q) * g.lm + cx_of_or0(q));
+        if (reinterpret_cast<uintptr_t>(pb.p[q]) % 16 != 0) return false;
+    }
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return false;
+    const size_t smem = (size_t)stage_bytes * sp.stages;
+    k_stream_collide_staged<S><<<(unsigned)(3 * sms), kStagedThreads, smem, st>>>(src, dst, g, ph, pb, sp);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Vectorised variant: each thread owns VW consecutive x-nodes of one (j,k)
 // row, so every population moves as one 16-byte (or 8-byte) load and store.
 // Pulls along x (cx = +-1) need one element of the neighbouring thread's
@@ -501,13 +744,17 @@ template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph,
                            int variant, cudaStream_t st, int part) {
     // EUP_STEP_VARIANT bit 0: 16-byte vectors, bit 2: 8-byte vectors (when l allows), bit 3: one
-    // node per thread, bits 4-6: occupancy target of the two-node kernel (n + 3 blocks per SM);
-    // default: two nodes per thread (FP32 arithmetic, l even).  A split step (interior columns,
+    // node per thread, bits 4-6: occupancy target of the two-node kernel (n + 3 blocks per SM),
+    // bit 7: 16-bit storage without shared-memory staging; default: 16-bit storage staged
+    // (l a multiple of 8), otherwise two nodes per thread (FP32 arithmetic, l even).  A split step (interior columns,
     // then the two x-face columns) uses the two-node or the one-node kernel.
     constexpr int VW = VecWidth<S>::value;
     if (part == kStreamAll) {
         if ((variant & 1) && launch_vec<S, R, VW>(src, dst, g, ph, st)) return;
         if ((variant & 4) && launch_vec<S, R, (VW / 2 > 0 ? VW / 2 : 1)>(src, dst, g, ph, st)) return;
+        if constexpr (DevStore<S>::value) {
+            if (!(variant & (8 | 128)) && launch_staged<S>(src, dst, g, ph, st)) return;
+        }
     }
     if (!(variant & 8) && launch_pair<S, R>(src, dst, g, ph, (variant >> 4) & 7, part, st)) return;
     const int bx = 128;
@@ -533,6 +780,21 @@ template void launch_stream_collide<__half, float>(const Lat<__half, float>&, co
 template void launch_stream_collide<__nv_bfloat16, float>(const Lat<__nv_bfloat16, float>&,
                                                           const Lat<__nv_bfloat16, float>&, const Geo&,
                                                           const Phys<float>&, int, cudaStream_t, int);
+
+cudaError_t prepare_stream_collide() {
+    // the staged kernels opt into more than 48 KB of dynamic shared memory (set once per
+    // device, before any launch is captured into a graph)
+    cudaError_t e = cudaFuncSetAttribute(k_stream_collide_staged<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kStagedSmemLimit);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_stream_collide_staged<__nv_bfloat16>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmemLimit);
+    return e;
+}
+
+cudaError_t staged_wait_timeouts(unsigned int* count) {
+    return cudaMemcpyFromSymbol(count, g_staged_timeouts, sizeof(unsigned int));
+}
 
 }  // namespace eup
 

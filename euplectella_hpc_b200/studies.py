@@ -130,7 +130,7 @@ def adjoint_study(steps=4000, avg_steps=1000, checkpoints=64, n_fd=32, h=1e-3, h
                      "adjoint_reverse_ms": st["reverse_ms"],
                      "adjoint_over_forward": (st["forward_ms"] + st["reverse_ms"]) / fwd_ms,
                      "recomputed_steps": st["recomputed_steps"], "checkpoints_used": st["checkpoints"],
-                     "segment_steps": st["segment_steps"], "stored_state_bytes": st["state_bytes"]}
+                     "repetitions": st["repetitions"], "stored_state_bytes": st["state_bytes"]}
     out["grad_fp32_vs_fp64_rel_l2"] = float(np.linalg.norm(grads["fp32"] - grads["fp64"]) /
                                             np.linalg.norm(grads["fp64"]))
     # central differences (FP64) at seeded voxels away from the [0,1] bounds
@@ -278,7 +278,7 @@ def ridge_adjoint(scale=0.25, re=500.0, steps=2500, avg_steps=625, checkpoints=6
         J, g, st = s.adjoint(steps, avg_steps, checkpoints)
     out.update({"objective": J, "forward_ms": fwd_ms, "adjoint_ms": st["forward_ms"] + st["reverse_ms"],
                 "adjoint_over_forward": (st["forward_ms"] + st["reverse_ms"]) / fwd_ms,
-                "checkpoints_used": st["checkpoints"], "segment_steps": st["segment_steps"]})
+                "checkpoints_used": st["checkpoints"], "repetitions": st["repetitions"]})
     out["dJ_dh_adjoint"] = float((g * dns).sum())
 
     def objective(h):

@@ -391,17 +391,21 @@ int eup_set_solid_fraction(eup_handle* h, const double* ns);
 typedef struct eup_adjoint_config {
     int32_t nsteps;       /* forward steps T from the current state */
     int32_t avg_steps;    /* objective: mean C_d over the last avg_steps steps */
-    int32_t checkpoints;  /* checkpoint slots; 0 selects 64 */
+    int32_t checkpoints;  /* stored states (snapshot slots); 0 selects 64 */
     int32_t reserved;
 } eup_adjoint_config;
 
 /* Runs T partial-bounce-back steps from the current state and the discrete
  * adjoint back to it: *objective = mean C_d over the last avg_steps steps,
  * grad_ns[l*m*n] = d objective / d n_s per voxel (FP64, Fortran order).
- * Checkpoints every K = ceil(T/checkpoints) steps and recomputes each segment
- * once.  Leaves the handle at step itime + T.  stats (may be NULL): forward ms,
- * reverse ms (recomputation + adjoint), recomputed steps, checkpoints, K,
- * device bytes of stored states, T, avg_steps. */
+ * Binomial checkpointing (Griewank 1992; Griewank & Walther 2000): with c =
+ * checkpoints stored states the reverse sweep recomputes the fewest forward
+ * steps possible, t(T, c) - (T - 1) beyond the forward sweep, where t(n, c) =
+ * r n - C(c + r, r - 1) and r is the smallest repetition number with
+ * C(c + r, c) >= n; device memory is c + 4 states.  Leaves the handle at step
+ * itime + T.  stats (may be NULL): forward ms, reverse ms (recomputation +
+ * adjoint), recomputed steps, stored states c, repetition number r, device
+ * bytes of the states, T, avg_steps. */
 int eup_adjoint_run(eup_handle* h, const eup_adjoint_config* cfg, double* objective, double* grad_ns,
                     double stats[8]);
 

@@ -57,7 +57,10 @@ def test_adjoint_matches_central_differences_fp64(eup, require_gpu):
         s.set_solid_fraction(ns)
         s.upload(a)
         J, grad, st = s.adjoint(T, A, checkpoints=8)
-    assert st["recomputed_steps"] > 0
+    # binomial checkpointing with 8 stored states: r = 3 (C(11, 8) = 165 >= 150), t(150, 8) =
+    # 3*150 - C(11, 2) = 395 forward steps, 149 of them in the forward sweep
+    assert st["checkpoints"] == 8 and st["repetitions"] == 3
+    assert st["recomputed_steps"] == 395 - 149
     assert abs(J - run_objective(eup, cfg, ns, a)) <= 1e-12 * abs(J)
     rng = np.random.default_rng(7)
     cand = np.argwhere((ns > 0.01) & (ns < 0.99))

@@ -329,9 +329,10 @@ def test_deviation_storage_against_fp64(eup, require_gpu, prec):
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16", "bf16"])
 def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
-    """Two nodes per thread (default for 16/32-bit storage, at several occupancies) vs one
-    node per thread vs 16-byte and 8-byte vectorised stream-collide, CUDA graphs vs plain
-    launches: all paths give the same bits in every storage format."""
+    """Two nodes per thread (default for 32-bit storage, at several occupancies; for 16-bit
+    storage the default stages the pulls in shared memory, variant 128 loads them into
+    registers) vs one node per thread vs 16-byte and 8-byte vectorised stream-collide, CUDA
+    graphs vs plain launches: all paths give the same bits in every storage format."""
     l, m, n = 256, 20, 13
     code = {"fp32": eup.FP32, "fp64": eup.FP64, "fp16": eup.FP16_DEV, "bf16": eup.BF16_DEV}[prec]
     dt = np.float64 if prec == "fp64" else np.float32
@@ -339,7 +340,7 @@ def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
     a = eup.init_equilibrium(l, m, n, 0.05, 1e-3, 77, dt)
     cfg = eup.Config(l, m, n, bc=(5, 4, 3, 3, 0, 0), svisc=0.01, u_inflow=0.05, precision=code)
     res = []
-    for var in ("0", "1", "2", "3", "4", "6", "8", "10", "16", "48", "80"):
+    for var in ("0", "1", "2", "3", "4", "6", "8", "10", "16", "48", "80", "128", "130", "144"):
         monkeypatch.setenv("EUP_STEP_VARIANT", var)
         with eup.Solver(cfg) as s:
             s.set_obstacles(obs)
