@@ -1361,32 +1361,47 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
         if (state != T - 1) return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: internal schedule error");
     }
 
+    // state buffers: the slots, then two working buffers; each with its own x-face copy
+    // (the columns x = 1 and x = l the halo blocks read), so a state is never copied to be
+    // read: a restore only makes a slot the working state, and the forward step that ends
+    // where the schedule stores a state writes it into the slot directly
     const size_t state = (size_t)Q * h->Nq;
     const size_t shell = (size_t)Q * g.G;
-    DevBuf<R> snap, work, lam, gmu, wshell;
+    const size_t xfs = (size_t)2 * 18 * g.m * g.n;
+    const int nbuf = slots + 2;
+    DevBuf<R> bufs, xfaces, lam, gmu, wshell;
     DevBuf<double> grad;
-    CK(h, snap.alloc(state * slots));
-    CK(h, work.alloc(state * 2));
+    CK(h, bufs.alloc(state * nbuf));
+    CK(h, xfaces.alloc(xfs * nbuf));
     CK(h, lam.alloc(state * 2));
     CK(h, gmu.alloc(shell));
     CK(h, wshell.alloc(shell));
     CK(h, grad.alloc(g.N));
     CK(h, cudaMemsetAsync(grad.p, 0, sizeof(double) * g.N, st));
     CK(h, cudaMemsetAsync(lam.p, 0, sizeof(R) * state * 2, st));
-    CK(h, cudaMemsetAsync(work.p, 0, sizeof(R) * state * 2, st));
     const Reduce red = make_reduce(h);
+    auto buf_lat = [&](int b) {
+        Lat<R, R> L = lat_at<R>(h, bufs.p + state * b, wshell.p);
+        L.xface = xfaces.p + xfs * b;
+        return L;
+    };
+    auto keep = [&](int b) -> cudaError_t {  // the handle's current state (and x-face copy) into buffer b
+        cudaError_t e = cudaMemcpyAsync(bufs.p + state * b, h->lat[h->cur], sizeof(R) * state,
+                                        cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(xfaces.p + xfs * b, h->xface, sizeof(R) * xfs, cudaMemcpyDeviceToDevice, st);
+        return e;
+    };
 
     cudaEvent_t ev[3];
     for (auto& e : ev) CK(h, cudaEventCreate(&e));
     // ---- forward sweep (the handle's own state, force series recorded) ----
     const int64_t t0 = h->itime;
+    const int w0 = slots, w1 = slots + 1;  // the working buffers
     CK(h, cudaEventRecord(ev[0], st));
     for (int s = 0; s < T; ++s) {
-        if (store_at[(size_t)s] >= 0)
-            CK(h, cudaMemcpyAsync(snap.p + state * store_at[(size_t)s], h->lat[h->cur], sizeof(R) * state,
-                                  cudaMemcpyDeviceToDevice, st));
-        if (s == T - 1)
-            CK(h, cudaMemcpyAsync(work.p, h->lat[h->cur], sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
+        if (store_at[(size_t)s] >= 0) CK(h, keep(store_at[(size_t)s]));
+        if (s == T - 1) CK(h, keep(w0));
         const Lat<R, R> src = make_lat<R, R>(h, h->cur), dst = make_lat<R, R>(h, h->cur ^ 1);
         launch_bc<R, R>(src, g, bc, ph, st);
         launch_pbb_step<R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, h->series, h->cap, h->d_itime, st);
@@ -1408,30 +1423,37 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     J *= gamma;
     if (!std::isfinite(J)) return fail(h, EUP_ERR_DIVERGED, "eup_adjoint_run: forward run diverged");
 
-    // ---- reverse sweep: the rest of the schedule on the working buffers ----
-    int w = 0;              // work[w] holds the working state (state T-1 now)
+    // ---- reverse sweep: the rest of the schedule ----
+    int cur = w0;           // buffer holding the working state (state T-1 now)
     int cur_lam = 0;        // lam[cur_lam] = adjoint of the state after the step being reversed
     int64_t recomputed = 0;
-    R* const wb[2] = {work.p, work.p + state};
-    launch_fill_xface<R, R>(lat_at<R>(h, wb[w], wshell.p), g, st);
     for (size_t a = first_adj; a < acts.size(); ++a) {
         const RevAct act = acts[a];
         if (act.kind == kActAdvance) {
+            // the last step goes straight into the slot the next action stores
+            const int target = (a + 1 < acts.size() && acts[a + 1].kind == kActSnapshot) ? acts[a + 1].arg : -1;
             for (int s = 0; s < act.arg; ++s) {
-                const Lat<R, R> src = lat_at<R>(h, wb[w], wshell.p), dst = lat_at<R>(h, wb[w ^ 1], wshell.p);
+                const int next = (s + 1 == act.arg && target >= 0) ? target : (cur == w0 ? w1 : w0);
+                const Lat<R, R> src = buf_lat(cur), dst = buf_lat(next);
                 launch_bc<R, R>(src, g, bc, ph, st);
                 launch_pbb_step<R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
-                w ^= 1;
+                cur = next;
                 ++recomputed;
             }
+            if (target >= 0) ++a;  // the store is done
         } else if (act.kind == kActSnapshot) {
-            CK(h, cudaMemcpyAsync(snap.p + state * act.arg, wb[w], sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
+            if (cur != act.arg) {  // not reached in these schedules: a store always follows a forward step
+                CK(h, cudaMemcpyAsync(bufs.p + state * act.arg, bufs.p + state * cur, sizeof(R) * state,
+                                      cudaMemcpyDeviceToDevice, st));
+                CK(h, cudaMemcpyAsync(xfaces.p + xfs * act.arg, xfaces.p + xfs * cur, sizeof(R) * xfs,
+                                      cudaMemcpyDeviceToDevice, st));
+                cur = act.arg;
+            }
         } else if (act.kind == kActRestore) {
-            CK(h, cudaMemcpyAsync(wb[w], snap.p + state * act.arg, sizeof(R) * state, cudaMemcpyDeviceToDevice, st));
-            launch_fill_xface<R, R>(lat_at<R>(h, wb[w], wshell.p), g, st);
+            cur = act.arg;  // read in place; forward steps write elsewhere
         } else {  // adjoint of step t from state t-1
             const int t = act.arg;
-            const Lat<R, R> f = lat_at<R>(h, wb[w], wshell.p);
+            const Lat<R, R> f = buf_lat(cur);
             launch_bc<R, R>(f, g, bc, ph, st);  // the halo of step t, from state t-1
             const Lat<R, R> lin_ = lat_at<R>(h, lam.p + state * cur_lam), lout = lat_at<R>(h, lam.p + state * (cur_lam ^ 1));
             const R gam = (t > T - A) ? (R)gamma : R(0);
@@ -1440,8 +1462,6 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
         }
     }
     CK(h, cudaEventRecord(ev[2], st));
-    // the x-face copy of the handle's current state (the working states wrote over it)
-    launch_fill_xface<R, R>(make_lat<R, R>(h, h->cur), g, st);
     CK(h, cudaGetLastError());
     CK(h, cudaMemcpyAsync(grad_out, grad.p, sizeof(double) * g.N, cudaMemcpyDeviceToHost, st));
     CK(h, cudaStreamSynchronize(st));
@@ -1456,7 +1476,7 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
         stats[2] = (double)recomputed;
         stats[3] = slots;
         stats[4] = revolve_repetition(T, slots);
-        stats[5] = (double)(sizeof(R) * (state * ((size_t)slots + 4) + shell * 2));
+        stats[5] = (double)(sizeof(R) * ((state + xfs) * (size_t)nbuf + state * 2 + shell * 2));
         stats[6] = T;
         stats[7] = A;
     }

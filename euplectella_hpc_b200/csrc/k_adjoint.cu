@@ -321,189 +321,221 @@ __device__ __forceinline__ R pull_pre(const Lat<R, R>& L, const Geo& g, int q, i
     return lat_load(L, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
 }
 
-// Forward partial-bounce-back step, one node per thread (FP64 storage, odd l).  The force
-// of the step is k_pbb_force's.
+// The partial-bounce-back step is the plain stream-collide (every node's BGK value, the
+// same kernels and bits as the plain step) followed by this kernel over the list of
+// voxels with n_s > 0: it pulls their pre-collision populations again, mixes
+//   f*_q = (1 - n_s) BGK_q + n_s f_opp(q)
+// into the destination lattice (and its x-face copy), and with `series` adds the
+// momentum the solid takes, F = sum 2 n_s j(x) over the list, j the momentum of the pulled
+// populations, in FP64 into series[(itime + 1) % cap], advancing the device step counter
+// (one block at least, so an empty list records a zero force).
 template <typename R>
-__global__ void __launch_bounds__(256) k_pbb_step(Lat<R, R> src, Lat<R, R> dst, Geo g, Phys<R> ph, const R* ns) {
-    for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.N;
-         lin += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(lin % g.l) + 1, j = (int)((lin / g.l) % g.m) + 1, k = (int)(lin / g.lm) + 1;
-        const bool face = (i == 1) | (i == g.l) | (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-        R x[19];
-#pragma unroll
-        for (int q = 0; q < 18; ++q) x[q] = pull_pre(src, g, q, i, j, k, lin, face);
-        x[18] = src.pop[18][lin];
-        collide<R>(x, ph.omega, ph.omega1, ph.fgrad);
-        const R s = ns[lin];
-        if (s != R(0)) {  // f* = (1 - n_s) BGK(f) + n_s f_opp; n_s = 0 leaves the BGK value
-            const R s1 = R(1) - s;
-#pragma unroll
-            for (int q = 0; q < 19; ++q) {
-                const int qo = opp_of(q);
-                const R pre_o = qo == 18 ? src.pop[18][lin] : pull_pre(src, g, qo, i, j, k, lin, face);
-                x[q] = s1 * x[q] + s * pre_o;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            dst.pop[q][lin] = x[q];
-            if (q < 18 && i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = x[q];
-            if (q < 18 && i == g.l) dst.xface[xface_idx(g, 1, q, j, k)] = x[q];
-        }
-    }
-}
-
-// Pulled population q of the pair (i, i+1), i odd, of row (j, k) (rowlin = linear index of
-// x = 1 on the row): rows on the y/z boundary planes node by node through the halo shell,
-// elsewhere two shifted loads (one 8-byte load when cx = 0) with the x-halo values of the
-// row's first and last node from the shell.
-__device__ __forceinline__ F2 pull_pair_f32(const Lat<float, float>& L, const Geo& g, int q, int i, int j, int k,
-                                            int rowlin, bool face) {
-    const int cx = q == 18 ? 0 : cx_of(q), cy = q == 18 ? 0 : cy_of(q), cz = q == 18 ? 0 : cz_of(q);
-    if (face) return F2(lat_load(L, g, q, i - cx, j - cy, k - cz), lat_load(L, g, q, i + 1 - cx, j - cy, k - cz));
-    const float* rp = L.pop[q] + (rowlin - cy * g.l - cz * (int)g.lm);
-    if (cx == 0) return F2(*reinterpret_cast<const float2*>(rp + (i - 1)));
-    // both loads stay inside the population for interior rows (see the stream-collide kernel)
-    float a = rp[i - 1 - cx], b = rp[i - cx];
-    if (cx == 1 && i == 1) a = L.ghost[(int64_t)q * g.G + g.gidx(0, j - cy, k - cz)];
-    if (cx == -1 && i + 1 == g.l) b = L.ghost[(int64_t)q * g.G + g.gidx(g.l + 1, j - cy, k - cz)];
-    return F2(a, b);
-}
-
-// Forward partial-bounce-back step, FP32, two nodes per thread (l even): the BGK collision
-// runs once on F2 values (packed FP32, each lane rounded as the one-node kernel, so the
-// bits are the same), and only pairs with n_s != 0 on either node pull the opposite
-// populations again for the mixing.  grid (ceil(np/128), m, n), pairs p0 .. p0+np-1.
-template <int MINB>
-__global__ void __launch_bounds__(128, MINB) k_pbb_pair(Lat<float, float> src, Lat<float, float> dst, Geo g,
-                                                        Phys<float> ph, const float* ns, int np) {
-    const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    if (t >= np) return;
-    const int i = 2 * t + 1, j = (int)blockIdx.y + 1, k = (int)blockIdx.z + 1;
-    const int rowlin = g.l * ((j - 1) + g.m * (k - 1));
-    const bool face = (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-    F2 x[19];
-#pragma unroll
-    for (int q = 0; q < 19; ++q) x[q] = pull_pair_f32(src, g, q, i, j, k, rowlin, face);
-    collide<F2>(x, F2(ph.omega), F2(ph.omega1), F2(ph.fgrad));
-    const float2 sv = *reinterpret_cast<const float2*>(ns + rowlin + (i - 1));
-    if (sv.x != 0.0f || sv.y != 0.0f) {
-        const F2 s(sv), s1 = F2(1.0f) - s;
-#pragma unroll
-        for (int q = 0; q < 19; ++q) x[q] = s1 * x[q] + s * pull_pair_f32(src, g, opp_of(q), i, j, k, rowlin, face);
-    }
-    if (i == 1) {
-#pragma unroll
-        for (int q = 0; q < 18; ++q) dst.xface[xface_idx(g, 0, q, j, k)] = x[q].v.x;
-    }
-    if (i + 1 == g.l) {
-#pragma unroll
-        for (int q = 0; q < 18; ++q) dst.xface[xface_idx(g, 1, q, j, k)] = x[q].v.y;
-    }
-#pragma unroll
-    for (int q = 0; q < 19; ++q) *reinterpret_cast<float2*>(dst.pop[q] + rowlin + (i - 1)) = x[q].v;
-}
-
-// Momentum the solid takes in the step, F = sum over voxels with n_s > 0 of 2 n_s j(x), j
-// the momentum of the pulled (pre-collision) populations, in FP64 over the list of those
-// voxels; written to series[(itime + 1) % cap] and the device step counter advanced (one
-// block at least, so an empty list records a zero force).
-template <typename R>
-__global__ void __launch_bounds__(256) k_pbb_force(Lat<R, R> src, Geo g, const R* ns, const int32_t* list,
-                                                   int64_t nlist, Reduce red, double* series, int64_t cap,
-                                                   int64_t* d_itime) {
+__global__ void __launch_bounds__(256) k_pbb_list(Lat<R, R> src, Lat<R, R> dst, Geo g, const R* ns,
+                                                  const int32_t* list, int64_t nlist, Reduce red, double* series,
+                                                  int64_t cap, int64_t* d_itime) {
     double f[3] = {0.0, 0.0, 0.0};
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nlist;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t lin = list[t];
-        const int i = (int)(lin % g.l) + 1, j = (int)((lin / g.l) % g.m) + 1, k = (int)(lin / g.lm) + 1;
+        const int32_t l32 = list[t];  // one lattice holds fewer than 2^31 nodes
+        const int64_t lin = l32;
+        const int row = l32 / g.l;
+        const int i = l32 - row * g.l + 1, j = row % g.m + 1, k = row / g.m + 1;
         const bool face = (i == 1) | (i == g.l) | (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-        double jx = 0.0, jy = 0.0, jz = 0.0;
+        // every load before the first store (the stores go to the lattice the BGK values are
+        // read from, so loads after them could not be issued ahead)
+        R pre[19], x[19];
+#pragma unroll
+        for (int q = 0; q < 18; ++q) pre[q] = pull_pre(src, g, q, i, j, k, lin, face);
+        pre[18] = src.pop[18][lin];
+#pragma unroll
+        for (int q = 0; q < 19; ++q) x[q] = dst.pop[q][lin];
+        const R s = ns[lin], s1 = R(1) - s;
+        if (series) {
+            double jx = 0.0, jy = 0.0, jz = 0.0;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                jx += (q == 18 ? 0 : cx_of(q)) * (double)pre[q];
+                jy += (q == 18 ? 0 : cy_of(q)) * (double)pre[q];
+                jz += (q == 18 ? 0 : cz_of(q)) * (double)pre[q];
+            }
+            f[0] += 2.0 * (double)s * jx;
+            f[1] += 2.0 * (double)s * jy;
+            f[2] += 2.0 * (double)s * jz;
+        }
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            const double v = (double)(q == 18 ? src.pop[18][lin] : pull_pre(src, g, q, i, j, k, lin, face));
-            jx += (q == 18 ? 0 : cx_of(q)) * v;
-            jy += (q == 18 ? 0 : cy_of(q)) * v;
-            jz += (q == 18 ? 0 : cz_of(q)) * v;
+            const R v = s1 * x[q] + s * pre[opp_of(q)];
+            dst.pop[q][lin] = v;
+            if (q < 18 && i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = v;
+            if (q < 18 && i == g.l) dst.xface[xface_idx(g, 1, q, j, k)] = v;
         }
-        const double s = (double)ns[lin];
-        f[0] += 2.0 * s * jx;
-        f[1] += 2.0 * s * jy;
-        f[2] += 2.0 * s * jz;
     }
-    block_reduce_store<3>(f, red, nullptr, series, cap, d_itime, 1, 1);
+    if (series) block_reduce_store<3>(f, red, nullptr, series, cap, d_itime, 1, 1);
+}
+
+// c_q . (x, y, z) with the zero components of c_q left out at compile time (q a constant
+// once the loops over q are unrolled): a product by a zero component is not folded away
+// under IEEE rules, and most of these products are by zero.
+template <typename R>
+__device__ __forceinline__ R cdot(int q, R x, R y, R z) {
+    const int c[3] = {q == 18 ? 0 : cx_of(q), q == 18 ? 0 : cy_of(q), q == 18 ? 0 : cz_of(q)};
+    const R v[3] = {x, y, z};
+    R acc = R(0);
+    bool any = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (c[d] == 0) continue;
+        const R term = c[d] > 0 ? v[d] : -v[d];
+        acc = any ? acc + term : term;
+        any = true;
+    }
+    return acc;
 }
 
 // Adjoint of one step: state f (entering the step, its halo shell holding the
 // halo values of that step), lam_in = adjoint of the state the step produced;
 // writes the adjoint of f (lam_out, pushed), the halo part of it (gmu, per
-// halo slot), and accumulates dJ/dn_s.  The pulled populations stay in registers;
-// lam_in is read in two passes over the 19 directions (the sums of the BGK
-// Jacobian's transpose first, then the pushed values, whose second read of the
-// node's 19 words comes from the cache), so one node fits in few registers and
-// many nodes are in flight per SM.  The BGK post-collision value needed by dJ/dn_s
-// is re-evaluated from rho and u.
-template <typename R, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_pbb_adjoint(Lat<R, R> f, Geo g, Phys<R> ph, const R* ns, Lat<R, R> lam_in,
-                                                     Lat<R, R> lam_out, R* gmu, double* grad, R gamma) {
-    for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.N;
-         lin += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(lin % g.l) + 1, j = (int)((lin / g.l) % g.m) + 1, k = (int)(lin / g.lm) + 1;
-        const bool face = (i == 1) | (i == g.l) | (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
-        R pre[19];
+// halo slot), and accumulates dJ/dn_s.  Everything the transpose of the BGK
+// Jacobian needs from lam comes from ten weighted moments of it (sum w lam,
+// sum w lam c_a, sum w lam c_a c_b) and sum lam c_x, and dJ/dn_s from sum lam f,
+// sum lam f_opp and the same moments (sum lam f_eq is quadratic in u), so each
+// direction costs a few signed additions instead of an equilibrium evaluation.
+// FACE: the node lies on one of the six boundary planes (its pulls and pushes may cross the
+// halo); the interior kernel is compiled without that code.
+template <typename R, bool FACE>
+__device__ __forceinline__ void adjoint_node(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, const R* ns,
+                                             const Lat<R, R>& lam_in, const Lat<R, R>& lam_out, R* gmu,
+                                             double* grad, R gamma, int i, int j, int k) {
+    {
+        const int64_t lin = (int64_t)(i - 1) + (int64_t)g.l * ((j - 1) + (int64_t)g.m * (k - 1));
+        constexpr bool face = FACE;
+        R pre[19], lam[19];
 #pragma unroll
         for (int q = 0; q < 18; ++q) pre[q] = pull_pre(f, g, q, i, j, k, lin, face);
         pre[18] = f.pop[18][lin];
-        const R s = ns[lin], s1 = R(1) - s;
-        R rho = R(0), jx = R(0), jy = R(0), jz = R(0);
 #pragma unroll
-        for (int q = 0; q < 19; ++q) {
+        for (int q = 0; q < 19; ++q) lam[q] = lam_in.pop[q][lin];
+        const R s = ns[lin], s1 = R(1) - s;
+        R rho = pre[0], jx = pre[0], jy = -pre[0], jz = R(0);
+        R lp = lam[0] * pre[0], lpo = lam[0] * pre[opp_of(0)];  // sum lam_q f_q, sum lam_q f_opp(q)
+#pragma unroll
+        for (int q = 1; q < 19; ++q) {
             rho += pre[q];
-            jx += R(cx_of(q)) * pre[q];
-            jy += R(cy_of(q)) * pre[q];
-            jz += R(cz_of(q)) * pre[q];
+            const int cx = q == 18 ? 0 : cx_of(q), cy = q == 18 ? 0 : cy_of(q), cz = q == 18 ? 0 : cz_of(q);
+            if (cx != 0) jx = cx > 0 ? jx + pre[q] : jx - pre[q];
+            if (cy != 0) jy = cy > 0 ? jy + pre[q] : jy - pre[q];
+            if (cz != 0) jz = cz > 0 ? jz + pre[q] : jz - pre[q];
+            lp += lam[q] * pre[q];
+            lpo += lam[q] * pre[opp_of(q)];
         }
         const R ux = jx / rho, uy = jy / rho, uz = jz / rho;
         const R usq = ux * ux + uy * uy + uz * uz;
-        const R frho = ph.fgrad * rho;
-        R gs = R(2) * gamma * jx;  // dJ/dn_s of this step
-        R A = R(0), Bx = R(0), By = R(0), Bz = R(0), Fx = R(0);
+        // moments of lam: sum lam c_a c_b (ab = xx, yy, zz, xy, xz, yz), sum lam c_a and sum lam
+        // over the axis (w = 1/18) and diagonal (w = 1/36) directions apart; c has components 0
+        // and +-1, so each is a signed sum
+        R m0[2] = {R(0), R(0)}, m1[2][3] = {}, m2[2][6] = {};
 #pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            const R lam = lam_in.pop[q][lin];
-            const R w = weight<R>(q);
-            const R cu = R(cx_of(q)) * ux + R(cy_of(q)) * uy + R(cz_of(q)) * uz;
-            const R feq = w * rho * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq);
-            const R bgk = ph.omega1 * pre[q] + ph.omega * feq + frho * R(cx_of(q));
-            gs += lam * (pre[opp_of(q)] - bgk);
-            const R nw = s1 * lam * w;
-            A += nw * (R(1) - R(4.5) * cu * cu + R(1.5) * usq);
-            const R b9 = nw * R(9) * cu;
-            Bx += nw * R(3) * (R(cx_of(q)) - ux) + b9 * R(cx_of(q));
-            By += nw * R(3) * (R(cy_of(q)) - uy) + b9 * R(cy_of(q));
-            Bz += nw * R(3) * (R(cz_of(q)) - uz) + b9 * R(cz_of(q));
-            Fx += s1 * lam * R(cx_of(q));
+        for (int q = 0; q < 18; ++q) {
+            const int cls = wclass_of(q) == 1 ? 0 : 1;
+            const int c[3] = {cx_of(q), cy_of(q), cz_of(q)};
+            const R v = lam[q];
+            m0[cls] += v;
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                if (c[d] != 0) m1[cls][d] = c[d] > 0 ? m1[cls][d] + v : m1[cls][d] - v;
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                if (c[d] != 0) m2[cls][d] += v;  // c_d^2 = 1
+            const int pr[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                const int cc = c[pr[e][0]] * c[pr[e][1]];
+                if (cc != 0) m2[cls][3 + e] = cc > 0 ? m2[cls][3 + e] + v : m2[cls][3 + e] - v;
+            }
         }
+        const R p0 = weight<R>(18), p1 = weight<R>(4), p2 = weight<R>(0);
+        const R L0 = p0 * lam[18] + p1 * m0[0] + p2 * m0[1];           // sum w lam
+        R L1[3], L2[6];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) L1[d] = p1 * m1[0][d] + p2 * m1[1][d];  // sum w lam c
+#pragma unroll
+        for (int e = 0; e < 6; ++e) L2[e] = p1 * m2[0][e] + p2 * m2[1][e];  // sum w lam c c
+        const R fxu = m1[0][0] + m1[1][0];                                  // sum lam c_x
+        const R uL1 = ux * L1[0] + uy * L1[1] + uz * L1[2];
+        const R L2u[3] = {L2[0] * ux + L2[3] * uy + L2[4] * uz, L2[3] * ux + L2[1] * uy + L2[5] * uz,
+                          L2[4] * ux + L2[5] * uy + L2[2] * uz};
+        const R uL2u = ux * L2u[0] + uy * L2u[1] + uz * L2u[2];
+        const R c15 = R(1.5) * usq;
+        // sum lam f_eq = rho (L0 (1 - 1.5 u^2) + 3 u.L1 + 4.5 u.L2.u); the step's BGK value is
+        // omega1 f + omega f_eq + fgrad rho c_x
+        const R lfeq = rho * (L0 * (R(1) - c15) + R(3) * uL1 + R(4.5) * uL2u);
+        const R lbgk = ph.omega1 * lp + ph.omega * lfeq + ph.fgrad * rho * fxu;
+        const R gs = R(2) * gamma * jx + (lpo - lbgk);  // dJ/dn_s of this step
+        // transpose of the BGK Jacobian through rho and u:
+        //   A = s1 sum w lam (1 - 4.5 (c.u)^2 + 1.5 u^2), B = s1 (3 (L1 - u L0) + 9 L2 u), Fx = s1 sum lam c_x
+        const R A = s1 * (L0 * (R(1) + c15) - R(4.5) * uL2u);
+        const R Bx = s1 * (R(3) * (L1[0] - ux * L0) + R(9) * L2u[0]);
+        const R By = s1 * (R(3) * (L1[1] - uy * L0) + R(9) * L2u[1]);
+        const R Bz = s1 * (R(3) * (L1[2] - uz * L0) + R(9) * L2u[2]);
+        const R Fx = s1 * fxu;
         grad[lin] += (double)gs;
         const R common = ph.omega * A + ph.fgrad * Fx;
         const R g2 = gamma * R(2) * s;
+        const R o1s1 = ph.omega1 * s1;
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            const R lam = lam_in.pop[q][lin], lam_o = lam_in.pop[opp_of(q)][lin];
-            const R mu = ph.omega1 * s1 * lam + common +
-                         ph.omega * (R(cx_of(q)) * Bx + R(cy_of(q)) * By + R(cz_of(q)) * Bz) +
-                         s * lam_o + g2 * R(cx_of(q));
+            const int cx = q == 18 ? 0 : cx_of(q), cy = q == 18 ? 0 : cy_of(q), cz = q == 18 ? 0 : cz_of(q);
+            R mu = o1s1 * lam[q] + common;
+            if (cx != 0 || cy != 0 || cz != 0) mu = mu + ph.omega * cdot<R>(q, Bx, By, Bz);
+            mu = mu + s * lam[opp_of(q)];
+            if (cx != 0) mu = cx > 0 ? mu + g2 : mu - g2;
             if (!face) {  // f_q(x) was pulled from the interior node x - c_q
-                lam_out.pop[q][lin - cx_of(q) - (int64_t)cy_of(q) * g.l - (int64_t)cz_of(q) * g.lm] = mu;
+                lam_out.pop[q][lin - cx - (int64_t)cy * g.l - (int64_t)cz * g.lm] = mu;
             } else {
-                const int si = i - cx_of(q), sj = j - cy_of(q), sk = k - cz_of(q);
+                const int si = i - cx, sj = j - cy, sk = k - cz;
                 if (g.interior(si, sj, sk)) lam_out.pop[q][g.lin(si, sj, sk)] = mu;
                 else gmu[(int64_t)q * g.G + g.gidx(si, sj, sk)] = mu;
                 // no interior node pulls f_q(x) when x + c_q is outside: start that slot at zero
-                if (!g.interior(i + cx_of(q), j + cy_of(q), k + cz_of(q))) lam_out.pop[q][lin] = R(0);
+                if (!g.interior(i + cx, j + cy, k + cz)) lam_out.pop[q][lin] = R(0);
             }
         }
     }
+}
+
+// Nodes with 2 <= i <= l-1, 2 <= j <= m-1, 2 <= k <= n-1, one per thread; grid
+// (ceil((l-2)/128), m-2, n-2): indices from the block coordinates, no halo code.
+template <typename R, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pbb_adjoint(Lat<R, R> f, Geo g, Phys<R> ph, const R* ns,
+                                                           Lat<R, R> lam_in, Lat<R, R> lam_out, R* gmu,
+                                                           double* grad, R gamma) {
+    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) + 2;
+    if (i > g.l - 1) return;
+    adjoint_node<R, false>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma, i, (int)blockIdx.y + 2,
+                           (int)blockIdx.z + 2);
+}
+
+// The rest: every node of the rows on the y/z boundary planes (face rows f < nfr, in the
+// order of face_row), then the columns i = 1 and i = l of the other rows.
+template <typename R>
+__global__ void __launch_bounds__(128) k_pbb_adjoint_faces(Lat<R, R> f, Geo g, Phys<R> ph, const R* ns,
+                                                           Lat<R, R> lam_in, Lat<R, R> lam_out, R* gmu,
+                                                           double* grad, R gamma, int nfr, int64_t nitems) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nitems) return;
+    int i, j, k;
+    if (t < (int64_t)nfr * g.l) {
+        const int fr = (int)(t / g.l);
+        i = (int)(t - (int64_t)fr * g.l) + 1;
+        face_row(g, fr, &j, &k);
+    } else {
+        const int sides = g.l == 1 ? 1 : 2;
+        const int u = (int)(t - (int64_t)nfr * g.l);
+        const int r = u / sides, side = u - r * sides;
+        j = r % (g.m - 2) + 2;
+        k = r / (g.m - 2) + 2;
+        i = side ? g.l : 1;
+    }
+    adjoint_node<R, true>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma, i, j, k);
 }
 
 // Halo values copied from interior populations: add their adjoints back, one
@@ -546,9 +578,14 @@ __global__ void k_adj_outflow(Geo g, const int32_t* jk, const int32_t* start, co
         const R w = weight<R>(q);
         for (int a3 = 0; a3 < 3; ++a3) psi[a3] += mu * w * (R(3) * c[a3] + R(1.5) * (R(6) * cJ * c[a3] - R(2) * J[a3]));
     }
+    // all 18 values of the node first, then the updated ones (a load after a store through
+    // another population's pointer would wait for it)
+    R old[18];
+#pragma unroll
+    for (int p = 0; p < 18; ++p) old[p] = lam_out.pop[p][lin];
 #pragma unroll
     for (int p = 0; p < 18; ++p)
-        lam_out.pop[p][lin] += R(cx_of(p)) * psi[0] + R(cy_of(p)) * psi[1] + R(cz_of(p)) * psi[2];
+        lam_out.pop[p][lin] = old[p] + (R(cx_of(p)) * psi[0] + R(cy_of(p)) * psi[1] + R(cz_of(p)) * psi[2]);
 }
 
 unsigned capped_grid(int64_t work, int tpb) {
@@ -564,38 +601,33 @@ template <typename R>
 void launch_pbb_step(const Lat<R, R>& src, const Lat<R, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
                      const int32_t* ns_list, int64_t ns_count, const Reduce& red, double* series, int64_t cap,
                      int64_t* d_itime, cudaStream_t st) {
-    if (series) {  // the force first: it reads the source lattice the step leaves unchanged
-        k_pbb_force<R><<<capped_grid(ns_count, 256), 256, 0, st>>>(src, g, ns, ns_list, ns_count, red, series, cap,
-                                                                    d_itime);
-    }
-    if constexpr (sizeof(R) == 4) {
-        bool aligned = true;
-        for (int q = 0; q < Q; ++q)
-            aligned = aligned && reinterpret_cast<uintptr_t>(src.pop[q]) % 8 == 0 &&
-                      reinterpret_cast<uintptr_t>(dst.pop[q]) % 8 == 0;
-        if (g.l % 2 == 0 && aligned && reinterpret_cast<uintptr_t>(ns) % 8 == 0) {
-            const int np = g.l / 2;
-            dim3 grid((np + 127) / 128, g.m, g.n);
-            k_pbb_pair<5><<<grid, 128, 0, st>>>(src, dst, g, ph, ns, np);
-            return;
-        }
-    }
-    k_pbb_step<R><<<capped_grid(g.N, 256), 256, 0, st>>>(src, dst, g, ph, ns);
+    launch_stream_collide<R, R>(src, dst, g, ph, 0, st);
+    k_pbb_list<R><<<capped_grid(ns_count, 256), 256, 0, st>>>(src, dst, g, ns, ns_list, ns_count, red, series, cap,
+                                                               d_itime);
 }
 
 template <typename R>
 void launch_pbb_adjoint(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
                         const Lat<R, R>& lam_out, R* gmu, double* grad, R gamma, const HaloAdjointDevice& t,
                         cudaStream_t st) {
-    // resident blocks of 256 per SM the registers are sized for: FP32 3 (80 registers), FP64 2
-    k_pbb_adjoint<R, sizeof(R) == 4 ? 3 : 2><<<capped_grid(g.N, 256), 256, 0, st>>>(f, g, ph, ns, lam_in, lam_out,
-                                                                                      gmu, grad, gamma);
+    // resident blocks of 128 per SM the registers are sized for: FP32 6 (80 registers), FP64 4
+    if (g.l > 2 && g.m > 2 && g.n > 2) {
+        const dim3 grid((unsigned)((g.l - 2 + 127) / 128), (unsigned)(g.m - 2), (unsigned)(g.n - 2));
+        k_pbb_adjoint<R, sizeof(R) == 4 ? 6 : 4><<<grid, 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma);
+    }
+    const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
+    const int nfr = nz * g.m + (g.n > 2 ? (g.n - 2) * ny : 0);
+    const int64_t inner_rows = (g.m > 2 && g.n > 2) ? (int64_t)(g.m - 2) * (g.n - 2) : 0;
+    const int64_t nitems = (int64_t)nfr * g.l + inner_rows * (g.l == 1 ? 1 : 2);
+    k_pbb_adjoint_faces<R><<<(unsigned)((nitems + 127) / 128), 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu, grad,
+                                                                              gamma, nfr, nitems);
     if (t.ncopy > 0)
-        k_adj_copy<R><<<(unsigned)((t.ncopy + 255) / 256), 256, 0, st>>>(g, t.copy_key, t.copy_start, t.copy_slot,
-                                                                          t.ncopy, gmu, lam_out);
+        // small blocks: a few thousand threads still spread over every SM
+        k_adj_copy<R><<<(unsigned)((t.ncopy + 63) / 64), 64, 0, st>>>(g, t.copy_key, t.copy_start, t.copy_slot,
+                                                                       t.ncopy, gmu, lam_out);
     if (t.nout > 0)
-        k_adj_outflow<R><<<(unsigned)((t.nout + 255) / 256), 256, 0, st>>>(g, t.out_jk, t.out_start, t.out_slot,
-                                                                            t.out_q, t.nout, gmu, f, lam_out);
+        k_adj_outflow<R><<<(unsigned)((t.nout + 63) / 64), 64, 0, st>>>(g, t.out_jk, t.out_start, t.out_slot,
+                                                                         t.out_q, t.nout, gmu, f, lam_out);
 }
 
 template void launch_pbb_step<float>(const Lat<float, float>&, const Lat<float, float>&, const Geo&,

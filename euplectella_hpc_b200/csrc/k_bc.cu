@@ -651,14 +651,16 @@ __global__ void k_gather(Lat<S, R> L, Geo g, int q, T* dst, int64_t total) {
 // x-face copy of the current lattice (after an upload): one thread per (j,k).
 template <typename S, typename R>
 __global__ void k_fill_xface(Lat<S, R> L, Geo g) {
+    // one thread per (side, q, j, k), j fastest: the stores are coalesced, and every load
+    // (a column of the lattice, stride l) is in flight at once
+    const int64_t mn = (int64_t)g.m * g.n;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int64_t)g.m * g.n) return;
-    const int j = (int)(t % g.m) + 1, k = (int)(t / g.m) + 1;
-#pragma unroll
-    for (int q = 0; q < 18; ++q) {
-        L.xface[xface_idx(g, 0, q, j, k)] = lat_load(L, g, q, 1, j, k);
-        L.xface[xface_idx(g, 1, q, j, k)] = lat_load(L, g, q, g.l, j, k);
-    }
+    if (t >= 36 * mn) return;
+    const int sq = (int)(t / mn);  // side * 18 + q
+    const int64_t jk = t - sq * mn;
+    const int side = sq / 18, q = sq - 18 * side;
+    const int j = (int)(jk % g.m) + 1, k = (int)(jk / g.m) + 1;
+    L.xface[t] = lat_load(L, g, q, side ? g.l : 1, j, k);
 }
 
 unsigned grid_for(int64_t work, int tpb, unsigned cap = 148u * 16u) {
@@ -781,7 +783,7 @@ void launch_bounce_drag(const Lat<S, R>& L, const Geo& g, const int bc[6], const
 
 template <typename S, typename R>
 void launch_fill_xface(const Lat<S, R>& L, const Geo& g, cudaStream_t st) {
-    const int64_t work = (int64_t)g.m * g.n;
+    const int64_t work = 36 * (int64_t)g.m * g.n;
     k_fill_xface<S, R><<<(unsigned)((work + kTpb - 1) / kTpb), kTpb, 0, st>>>(L, g);
 }
 

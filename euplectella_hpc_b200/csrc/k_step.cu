@@ -327,7 +327,11 @@ bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const
             if (reinterpret_cast<uintptr_t>(s0) % (2 * sizeof(S)) != 0) return false;
             if ((!dev || cx == 0) && reinterpret_cast<uintptr_t>(dst.pop[q]) % (2 * sizeof(S)) != 0) return false;
         }
-        const int bx = 128;
+        // blocks of at most 128 threads, the row's pairs split evenly over its blocks (a
+        // warp multiple), so short rows leave no idle threads (l = 192: one block of 96)
+        const int npr = part == kStreamInterior ? g.l / 2 - 2 : (part == kStreamFaces ? 0 : g.l / 2);
+        const int nblk = npr > 0 ? (npr + 127) / 128 : 1;
+        const int bx = npr > 0 ? ((npr + nblk - 1) / nblk + 31) / 32 * 32 : 128;
         PullBase<S> pb;
         for (int q = 0; q < Q; ++q) {
             const int64_t c = (q == 18) ? 0 : (int64_t)cy_of(q) * g.l + (int64_t)cz_of(q) * g.lm + cx_of(q);
@@ -336,8 +340,8 @@ bool launch_pair(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const
         if (part == kStreamFaces) {
             const int sides = g.l == 2 ? 1 : 2;
             const int64_t threads = (int64_t)sides * g.m * g.n;
-            k_stream_collide_pair_faces<S><<<(unsigned)((threads + bx - 1) / bx), bx, 0, st>>>(src, dst, g, ph, pb,
-                                                                                              sides);
+            k_stream_collide_pair_faces<S><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(src, dst, g, ph, pb,
+                                                                                             sides);
             return true;
         }
         // all pairs, or all but the first and last of each row
@@ -444,22 +448,8 @@ struct StagedPlan {
     float inv_l;          // 1/l (rows of a node offset, corrected to exact)
 };
 
-// Row (j, k) of face row index f: the planes k = 1 and k = n (all j), then j = 1 and j = m
-// of the planes k = 2 .. n-1.
-__device__ __forceinline__ void face_row(const Geo& g, int f, int* j, int* k) {
-    const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
-    if (f < nz * g.m) {
-        *k = f < g.m ? 1 : g.n;
-        *j = f % g.m + 1;
-    } else {
-        const int r = f - nz * g.m;
-        *k = 2 + r / ny;
-        *j = (r % ny == 0) ? 1 : g.m;
-    }
-}
-
-template <typename S>
-__global__ void __launch_bounds__(kStagedThreads, 3) k_stream_collide_staged(Lat<S, float> src, Lat<S, float> dst,
+template <typename S, int MINB>
+__global__ void __launch_bounds__(kStagedThreads, MINB) k_stream_collide_staged(Lat<S, float> src, Lat<S, float> dst,
                                                                               Geo g, Phys<float> ph, PullBase<S> pb,
                                                                               StagedPlan sp) {
     using V2 = Vec2<S>;
@@ -568,7 +558,7 @@ constexpr int kSmemPerSM = 228 * 1024;
 
 template <typename S>
 bool launch_staged(const Lat<S, float>& src, const Lat<S, float>& dst, const Geo& g, const Phys<float>& ph,
-                   cudaStream_t st) {
+                   int per_sm, cudaStream_t st) {
     if (g.l % 8 != 0 || g.l < 8) return false;
     StagedPlan sp;
     const int64_t plane_nodes = (int64_t)g.l * (g.m - 2);
@@ -579,9 +569,9 @@ bool launch_staged(const Lat<S, float>& src, const Lat<S, float>& dst, const Geo
     sp.nface = nz * g.m + (g.n > 2 ? (g.n - 2) * ny : 0);
     sp.inv_l = 1.0f / (float)g.l;
     const int stage_bytes = 19 * kTileNodes * (int)sizeof(S);
-    // three CTAs per SM, each with as many stages as fit (at most four)
+    // per_sm CTAs per SM (3: 72 registers, 2: no spills), each with as many stages as fit
     sp.stages = kStagedMaxStages;
-    while (sp.stages > 2 && 3 * (stage_bytes * sp.stages + 1024) > kSmemPerSM) --sp.stages;
+    while (sp.stages > 2 && per_sm * (stage_bytes * sp.stages + 1024) > kSmemPerSM) --sp.stages;
     // every run starts on a 16-byte boundary: the pull bases (a tile starts at a multiple of 8)
     PullBase<S> pb;
     for (int q = 0; q < Q; ++q) {
@@ -593,7 +583,10 @@ bool launch_staged(const Lat<S, float>& src, const Lat<S, float>& dst, const Geo
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return false;
     const size_t smem = (size_t)stage_bytes * sp.stages;
-    k_stream_collide_staged<S><<<(unsigned)(3 * sms), kStagedThreads, smem, st>>>(src, dst, g, ph, pb, sp);
+    if (per_sm == 2)
+        k_stream_collide_staged<S, 2><<<(unsigned)(2 * sms), kStagedThreads, smem, st>>>(src, dst, g, ph, pb, sp);
+    else
+        k_stream_collide_staged<S, 3><<<(unsigned)(3 * sms), kStagedThreads, smem, st>>>(src, dst, g, ph, pb, sp);
     return true;
 }
 
@@ -745,15 +738,17 @@ void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo
                            int variant, cudaStream_t st, int part) {
     // EUP_STEP_VARIANT bit 0: 16-byte vectors, bit 2: 8-byte vectors (when l allows), bit 3: one
     // node per thread, bits 4-6: occupancy target of the two-node kernel (n + 3 blocks per SM),
-    // bit 7: 16-bit storage without shared-memory staging; default: 16-bit storage staged
-    // (l a multiple of 8), otherwise two nodes per thread (FP32 arithmetic, l even).  A split step (interior columns,
+    // bit 7: 16-bit storage staged in shared memory by bulk copies (l a multiple of 8; with
+    // bit 11 two CTAs per SM instead of three); default: two nodes per thread (FP32
+    // arithmetic, l even), the pulls loaded into registers.  A split step (interior columns,
     // then the two x-face columns) uses the two-node or the one-node kernel.
     constexpr int VW = VecWidth<S>::value;
     if (part == kStreamAll) {
         if ((variant & 1) && launch_vec<S, R, VW>(src, dst, g, ph, st)) return;
         if ((variant & 4) && launch_vec<S, R, (VW / 2 > 0 ? VW / 2 : 1)>(src, dst, g, ph, st)) return;
-        if constexpr (DevStore<S>::value) {
-            if (!(variant & (8 | 128)) && launch_staged<S>(src, dst, g, ph, st)) return;
+        if constexpr (DevStore<S>::value) {  // opt-in: measured slower than the register pulls below
+            if ((variant & 128) && !(variant & 8) && launch_staged<S>(src, dst, g, ph, (variant & 2048) ? 2 : 3, st))
+                return;
         }
     }
     if (!(variant & 8) && launch_pair<S, R>(src, dst, g, ph, (variant >> 4) & 7, part, st)) return;
@@ -784,11 +779,12 @@ template void launch_stream_collide<__nv_bfloat16, float>(const Lat<__nv_bfloat1
 cudaError_t prepare_stream_collide() {
     // the staged kernels opt into more than 48 KB of dynamic shared memory (set once per
     // device, before any launch is captured into a graph)
-    cudaError_t e = cudaFuncSetAttribute(k_stream_collide_staged<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kStagedSmemLimit);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_stream_collide_staged<__nv_bfloat16>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmemLimit);
+    cudaError_t e = cudaSuccess;
+    const void* ks[] = {(const void*)k_stream_collide_staged<__half, 2>, (const void*)k_stream_collide_staged<__half, 3>,
+                        (const void*)k_stream_collide_staged<__nv_bfloat16, 2>,
+                        (const void*)k_stream_collide_staged<__nv_bfloat16, 3>};
+    for (const void* k : ks)
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmemLimit);
     return e;
 }
 

@@ -174,6 +174,21 @@ struct Geo {
     }
 };
 
+// Row (j, k) of face row index f, 0 <= f < nz m + (n-2) ny (nz = 2 for n >= 2, else 1;
+// ny = 2 for m >= 2, else 1): the rows on the y/z boundary planes, first the planes k = 1
+// and k = n (all j), then j = 1 and j = m of the planes k = 2 .. n-1.
+__host__ __device__ __forceinline__ void face_row(const Geo& g, int f, int* j, int* k) {
+    const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
+    if (f < nz * g.m) {
+        *k = f < g.m ? 1 : g.n;
+        *j = f % g.m + 1;
+    } else {
+        const int r = f - nz * g.m;
+        *k = 2 + r / ny;
+        *j = (r % ny == 0) ? 1 : g.m;
+    }
+}
+
 // Pointers of one lattice (19 population arrays) plus the halo shell and the
 // x-face copy.  The x-face copy holds, for the interior columns x = 1 (side 0)
 // and x = l (side 1), the 18 moving populations exactly as a load from the

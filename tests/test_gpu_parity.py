@@ -329,9 +329,8 @@ def test_deviation_storage_against_fp64(eup, require_gpu, prec):
 
 @pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16", "bf16"])
 def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
-    """Two nodes per thread (default for 32-bit storage, at several occupancies; for 16-bit
-    storage the default stages the pulls in shared memory, variant 128 loads them into
-    registers) vs one node per thread vs 16-byte and 8-byte vectorised stream-collide, CUDA
+    """Two nodes per thread (default, at several occupancies; for 16-bit storage variant 128
+    stages the pulls in shared memory instead of registers) vs one node per thread vs 16-byte and 8-byte vectorised stream-collide, CUDA
     graphs vs plain launches: all paths give the same bits in every storage format."""
     l, m, n = 256, 20, 13
     code = {"fp32": eup.FP32, "fp64": eup.FP64, "fp16": eup.FP16_DEV, "bf16": eup.BF16_DEV}[prec]

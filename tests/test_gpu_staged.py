@@ -1,9 +1,9 @@
 """The staged 16-bit stream-collide kernel (pulls brought into shared memory by bulk
-asynchronous copies, a ring of stages per persistent CTA) against the register-pull
-two-node kernel (EUP_STEP_VARIANT=128), bit for bit, over lattice shapes that exercise
-its tiling: rows per tile clamped to the interior rows, partial last tiles, one interior
-row or plane, no interior rows at all (every row on a y/z boundary plane), 384 and 512
-threads per CTA, and tiles of 256 pairs (idle threads)."""
+asynchronous copies, a ring of stages per persistent CTA; EUP_STEP_VARIANT=128, and 2176
+for two CTAs per SM instead of three) against the register-pull two-node kernel (the
+default), bit for bit, over lattice shapes that exercise its tiling: 512-node tiles that
+cross rows, partial last tiles of a plane, one interior row or plane, no interior rows at
+all (every row on a y/z boundary plane), rows shorter and longer than a tile."""
 import numpy as np
 import pytest
 
@@ -31,7 +31,7 @@ def test_staged_equals_register_pull(eup, require_gpu, monkeypatch, prec, shape,
     a = eup.init_equilibrium(l, m, n, 0.05, 1e-3, 5, np.float64)
     cfg = eup.Config(l, m, n, bc=bc, svisc=0.01, u_inflow=0.05 if bc[0] == 5 else 0.0, precision=code)
     res = []
-    for var in ("0", "128"):
+    for var in ("128", "0", "2176"):
         monkeypatch.setenv("EUP_STEP_VARIANT", var)
         with eup.Solver(cfg) as s:
             s.set_obstacles(obs)
@@ -39,5 +39,6 @@ def test_staged_equals_register_pull(eup, require_gpu, monkeypatch, prec, shape,
             s.step(9)
             s.synchronize()
             res.append((s.download(np.float64), s.force_series(0, 10)))
-    assert np.array_equal(res[0][0], res[1][0])
-    assert np.array_equal(res[0][1], res[1][1])
+    for got, f in res[1:]:
+        assert np.array_equal(res[0][0], got)
+        assert np.array_equal(res[0][1], f)
