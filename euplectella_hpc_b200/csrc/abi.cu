@@ -156,17 +156,14 @@ int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
     const Lat<S, R> src = make_lat<S, R>(h, src_idx), dst = make_lat<S, R>(h, src_idx ^ 1);
     int n = 0;
     if (pe) pe->mark(4 * s + 0, h->stream);
-    if constexpr (std::is_same<S, R>::value) {
-        if (h->pbb) {  // partial bounce-back: halo planes, then stream + PBB collide (force of the step)
-            if (pe) pe->mark(4 * s + 1, h->stream);
-            n += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
-            if (pe) pe->mark(4 * s + 2, h->stream);
-            launch_pbb_step<R>(src, dst, h->g, ph, static_cast<const R*>(h->ns), h->ns_list, h->ns_count,
-                               make_reduce(h), h->series, h->cap,
-                               h->d_itime, h->stream);
-            if (pe) pe->mark(4 * s + 3, h->stream);
-            return n + 1;
-        }
+    if (h->pbb) {  // partial bounce-back: halo planes, stream-collide, mixing and force of the step
+        if (pe) pe->mark(4 * s + 1, h->stream);
+        n += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
+        if (pe) pe->mark(4 * s + 2, h->stream);
+        launch_pbb_step<S, R>(src, dst, h->g, ph, static_cast<const R*>(h->ns), h->ns_list, h->ns_count,
+                              make_reduce(h), h->series, h->cap, h->d_itime, h->stream);
+        if (pe) pe->mark(4 * s + 3, h->stream);
+        return n + 2;
     }
     // boundaries: bounce-back then halo planes (CODE/SRC/boundaries.F90:36-49,235-248)
     launch_bounce_drag<S, R>(src, h->g, bc, h->blist, h->blinks, h->nblist, true, make_reduce(h), h->series,
@@ -1214,10 +1211,10 @@ cudaError_t upload_vec(DevBuf<T>& b, const std::vector<T>& v) {
 }
 
 // Lattice view of an arbitrary state buffer laid out like the handle's lattices.
-template <typename R>
-Lat<R, R> lat_at(const eup_handle* h, R* base, R* shell = nullptr) {
-    Lat<R, R> L = make_lat<R, R>(h, 0);
-    for (int q = 0; q < Q; ++q) L.pop[q] = pop_ptr<R>(h, base, q);
+template <typename S, typename R>
+Lat<S, R> lat_at(const eup_handle* h, S* base, R* shell = nullptr) {
+    Lat<S, R> L = make_lat<S, R>(h, 0);
+    for (int q = 0; q < Q; ++q) L.pop[q] = pop_ptr<S>(h, base, q);
     if (shell) L.ghost = shell;
     return L;
 }
@@ -1311,7 +1308,7 @@ void revolve_schedule(int a, int b, int slot_a, std::vector<int>& free, std::vec
 // forward or adjoint step the halo blocks run on the working state (its halo follows from
 // it: configurations whose halo holds older values are refused), writing a working halo
 // shell that starts as a copy of the handle's (its never-written slots are constant).
-template <typename R>
+template <typename S, typename R>
 int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, double* grad_out, double* stats) {
     const Geo& g = h->g;
     const int T = ac->nsteps, A = ac->avg_steps;
@@ -1369,7 +1366,8 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     const size_t shell = (size_t)Q * g.G;
     const size_t xfs = (size_t)2 * 18 * g.m * g.n;
     const int nbuf = slots + 2;
-    DevBuf<R> bufs, xfaces, lam, gmu, wshell;
+    DevBuf<S> bufs;
+    DevBuf<R> xfaces, lam, gmu, wshell;
     DevBuf<double> grad;
     CK(h, bufs.alloc(state * nbuf));
     CK(h, xfaces.alloc(xfs * nbuf));
@@ -1381,12 +1379,12 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     CK(h, cudaMemsetAsync(lam.p, 0, sizeof(R) * state * 2, st));
     const Reduce red = make_reduce(h);
     auto buf_lat = [&](int b) {
-        Lat<R, R> L = lat_at<R>(h, bufs.p + state * b, wshell.p);
+        Lat<S, R> L = lat_at<S, R>(h, bufs.p + state * b, wshell.p);
         L.xface = xfaces.p + xfs * b;
         return L;
     };
     auto keep = [&](int b) -> cudaError_t {  // the handle's current state (and x-face copy) into buffer b
-        cudaError_t e = cudaMemcpyAsync(bufs.p + state * b, h->lat[h->cur], sizeof(R) * state,
+        cudaError_t e = cudaMemcpyAsync(bufs.p + state * b, h->lat[h->cur], sizeof(S) * state,
                                         cudaMemcpyDeviceToDevice, st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(xfaces.p + xfs * b, h->xface, sizeof(R) * xfs, cudaMemcpyDeviceToDevice, st);
@@ -1402,9 +1400,9 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     for (int s = 0; s < T; ++s) {
         if (store_at[(size_t)s] >= 0) CK(h, keep(store_at[(size_t)s]));
         if (s == T - 1) CK(h, keep(w0));
-        const Lat<R, R> src = make_lat<R, R>(h, h->cur), dst = make_lat<R, R>(h, h->cur ^ 1);
-        launch_bc<R, R>(src, g, bc, ph, st);
-        launch_pbb_step<R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, h->series, h->cap, h->d_itime, st);
+        const Lat<S, R> src = make_lat<S, R>(h, h->cur), dst = make_lat<S, R>(h, h->cur ^ 1);
+        launch_bc<S, R>(src, g, bc, ph, st);
+        launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, h->series, h->cap, h->d_itime, st);
         h->cur ^= 1;
         h->itime += 1;
     }
@@ -1434,16 +1432,16 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
             const int target = (a + 1 < acts.size() && acts[a + 1].kind == kActSnapshot) ? acts[a + 1].arg : -1;
             for (int s = 0; s < act.arg; ++s) {
                 const int next = (s + 1 == act.arg && target >= 0) ? target : (cur == w0 ? w1 : w0);
-                const Lat<R, R> src = buf_lat(cur), dst = buf_lat(next);
-                launch_bc<R, R>(src, g, bc, ph, st);
-                launch_pbb_step<R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
+                const Lat<S, R> src = buf_lat(cur), dst = buf_lat(next);
+                launch_bc<S, R>(src, g, bc, ph, st);
+                launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
                 cur = next;
                 ++recomputed;
             }
             if (target >= 0) ++a;  // the store is done
         } else if (act.kind == kActSnapshot) {
             if (cur != act.arg) {  // not reached in these schedules: a store always follows a forward step
-                CK(h, cudaMemcpyAsync(bufs.p + state * act.arg, bufs.p + state * cur, sizeof(R) * state,
+                CK(h, cudaMemcpyAsync(bufs.p + state * act.arg, bufs.p + state * cur, sizeof(S) * state,
                                       cudaMemcpyDeviceToDevice, st));
                 CK(h, cudaMemcpyAsync(xfaces.p + xfs * act.arg, xfaces.p + xfs * cur, sizeof(R) * xfs,
                                       cudaMemcpyDeviceToDevice, st));
@@ -1453,11 +1451,12 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
             cur = act.arg;  // read in place; forward steps write elsewhere
         } else {  // adjoint of step t from state t-1
             const int t = act.arg;
-            const Lat<R, R> f = buf_lat(cur);
-            launch_bc<R, R>(f, g, bc, ph, st);  // the halo of step t, from state t-1
-            const Lat<R, R> lin_ = lat_at<R>(h, lam.p + state * cur_lam), lout = lat_at<R>(h, lam.p + state * (cur_lam ^ 1));
+            const Lat<S, R> f = buf_lat(cur);
+            launch_bc<S, R>(f, g, bc, ph, st);  // the halo of step t, from state t-1
+            const Lat<R, R> lin_ = lat_at<R, R>(h, lam.p + state * cur_lam),
+                            lout = lat_at<R, R>(h, lam.p + state * (cur_lam ^ 1));
             const R gam = (t > T - A) ? (R)gamma : R(0);
-            launch_pbb_adjoint<R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st);
+            launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st);
             cur_lam ^= 1;
         }
     }
@@ -1476,7 +1475,7 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
         stats[2] = (double)recomputed;
         stats[3] = slots;
         stats[4] = revolve_repetition(T, slots);
-        stats[5] = (double)(sizeof(R) * ((state + xfs) * (size_t)nbuf + state * 2 + shell * 2));
+        stats[5] = (double)(sizeof(S) * state * (size_t)nbuf + sizeof(R) * (xfs * (size_t)nbuf + state * 2 + shell * 2));
         stats[6] = T;
         stats[7] = A;
     }
@@ -1501,8 +1500,6 @@ int eup_set_solid_fraction(eup_handle* h, const double* ns) {
         h->pbb = false;
         return EUP_OK;
     }
-    if (h->prec != EUP_FP32 && h->prec != EUP_FP64)
-        return fail(h, EUP_ERR_UNSUPPORTED, "eup_set_solid_fraction: the partial-bounce-back model runs in FP32 or FP64");
     if (has_exchange_face(h))
         return fail(h, EUP_ERR_UNSUPPORTED, "eup_set_solid_fraction: not offered on an x-slab lattice");
     if (h->nblist > 0 || h->bits)
@@ -1546,8 +1543,12 @@ int eup_adjoint_run(eup_handle* h, const eup_adjoint_config* cfg, double* object
         return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: need 1 <= avg_steps <= nsteps, checkpoints >= 0");
     if (!(h->cfg.cd_rho0 > 0 && h->cfg.cd_uref != 0 && h->cfg.cd_length > 0 && h->cfg.cd_span > 0))
         return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: drag normalisation not set in eup_config");
-    if (h->prec == EUP_FP64) return adjoint_run<double>(h, cfg, objective, grad_ns, stats);
-    return adjoint_run<float>(h, cfg, objective, grad_ns, stats);
+    switch (h->prec) {
+        case EUP_FP64: return adjoint_run<double, double>(h, cfg, objective, grad_ns, stats);
+        case EUP_FP16_DEV: return adjoint_run<__half, float>(h, cfg, objective, grad_ns, stats);
+        case EUP_BF16_DEV: return adjoint_run<__nv_bfloat16, float>(h, cfg, objective, grad_ns, stats);
+        default: return adjoint_run<float, float>(h, cfg, objective, grad_ns, stats);
+    }
 }
 
 }  // extern "C"

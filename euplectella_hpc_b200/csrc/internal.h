@@ -221,15 +221,19 @@ struct HaloAdjointDevice {
 // Returns EUP_OK or EUP_ERR_UNSUPPORTED (err says why).
 int build_halo_adjoint_tables(const Geo& g, const int bc[6], HaloAdjointTables* out, std::string* err);
 
-// One partial-bounce-back step src -> dst; with `series` the FP64 force of the step (over the
-// ns_count voxels of ns_list, those with n_s > 0) goes to series[(itime + 1) % cap] and the
-// device step counter advances; series == nullptr skips it (recomputation in the adjoint).
-template <typename R>
-void launch_pbb_step(const Lat<R, R>& src, const Lat<R, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
+// One partial-bounce-back step src -> dst (any storage; FP32 arithmetic for 16-bit storage):
+// the plain stream-collide, then the mixing f* = (1 - n_s) BGK(f) + n_s f_opp on the ns_count
+// voxels of ns_list (those with n_s > 0).  With `series` the FP64 force of the step goes to
+// series[(itime + 1) % cap] and the device step counter advances; series == nullptr skips it
+// (recomputation in the adjoint).
+template <typename S, typename R>
+void launch_pbb_step(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
                      const int32_t* ns_list, int64_t ns_count, const Reduce& red, double* series, int64_t cap,
                      int64_t* d_itime, cudaStream_t st);
-template <typename R>
-void launch_pbb_adjoint(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
+// Adjoint of one partial-bounce-back step from state f (its halo shell holding the step's
+// halo values); the adjoint fields lam are in the arithmetic type.
+template <typename S, typename R>
+void launch_pbb_adjoint(const Lat<S, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
                         const Lat<R, R>& lam_out, R* gmu, double* grad, R gamma, const HaloAdjointDevice& t,
                         cudaStream_t st);
 

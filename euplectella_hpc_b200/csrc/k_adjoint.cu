@@ -314,11 +314,47 @@ int build_halo_adjoint_tables(const Geo& g, const int bc[6], HaloAdjointTables* 
 // ---------------------------------------------------------------------------
 namespace {
 
+// Values of a state stored as S, worked on in R: the populations f themselves (FP32/FP64
+// storage), or for 16-bit storage the scaled deviations D = (f - w) S in the step kernels
+// ("kernel values", as the stream-collide kernels use them) and f in the adjoint.
+template <typename S, typename R>
+struct PState {
+    static constexpr bool dev = DevStore<S>::value;
+    static __device__ __forceinline__ R kval(S raw) {
+        if constexpr (dev) return DevStore<S>::to_f(raw);
+        else return raw;
+    }
+    static __device__ __forceinline__ S kstore(R v) {
+        if constexpr (dev) return DevStore<S>::from_f(v);
+        else return v;
+    }
+    // kernel value of population q pulled to node (i, j, k) (linear index lin)
+    static __device__ __forceinline__ R pull_k(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k,
+                                               int64_t lin, bool face) {
+        if (!face) return kval(L.pop[q][lin - cx_of(q) - (int64_t)cy_of(q) * g.l - (int64_t)cz_of(q) * g.lm]);
+        const int si = i - cx_of(q), sj = j - cy_of(q), sk = k - cz_of(q);
+        if (g.interior(si, sj, sk)) return kval(L.pop[q][g.lin(si, sj, sk)]);
+        const R f = L.ghost[(int64_t)q * g.G + g.gidx(si, sj, sk)];
+        if constexpr (dev) return (f - weight<R>(q)) * L.scale;
+        else return f;
+    }
+    // population f_q pulled to node (i, j, k)
+    static __device__ __forceinline__ R pull_f(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k,
+                                               int64_t lin, bool face) {
+        if (!face)
+            return Store<S, R>::load(L.pop[q][lin - cx_of(q) - (int64_t)cy_of(q) * g.l - (int64_t)cz_of(q) * g.lm], q,
+                                     L.inv_scale);
+        return lat_load(L, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
+    }
+    static __device__ __forceinline__ R f_of(const Lat<S, R>& L, int q, int64_t lin) {
+        return Store<S, R>::load(L.pop[q][lin], q, L.inv_scale);
+    }
+};
+
 template <typename R>
 __device__ __forceinline__ R pull_pre(const Lat<R, R>& L, const Geo& g, int q, int i, int j, int k, int64_t lin,
                                       bool face) {
-    if (!face) return L.pop[q][lin - cx_of(q) - (int64_t)cy_of(q) * g.l - (int64_t)cz_of(q) * g.lm];
-    return lat_load(L, g, q, i - cx_of(q), j - cy_of(q), k - cz_of(q));
+    return PState<R, R>::pull_f(L, g, q, i, j, k, lin, face);
 }
 
 // The partial-bounce-back step is the plain stream-collide (every node's BGK value, the
@@ -329,10 +365,11 @@ __device__ __forceinline__ R pull_pre(const Lat<R, R>& L, const Geo& g, int q, i
 // momentum the solid takes, F = sum 2 n_s j(x) over the list, j the momentum of the pulled
 // populations, in FP64 into series[(itime + 1) % cap], advancing the device step counter
 // (one block at least, so an empty list records a zero force).
-template <typename R>
-__global__ void __launch_bounds__(256) k_pbb_list(Lat<R, R> src, Lat<R, R> dst, Geo g, const R* ns,
+template <typename S, typename R>
+__global__ void __launch_bounds__(256) k_pbb_list(Lat<S, R> src, Lat<S, R> dst, Geo g, const R* ns,
                                                   const int32_t* list, int64_t nlist, Reduce red, double* series,
                                                   int64_t cap, int64_t* d_itime) {
+    using P = PState<S, R>;
     double f[3] = {0.0, 0.0, 0.0};
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nlist;
          t += (int64_t)gridDim.x * blockDim.x) {
@@ -342,13 +379,14 @@ __global__ void __launch_bounds__(256) k_pbb_list(Lat<R, R> src, Lat<R, R> dst, 
         const int i = l32 - row * g.l + 1, j = row % g.m + 1, k = row / g.m + 1;
         const bool face = (i == 1) | (i == g.l) | (j == 1) | (j == g.m) | (k == 1) | (k == g.n);
         // every load before the first store (the stores go to the lattice the BGK values are
-        // read from, so loads after them could not be issued ahead)
+        // read from, so loads after them could not be issued ahead); kernel values: f, or the
+        // deviations D for 16-bit storage, where the mixing is the same (w_q = w_opp(q))
         R pre[19], x[19];
 #pragma unroll
-        for (int q = 0; q < 18; ++q) pre[q] = pull_pre(src, g, q, i, j, k, lin, face);
-        pre[18] = src.pop[18][lin];
+        for (int q = 0; q < 18; ++q) pre[q] = P::pull_k(src, g, q, i, j, k, lin, face);
+        pre[18] = P::kval(src.pop[18][lin]);
 #pragma unroll
-        for (int q = 0; q < 19; ++q) x[q] = dst.pop[q][lin];
+        for (int q = 0; q < 19; ++q) x[q] = P::kval(dst.pop[q][lin]);
         const R s = ns[lin], s1 = R(1) - s;
         if (series) {
             double jx = 0.0, jy = 0.0, jz = 0.0;
@@ -358,16 +396,21 @@ __global__ void __launch_bounds__(256) k_pbb_list(Lat<R, R> src, Lat<R, R> dst, 
                 jy += (q == 18 ? 0 : cy_of(q)) * (double)pre[q];
                 jz += (q == 18 ? 0 : cz_of(q)) * (double)pre[q];
             }
-            f[0] += 2.0 * (double)s * jx;
-            f[1] += 2.0 * (double)s * jy;
-            f[2] += 2.0 * (double)s * jz;
+            // sum_q c_q w_q = 0: the momentum of the deviations is the momentum
+            const double js = P::dev ? 1.0 / (double)src.scale : 1.0;
+            f[0] += 2.0 * (double)s * (jx * js);
+            f[1] += 2.0 * (double)s * (jy * js);
+            f[2] += 2.0 * (double)s * (jz * js);
         }
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            const R v = s1 * x[q] + s * pre[opp_of(q)];
+            const S v = P::kstore(s1 * x[q] + s * pre[opp_of(q)]);
             dst.pop[q][lin] = v;
-            if (q < 18 && i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = v;
-            if (q < 18 && i == g.l) dst.xface[xface_idx(g, 1, q, j, k)] = v;
+            if (q < 18 && (i == 1 || i == g.l)) {
+                const R fv = Store<S, R>::load(v, q, dst.inv_scale);  // what a later load returns
+                if (i == 1) dst.xface[xface_idx(g, 0, q, j, k)] = fv;
+                if (i == g.l) dst.xface[xface_idx(g, 1, q, j, k)] = fv;
+            }
         }
     }
     if (series) block_reduce_store<3>(f, red, nullptr, series, cap, d_itime, 1, 1);
@@ -402,8 +445,8 @@ __device__ __forceinline__ R cdot(int q, R x, R y, R z) {
 // direction costs a few signed additions instead of an equilibrium evaluation.
 // FACE: the node lies on one of the six boundary planes (its pulls and pushes may cross the
 // halo); the interior kernel is compiled without that code.
-template <typename R, bool FACE>
-__device__ __forceinline__ void adjoint_node(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, const R* ns,
+template <typename S, typename R, bool FACE>
+__device__ __forceinline__ void adjoint_node(const Lat<S, R>& f, const Geo& g, const Phys<R>& ph, const R* ns,
                                              const Lat<R, R>& lam_in, const Lat<R, R>& lam_out, R* gmu,
                                              double* grad, R gamma, int i, int j, int k) {
     {
@@ -411,8 +454,8 @@ __device__ __forceinline__ void adjoint_node(const Lat<R, R>& f, const Geo& g, c
         constexpr bool face = FACE;
         R pre[19], lam[19];
 #pragma unroll
-        for (int q = 0; q < 18; ++q) pre[q] = pull_pre(f, g, q, i, j, k, lin, face);
-        pre[18] = f.pop[18][lin];
+        for (int q = 0; q < 18; ++q) pre[q] = PState<S, R>::pull_f(f, g, q, i, j, k, lin, face);
+        pre[18] = PState<S, R>::f_of(f, 18, lin);
 #pragma unroll
         for (int q = 0; q < 19; ++q) lam[q] = lam_in.pop[q][lin];
         const R s = ns[lin], s1 = R(1) - s;
@@ -504,20 +547,20 @@ __device__ __forceinline__ void adjoint_node(const Lat<R, R>& f, const Geo& g, c
 
 // Nodes with 2 <= i <= l-1, 2 <= j <= m-1, 2 <= k <= n-1, one per thread; grid
 // (ceil((l-2)/128), m-2, n-2): indices from the block coordinates, no halo code.
-template <typename R, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_pbb_adjoint(Lat<R, R> f, Geo g, Phys<R> ph, const R* ns,
+template <typename S, typename R, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_pbb_adjoint(Lat<S, R> f, Geo g, Phys<R> ph, const R* ns,
                                                            Lat<R, R> lam_in, Lat<R, R> lam_out, R* gmu,
                                                            double* grad, R gamma) {
     const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) + 2;
     if (i > g.l - 1) return;
-    adjoint_node<R, false>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma, i, (int)blockIdx.y + 2,
+    adjoint_node<S, R, false>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma, i, (int)blockIdx.y + 2,
                            (int)blockIdx.z + 2);
 }
 
 // The rest: every node of the rows on the y/z boundary planes (face rows f < nfr, in the
 // order of face_row), then the columns i = 1 and i = l of the other rows.
-template <typename R>
-__global__ void __launch_bounds__(128) k_pbb_adjoint_faces(Lat<R, R> f, Geo g, Phys<R> ph, const R* ns,
+template <typename S, typename R>
+__global__ void __launch_bounds__(128) k_pbb_adjoint_faces(Lat<S, R> f, Geo g, Phys<R> ph, const R* ns,
                                                            Lat<R, R> lam_in, Lat<R, R> lam_out, R* gmu,
                                                            double* grad, R gamma, int nfr, int64_t nitems) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -535,7 +578,7 @@ __global__ void __launch_bounds__(128) k_pbb_adjoint_faces(Lat<R, R> f, Geo g, P
         k = r / (g.m - 2) + 2;
         i = side ? g.l : 1;
     }
-    adjoint_node<R, true>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma, i, j, k);
+    adjoint_node<S, R, true>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma, i, j, k);
 }
 
 // Halo values copied from interior populations: add their adjoints back, one
@@ -555,9 +598,9 @@ __global__ void k_adj_copy(Geo g, const int64_t* key, const int32_t* start, cons
 // Outflow halo values (equilibria of the momentum of x = l,
 // CODE/SRC/bcond.bc.F90:138-165): propagate their adjoints to the 18 moving
 // populations of the node they were computed from.
-template <typename R>
+template <typename S, typename R>
 __global__ void k_adj_outflow(Geo g, const int32_t* jk, const int32_t* start, const int64_t* slot, const int8_t* qo,
-                              int64_t nsrc, const R* gmu, Lat<R, R> f, Lat<R, R> lam_out) {
+                              int64_t nsrc, const R* gmu, Lat<S, R> f, Lat<R, R> lam_out) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nsrc) return;
     const int j = jk[t] % g.m + 1, k = jk[t] / g.m + 1;
@@ -565,7 +608,7 @@ __global__ void k_adj_outflow(Geo g, const int32_t* jk, const int32_t* start, co
     R J[3] = {R(0), R(0), R(0)};
     R a[18];
 #pragma unroll
-    for (int q = 0; q < 18; ++q) a[q] = f.pop[q][lin];
+    for (int q = 0; q < 18; ++q) a[q] = PState<S, R>::f_of(f, q, lin);
     J[0] = a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13];
     J[1] = a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17];
     J[2] = a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15];
@@ -597,50 +640,51 @@ unsigned capped_grid(int64_t work, int tpb) {
 
 }  // namespace
 
-template <typename R>
-void launch_pbb_step(const Lat<R, R>& src, const Lat<R, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
+template <typename S, typename R>
+void launch_pbb_step(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, const Phys<R>& ph, const R* ns,
                      const int32_t* ns_list, int64_t ns_count, const Reduce& red, double* series, int64_t cap,
                      int64_t* d_itime, cudaStream_t st) {
-    launch_stream_collide<R, R>(src, dst, g, ph, 0, st);
-    k_pbb_list<R><<<capped_grid(ns_count, 256), 256, 0, st>>>(src, dst, g, ns, ns_list, ns_count, red, series, cap,
-                                                               d_itime);
+    launch_stream_collide<S, R>(src, dst, g, ph, 0, st);
+    k_pbb_list<S, R><<<capped_grid(ns_count, 256), 256, 0, st>>>(src, dst, g, ns, ns_list, ns_count, red, series,
+                                                                  cap, d_itime);
 }
 
-template <typename R>
-void launch_pbb_adjoint(const Lat<R, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
+template <typename S, typename R>
+void launch_pbb_adjoint(const Lat<S, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
                         const Lat<R, R>& lam_out, R* gmu, double* grad, R gamma, const HaloAdjointDevice& t,
                         cudaStream_t st) {
-    // resident blocks of 128 per SM the registers are sized for: FP32 6 (80 registers), FP64 4
+    // resident blocks of 128 per SM the registers are sized for: FP32 arithmetic 6 (80
+    // registers), FP64 4
     if (g.l > 2 && g.m > 2 && g.n > 2) {
         const dim3 grid((unsigned)((g.l - 2 + 127) / 128), (unsigned)(g.m - 2), (unsigned)(g.n - 2));
-        k_pbb_adjoint<R, sizeof(R) == 4 ? 6 : 4><<<grid, 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu, grad, gamma);
+        k_pbb_adjoint<S, R, sizeof(R) == 4 ? 6 : 4><<<grid, 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu, grad,
+                                                                           gamma);
     }
     const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
     const int nfr = nz * g.m + (g.n > 2 ? (g.n - 2) * ny : 0);
     const int64_t inner_rows = (g.m > 2 && g.n > 2) ? (int64_t)(g.m - 2) * (g.n - 2) : 0;
     const int64_t nitems = (int64_t)nfr * g.l + inner_rows * (g.l == 1 ? 1 : 2);
-    k_pbb_adjoint_faces<R><<<(unsigned)((nitems + 127) / 128), 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu, grad,
-                                                                              gamma, nfr, nitems);
+    k_pbb_adjoint_faces<S, R><<<(unsigned)((nitems + 127) / 128), 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu,
+                                                                                 grad, gamma, nfr, nitems);
     if (t.ncopy > 0)
         // small blocks: a few thousand threads still spread over every SM
         k_adj_copy<R><<<(unsigned)((t.ncopy + 63) / 64), 64, 0, st>>>(g, t.copy_key, t.copy_start, t.copy_slot,
                                                                        t.ncopy, gmu, lam_out);
     if (t.nout > 0)
-        k_adj_outflow<R><<<(unsigned)((t.nout + 63) / 64), 64, 0, st>>>(g, t.out_jk, t.out_start, t.out_slot,
-                                                                         t.out_q, t.nout, gmu, f, lam_out);
+        k_adj_outflow<S, R><<<(unsigned)((t.nout + 63) / 64), 64, 0, st>>>(g, t.out_jk, t.out_start, t.out_slot,
+                                                                            t.out_q, t.nout, gmu, f, lam_out);
 }
 
-template void launch_pbb_step<float>(const Lat<float, float>&, const Lat<float, float>&, const Geo&,
-                                     const Phys<float>&, const float*, const int32_t*, int64_t, const Reduce&,
-                                     double*, int64_t, int64_t*, cudaStream_t);
-template void launch_pbb_step<double>(const Lat<double, double>&, const Lat<double, double>&, const Geo&,
-                                      const Phys<double>&, const double*, const int32_t*, int64_t, const Reduce&,
-                                      double*, int64_t, int64_t*, cudaStream_t);
-template void launch_pbb_adjoint<float>(const Lat<float, float>&, const Geo&, const Phys<float>&, const float*,
-                                        const Lat<float, float>&, const Lat<float, float>&, float*, double*, float,
-                                        const HaloAdjointDevice&, cudaStream_t);
-template void launch_pbb_adjoint<double>(const Lat<double, double>&, const Geo&, const Phys<double>&,
-                                         const double*, const Lat<double, double>&, const Lat<double, double>&,
-                                         double*, double*, double, const HaloAdjointDevice&, cudaStream_t);
+#define EUP_PBB_INST(S, R)                                                                                       \
+    template void launch_pbb_step<S, R>(const Lat<S, R>&, const Lat<S, R>&, const Geo&, const Phys<R>&, const R*, \
+                                        const int32_t*, int64_t, const Reduce&, double*, int64_t, int64_t*,        \
+                                        cudaStream_t);                                                             \
+    template void launch_pbb_adjoint<S, R>(const Lat<S, R>&, const Geo&, const Phys<R>&, const R*,                \
+                                           const Lat<R, R>&, const Lat<R, R>&, R*, double*, R,                     \
+                                           const HaloAdjointDevice&, cudaStream_t);
+EUP_PBB_INST(float, float)
+EUP_PBB_INST(double, double)
+EUP_PBB_INST(__half, float)
+EUP_PBB_INST(__nv_bfloat16, float)
 
 }  // namespace eup

@@ -257,9 +257,12 @@ def ridge_adjoint(scale=0.25, re=500.0, steps=2500, avg_steps=625, checkpoints=6
                   precision=FP64):
     """Gradient of mean C_d with respect to the ridge height of the ridged shell, chained through
     the solid-fraction field: dJ/dh = sum_x dJ/dn_s(x) dn_s(x)/dh, with n_s = 1 on the shell and
-    the cap and the ridges' radial extent smoothed over smooth_w.  Run on the scaled geometry
-    (scale 1/4: 256x128x128, shell D 24, ridges 2 lu) at the lattice viscosity of the full-size
-    case (Re 500 on the scaled diameter), checked against a central difference of J in h."""
+    the cap and the ridges' radial extent smoothed over smooth_w, checked against a central
+    difference of J in h (two forward runs).  Defaults: the scaled geometry (scale 1/4:
+    256x128x128, shell D 24, ridges 2 lu) at the lattice viscosity of the full-size case (Re 500
+    on the scaled diameter).  The full-size case is scale 1, Re 2000, 16-bit storage,
+    10000 steps (python -m euplectella_hpc_b200.studies --ridge-adjoint --scale 1 --re 2000
+    --precision fp16 --steps 10000 --checkpoints 8)."""
     from .workloads import U_IN, PERTURBATION, ridged_shell_channel
     wl = ridged_shell_channel(scale=scale, re=re, precision=precision)
     c = wl.cfg
@@ -278,8 +281,12 @@ def ridge_adjoint(scale=0.25, re=500.0, steps=2500, avg_steps=625, checkpoints=6
         J, g, st = s.adjoint(steps, avg_steps, checkpoints)
     out.update({"objective": J, "forward_ms": fwd_ms, "adjoint_ms": st["forward_ms"] + st["reverse_ms"],
                 "adjoint_over_forward": (st["forward_ms"] + st["reverse_ms"]) / fwd_ms,
-                "checkpoints_used": st["checkpoints"], "repetitions": st["repetitions"]})
+                "checkpoints_used": st["checkpoints"], "repetitions": st["repetitions"],
+                "recomputed_steps": st["recomputed_steps"], "stored_state_bytes": st["state_bytes"],
+                "nodes": c.lx * c.ly * c.lz, "partial_voxels": int((ns > 0).sum()),
+                "grad_abs_max": float(np.abs(g).max()), "grad_finite": bool(np.isfinite(g).all())})
     out["dJ_dh_adjoint"] = float((g * dns).sum())
+    del g
 
     def objective(h):
         f, _ = body.field(c.lx, c.ly, c.lz, smooth_w, ridge_h=h)
@@ -353,6 +360,10 @@ def main():
                     help="storage of a production run (default: the case's own)")
     ap.add_argument("--chunk", type=int, default=1000, help="steps between divergence checks of a production run")
     ap.add_argument("--voxelise", action="store_true", help="time the production obstacle masks, host against device")
+    ap.add_argument("--scale", type=float, default=0.25, help="ridge adjoint: geometry scale (1 = 1024x512x512)")
+    ap.add_argument("--checkpoints", type=int, default=64, help="ridge adjoint: stored states")
+    ap.add_argument("--avg", type=int, default=None, help="ridge adjoint: averaging window (default steps/4)")
+    ap.add_argument("--dh", type=float, default=0.01, help="ridge adjoint: central-difference step in h")
     args = ap.parse_args()
     if args.voxelise:
         rows = voxelise_timing()
@@ -364,8 +375,13 @@ def main():
         return
     if args.production or args.ridge_adjoint:
         prec = {None: None, "fp32": FP32, "fp64": FP64, "fp16": FP16_DEV, "bf16": BF16_DEV}[args.precision]
-        res = production_run(args.production, None if args.steps == 20000 else args.steps, prec, args.chunk) \
-            if args.production else ridge_adjoint()
+        if args.production:
+            res = production_run(args.production, None if args.steps == 20000 else args.steps, prec, args.chunk)
+        else:
+            steps = 2500 if args.steps == 20000 else args.steps
+            res = ridge_adjoint(scale=args.scale, re=float(args.re) if "," not in args.re else 500.0, steps=steps,
+                                avg_steps=args.avg or steps // 4, checkpoints=args.checkpoints, dh=args.dh,
+                                precision=FP64 if prec is None else prec)
         print(json.dumps(res))
         if args.out:
             with open(args.out, "w") as f:

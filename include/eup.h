@@ -384,7 +384,8 @@ int eup_set_x_planes(eup_handle* h, int32_t side, const void* src);
  * solid fraction n_s(1:l,1:m,1:n) in [0,1] switches the handle to the
  * partial-bounce-back collision of Walsh, Burwinkle & Saar (2009),
  * f*_i = (1-n_s) BGK_i(f) + n_s f_opp(i), whose drag is sum 2 n_s j_x; the force
- * of every step is recorded like eup_get_forces'.  FP32 or FP64 storage, no
+ * of every step is recorded like eup_get_forces'.  Any storage (16-bit
+ * deviations mix as D*_i = (1-n_s) D_i + n_s D_opp(i), since w_i = w_opp(i)), no
  * obstacles.  NULL switches the field off. */
 int eup_set_solid_fraction(eup_handle* h, const double* ns);
 
