@@ -41,14 +41,15 @@ def velocity(pops: np.ndarray) -> np.ndarray:
     return np.stack([np.tensordot(CX, c, 1), np.tensordot(CY, c, 1), np.tensordot(CZ, c, 1)]) / rho
 
 
-def run_one(wl, precision, steps, chunk=500, samples=10):
+def run_one(wl, precision, steps, chunk=500, samples=10, window=None):
     """Runs `steps` steps; returns final state (float64), C_d series, mass, seconds, diverged step and
-    the velocity field averaged over `samples` snapshots evenly spaced in the last quarter."""
+    the velocity field averaged over `samples` snapshots evenly spaced in the last `window` steps
+    (default the last quarter)."""
     wl.cfg.precision = precision
     a = wl.initial_state(np.float64)
     cd = np.zeros(steps + 1)
     diverged = None
-    first = steps - steps // 4
+    first = steps - (window if window else steps // 4)
     marks = set(int(round(first + (steps - first) * (t + 1) / samples)) for t in range(samples))
     vsum, nsum = None, 0
     with Solver(wl.cfg) as s:
@@ -102,6 +103,51 @@ def precision_study(re_list=(500.0, 1000.0, 2000.0), steps=20000):
                 row["cd_mean_fp64"] = float(ref_cd[tail].mean())
                 row["cd_rel_err"] = abs(row["cd_mean"] - row["cd_mean_fp64"]) / abs(row["cd_mean_fp64"])
                 row["mass_rel_diff"] = float(abs(mass - ref_mass) / ref_mass)
+            rows.append(row)
+    return rows
+
+
+def chaos_study(re_list=(500.0, 1000.0), steps=20000, avg_steps=10000, seeds=(1234, 1235, 1236, 1237),
+                samples=10):
+    """Storage error against the chaos floor.  For each Re, every storage format (FP64, FP32,
+    FP16 and BF16 deviations) runs the 256x128x64 cylinder channel from `seeds` (the same
+    equilibrium start with different seeded +-1e-4 perturbations): C_d averaged over the last
+    avg_steps steps and the velocity field averaged over `samples` snapshots of that window.
+    The spread of the FP64 runs over the seeds is what the flow's own sensitivity does to these
+    averages; a storage format whose ensemble mean sits within that spread of the FP64 mean has
+    an error below the chaos floor at this averaging length."""
+    rows = []
+    for re in re_list:
+        wl = cylinder_channel(re=re, steps=steps)
+        fluid = wl.obs == 0
+        ens = {}
+        for name, prec in (("fp64", FP64), ("fp32", FP32), ("fp16-dev", FP16_DEV), ("bf16-dev", BF16_DEV)):
+            cds, vms = [], []
+            for seed in seeds:
+                wl.seed = seed
+                _, cd, _, _, div, vm = run_one(wl, prec, steps, samples=samples, window=avg_steps)
+                if div is not None:
+                    cds.append(float("nan"))
+                    vms.append(None)
+                    continue
+                cds.append(float(cd[steps - avg_steps + 1:].mean()))
+                vms.append(vm[:, fluid])
+            ens[name] = (np.array(cds), vms)
+        cd64, v64 = ens["fp64"]
+        vbar64 = np.mean([v for v in v64 if v is not None], axis=0)
+        spread = float(np.std(cd64, ddof=1) / abs(np.mean(cd64)))
+        v_spread = float(np.mean([np.linalg.norm(v - vbar64) / np.linalg.norm(vbar64) for v in v64]))
+        for name, (cds, vms) in ens.items():
+            ok = [v for v in vms if v is not None]
+            row = {"re": re, "storage": name, "steps": steps, "avg_steps": avg_steps, "seeds": list(seeds),
+                   "cd_mean_per_seed": cds.tolist(), "cd_ensemble_mean": float(np.nanmean(cds)),
+                   "cd_ensemble_rel_std": float(np.nanstd(cds, ddof=1) / abs(np.nanmean(cds))),
+                   "fp64_cd_rel_std": spread, "fp64_mean_velocity_spread": v_spread,
+                   "cd_rel_diff_vs_fp64_ensemble": float(abs(np.nanmean(cds) - np.mean(cd64)) / abs(np.mean(cd64))),
+                   "cd_rel_diff_same_seed": float(np.nanmean(np.abs(cds - cd64) / np.abs(cd64)))}
+            if ok:
+                vbar = np.mean(ok, axis=0)
+                row["mean_velocity_rel_l2_vs_fp64_ensemble"] = float(np.linalg.norm(vbar - vbar64) / np.linalg.norm(vbar64))
             rows.append(row)
     return rows
 
@@ -352,6 +398,8 @@ def main():
     ap.add_argument("--re", default="500,1000,2000")
     ap.add_argument("--out", default=None)
     ap.add_argument("--adjoint", action="store_true", help="run the 192x96x96 partial-bounce-back adjoint study instead")
+    ap.add_argument("--chaos", action="store_true",
+                    help="storage error against the chaos floor: seed ensembles per storage format (--re, --steps)")
     ap.add_argument("--fd", type=int, default=32)
     ap.add_argument("--production", choices=["shell", "ridged"], default=None,
                     help="forward run of the 768x384x384 reticular shell or the 1024x512x512 ridged shell")
@@ -386,6 +434,14 @@ def main():
         if args.out:
             with open(args.out, "w") as f:
                 json.dump(res, f, indent=1)
+        return
+    if args.chaos:
+        rows = chaos_study(tuple(float(x) for x in args.re.split(",")), args.steps, args.steps // 2)
+        for r in rows:
+            print(json.dumps(r), flush=True)
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(rows, f, indent=1)
         return
     if args.adjoint:
         res = adjoint_study(steps=args.steps, n_fd=args.fd)
