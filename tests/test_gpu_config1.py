@@ -10,12 +10,12 @@ steps.  The step being matched is CODE/SRC/bgk3d.F90:114-152 (bounce-back
 bcond.obs.F90:47-77, halo planes bcond.bc.F90, streaming movef.F90:43-68, collision
 col.F90:96-235).
 
-* FP32 (the reference's native precision): every fluid and halo value of the state
-  after 2000 steps bit for bit against the float oracle; the obstacle mask, the link
+* FP32 (the reference's native precision) and FP64: every fluid and halo value of the
+  state after 2000 steps bit for bit against the float / double oracle; the obstacle mask, the link
   classification and the boundary-solid list exactly; the FP64 drag of each of the
   last 500 steps within 1e-12 and its time average within 0.1 %.
-* FP16 and BF16 deviation storage against the FP64 run of the same kernel (which the
-  parity tests hold bit-exact with the double oracle): velocity relative L2 over the
+* FP16 and BF16 deviation storage against the FP64 run of the same kernel (held bit-exact
+  with the double oracle on this very case above): velocity relative L2 over the
   fluid at step 2000 within 1e-3, C_d averaged over the last 500 steps within 0.5 %.
   BF16 misses the velocity bound (expected failure, with the measured value).
 """
@@ -64,14 +64,17 @@ def test_config1_geometry(eup, orc, require_gpu, wl):
         assert np.array_equal(s.boundary_solid(), orc.boundary_solid(p, disc))
 
 
-def test_config1_fp32_bit_exact_2000_steps(eup, orc, require_gpu, wl):
-    c = wl.cfg
-    a0 = wl.initial_state(np.float32)
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_config1_bit_exact_2000_steps(eup, orc, require_gpu, wl, prec):
+    import dataclasses as dc
+    dt, code = (np.float32, eup.FP32) if prec == "fp32" else (np.float64, eup.FP64)
+    c = dc.replace(wl.cfg, precision=code)
+    a0 = wl.initial_state(dt)
     with eup.Solver(c) as s:
         s.set_obstacles(wl.obs)
         s.upload(a0)
         s.step(STEPS)
-        got = s.download(np.float32)
+        got = s.download(dt)
         f_gpu = s.force_series(STEPS - AVG + 1, AVG)
         cd_gpu = s.cd_series(STEPS - AVG + 1, AVG)
     p = _oracle_params(orc, wl)

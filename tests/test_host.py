@@ -137,6 +137,59 @@ def test_geometry_ridged_shell(eup):
     assert np.abs(fd - d).max() < 1e-5 * max(1.0, np.abs(d).max())
 
 
+def _c_prototypes():
+    """name -> list of parameter declarations of every function in include/eup.h."""
+    src = open(os.path.join(ROOT, "include", "eup.h")).read()
+    src = re.sub(r"/\*.*?\*/", " ", src, flags=re.S)
+    src = re.sub(r"\s+", " ", src)
+    out = {}
+    for ret, name, params in re.findall(r"(int|int32_t|const char ?\*|uint64_t) ?(eup_[a-z0-9_]+)\(([^)]*)\);", src):
+        ps = [x.strip() for x in params.split(",")] if params.strip() not in ("", "void") else []
+        out[name] = ps
+    return out
+
+
+def _fortran_interfaces():
+    """name -> list of (dummy name, declaration line) of every bind(c) function in eup_mod.F90."""
+    src = open(os.path.join(ROOT, "fortran", "eup_mod.F90")).read()
+    out = {}
+    for m in re.finditer(r'function (eup_[a-z0-9_]+)\(([^)]*)\)\s*&?\s*bind\(c,\s*name="(eup_[a-z0-9_]+)"\)(.*?)end function',
+                         src, flags=re.S):
+        dummies = [d.strip() for d in m.group(2).replace("&", " ").split(",") if d.strip()]
+        decls = {}
+        for line in m.group(4).splitlines():
+            line = line.split("!")[0]
+            if "::" not in line:
+                continue
+            spec, names = line.split("::", 1)
+            for nm in re.findall(r"([a-z_0-9]+)\s*(?:\([^)]*\))?", names):
+                decls[nm] = spec.strip()
+        out[m.group(3)] = [(d, decls.get(d, "")) for d in dummies]
+    return out
+
+
+def test_fortran_interfaces_match_the_c_prototypes():
+    """Argument by argument (there is no Fortran compiler here to check the module): the same
+    count; a C scalar passed by value (int32_t, int64_t, uint64_t, double) is declared `value`
+    with the matching interop kind; a C pointer is not passed by value unless it is declared
+    type(c_ptr)."""
+    c, f = _c_prototypes(), _fortran_interfaces()
+    assert sorted(c) == sorted(f) == header_functions()
+    kinds = {"int32_t": "c_int32_t", "int64_t": "c_int64_t", "uint64_t": "c_int64_t", "double": "c_double"}
+    for name, params in c.items():
+        dummies = f[name]
+        assert len(params) == len(dummies), (name, params, dummies)
+        for p, (dn, decl) in zip(params, dummies):
+            assert decl, (name, dn, "undeclared dummy")
+            pointer = "*" in p or "[" in p
+            if pointer:
+                assert ("value" not in decl) or ("c_ptr" in decl) or ("c_funptr" in decl), (name, p, decl)
+            else:
+                ctype = p.split()[-2] if len(p.split()) > 1 else p
+                assert "value" in decl, (name, p, decl)
+                assert kinds[ctype] in decl, (name, p, decl)
+
+
 def test_fortran_module_binds_every_entry_point():
     """fortran/eup_mod.F90 declares a bind(c) interface, once, for every function of include/eup.h
     (it is not compiled here: there is no Fortran compiler), in free-form lines of at most 132
