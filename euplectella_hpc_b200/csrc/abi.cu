@@ -40,6 +40,7 @@ struct eup_handle {
     int64_t cap = 0;
     double* dscratch = nullptr;  // 64 doubles
     unsigned int* d_bad = nullptr;  // upload check: bit q set when population q had a non-finite value
+    unsigned int* bc_bar = nullptr; // grid barrier of the single-launch halo kernel: arrivals, generation, timeouts
     void* staging = nullptr;
     size_t staging_bytes = 0;
     int64_t itime = 0, series_first = 0;
@@ -129,6 +130,10 @@ Phys<R> make_phys(const eup_handle* h) {
 }
 
 Mask make_mask(const eup_handle* h) { return Mask{h->bits, h->wpr}; }
+
+// The halo kernels' grid barrier when they run as one cooperative launch (EUP_STEP_VARIANT
+// bit 12; measured slower than one launch per block, the default), else none.
+unsigned int* bc_bar(const eup_handle* h) { return (h->variant & 4096) ? h->bc_bar : nullptr; }
 Reduce make_reduce(const eup_handle* h) { return Reduce{h->partials, h->counter, kReduceMaxBlocks}; }
 
 template <typename S, typename R>
@@ -158,7 +163,7 @@ int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
     if (pe) pe->mark(4 * s + 0, h->stream);
     if (h->pbb) {  // partial bounce-back: halo planes, stream-collide, mixing and force of the step
         if (pe) pe->mark(4 * s + 1, h->stream);
-        n += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
+        n += launch_bc<S, R>(src, h->g, bc, ph, h->stream, bc_bar(h));
         if (pe) pe->mark(4 * s + 2, h->stream);
         launch_pbb_step<S, R>(src, dst, h->g, ph, static_cast<const R*>(h->ns), h->ns_list, h->ns_count,
                               make_reduce(h), h->series, h->cap, h->d_itime, h->stream);
@@ -170,7 +175,7 @@ int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
                              h->cap, h->d_itime, true, h->stream);
     n += 1;
     if (pe) pe->mark(4 * s + 1, h->stream);
-    n += launch_bc<S, R>(src, h->g, bc, ph, h->stream);
+    n += launch_bc<S, R>(src, h->g, bc, ph, h->stream, bc_bar(h));
     if (pe) pe->mark(4 * s + 2, h->stream);
     // propagation + collision (CODE/SRC/bgk3d.F90:133-138)
     launch_stream_collide<S, R>(src, dst, h->g, ph, h->variant, h->stream);
@@ -187,7 +192,7 @@ void enqueue_boundaries(eup_handle* h) {
     const Lat<S, R> src = make_lat<S, R>(h, h->cur);
     launch_bounce_drag<S, R>(src, h->g, bc, h->blist, h->blinks, h->nblist, true, make_reduce(h), h->series,
                              h->cap, h->d_itime, true, h->stream);
-    h->launches += 1 + launch_bc<S, R>(src, h->g, bc, ph, h->stream);
+    h->launches += 1 + launch_bc<S, R>(src, h->g, bc, ph, h->stream, bc_bar(h));
 }
 
 template <typename S, typename R>
@@ -401,6 +406,14 @@ int check_kernel_waits(eup_handle* h, const char* who) {
                     std::string(who) + ": " + std::to_string(n) +
                         " bulk copies of the staged stream-collide kernel did not complete within 2 s; "
                         "the steps since are incomplete");
+    unsigned int bar[3] = {0, 0, 0};
+    CK(h, cudaMemcpy(bar, h->bc_bar, sizeof(bar), cudaMemcpyDeviceToHost));
+    if (bar[2] != 0) {
+        cudaMemset(h->bc_bar, 0, sizeof(bar));  // a barrier that gave up leaves its counter behind
+        return fail(h, EUP_ERR_CUDA,
+                    std::string(who) + ": " + std::to_string(bar[2]) +
+                        " grid-barrier waits of the halo kernel gave up after 1 s; the steps since are incomplete");
+    }
     return EUP_OK;
 }
 
@@ -498,6 +511,12 @@ int eup_create(const eup_config* cfg, eup_handle** out) {
         return cleanup_fail(cuda_fail(h, e, "cudaMalloc(scratch)"));
     if ((e = cudaMalloc(&h->d_bad, sizeof(unsigned int))) != cudaSuccess)
         return cleanup_fail(cuda_fail(h, e, "cudaMalloc(upload check)"));
+    if ((e = cudaMalloc(&h->bc_bar, 3 * sizeof(unsigned int))) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMalloc(halo barrier)"));
+    if ((e = cudaMemset(h->bc_bar, 0, 3 * sizeof(unsigned int))) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "cudaMemset(halo barrier)"));
+    if ((h->variant & 4096) && (e = prepare_bc_fused(h->bc_bar)) != cudaSuccess)
+        return cleanup_fail(cuda_fail(h, e, "halo kernel set-up"));
     const size_t xface_bytes = (size_t)2 * 18 * h->g.m * h->g.n * h->rbytes;
     if ((e = cudaMalloc(&h->xface, xface_bytes)) != cudaSuccess)
         return cleanup_fail(cuda_fail(h, e, "cudaMalloc(x-face copy)"));
@@ -516,7 +535,8 @@ int eup_destroy(eup_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
     void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->blinks, h->partials, h->counter,
-                    h->series, h->dscratch, h->staging, h->xface, h->d_itime, h->ns, h->d_bad, h->ns_list};
+                    h->series, h->dscratch, h->staging, h->xface, h->d_itime, h->ns, h->d_bad, h->ns_list,
+                    h->bc_bar};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1401,7 +1421,7 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
         if (store_at[(size_t)s] >= 0) CK(h, keep(store_at[(size_t)s]));
         if (s == T - 1) CK(h, keep(w0));
         const Lat<S, R> src = make_lat<S, R>(h, h->cur), dst = make_lat<S, R>(h, h->cur ^ 1);
-        launch_bc<S, R>(src, g, bc, ph, st);
+        launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
         launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, h->series, h->cap, h->d_itime, st);
         h->cur ^= 1;
         h->itime += 1;
@@ -1433,7 +1453,7 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
             for (int s = 0; s < act.arg; ++s) {
                 const int next = (s + 1 == act.arg && target >= 0) ? target : (cur == w0 ? w1 : w0);
                 const Lat<S, R> src = buf_lat(cur), dst = buf_lat(next);
-                launch_bc<S, R>(src, g, bc, ph, st);
+                launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
                 launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
                 cur = next;
                 ++recomputed;
@@ -1452,7 +1472,7 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
         } else {  // adjoint of step t from state t-1
             const int t = act.arg;
             const Lat<S, R> f = buf_lat(cur);
-            launch_bc<S, R>(f, g, bc, ph, st);  // the halo of step t, from state t-1
+            launch_bc<S, R>(f, g, bc, ph, st, bc_bar(h));  // the halo of step t, from state t-1
             const Lat<R, R> lin_ = lat_at<R, R>(h, lam.p + state * cur_lam),
                             lout = lat_at<R, R>(h, lam.p + state * (cur_lam ^ 1));
             const R gam = (t > T - A) ? (R)gamma : R(0);

@@ -96,10 +96,17 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[W], const Reduce&
     }
 }
 
-// Halo-plane operations of CODE/SRC/bcond.bc.F90, launched in the reference's order;
-// returns the number of kernels launched.
+// Halo-plane operations of CODE/SRC/bcond.bc.F90 in the reference's order; returns the
+// number of kernels launched.  With `bar` (three zeroed words of device memory owned by the
+// caller, used by one stream at a time) and a device where prepare_bc_fused found cooperative
+// launches usable in CUDA graphs, all blocks run as phases of one launch separated by grid
+// barriers (measured slower); otherwise, and by default, one launch per block.
 template <typename S, typename R>
-int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& ph, cudaStream_t st);
+int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& ph, cudaStream_t st,
+              unsigned int* bar = nullptr);
+// Once per device (outside graph capture): occupancy of the single-launch halo kernel, and a
+// cooperative launch captured into a graph and run once, using `bar` (left zeroed).
+cudaError_t prepare_bc_fused(unsigned int* bar);
 
 // Bounce-back on solid voxels touching fluid/halo (CODE/SRC/bcond.obs.F90) and the
 // FP64 momentum-exchange force of the state it reads, written to

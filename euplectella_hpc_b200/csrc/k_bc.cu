@@ -4,6 +4,9 @@
 // (CODE/SRC/probe_global.F90) and the host-layout scatter/gather used by
 // upload and download.  All of it is O(surface) or O(solid surface) work.
 #include "init_eq.h"
+#include <algorithm>
+#include <type_traits>
+
 #include "internal.h"
 
 namespace eup {
@@ -13,13 +16,14 @@ namespace {
 // One thread per (a, b) pair of a face loop; a runs fastest.
 struct Range2 {
     int a0, na, b0, nb;
-    __device__ __forceinline__ bool get(int& a, int& b) const {
-        const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // element `t` of the loop (false beyond its end)
+    __device__ __forceinline__ bool at(int64_t t, int& a, int& b) const {
         if (t >= (int64_t)na * nb) return false;
         a = a0 + (int)(t % na);
         b = b0 + (int)(t / na);
         return true;
     }
+    int64_t size() const { return (int64_t)na * nb; }
     unsigned blocks(int tpb) const {
         const int64_t t = (int64_t)na * nb;
         return (unsigned)((t + tpb - 1) / tpb);
@@ -38,9 +42,9 @@ constexpr int kTpb = 256;
 
 // ---- front wall, x = l+1 -----------------------------------------------------
 template <typename S, typename R>
-__global__ void k_front(Lat<S, R> L, Geo g, Range2 r, int flag) {
+__device__ __forceinline__ void front_body(const Lat<S, R>& L, const Geo& g, const Range2& r, int flag, int64_t tid) {
     int j, k;
-    if (!r.get(j, k)) return;
+    if (!r.at(tid, j, k)) return;
     const int l = g.l, l1 = g.l + 1, m = g.m;
     if (flag == 0) {  // periodic, CODE/SRC/bcond.bc.F90:75-105 (SERIAL corner line :90)
         if (j == 0) { const R v = LD(12, 1, m, k); ST(12, l1, 0, k, v); return; }
@@ -81,9 +85,9 @@ __global__ void k_front(Lat<S, R> L, Geo g, Range2 r, int flag) {
 
 // Outflow border fix, CODE/SRC/bcond.bc.F90:172-203: copies of the edge rows.
 template <typename S, typename R>
-__global__ void k_front_fix(Lat<S, R> L, Geo g, Range2 r) {
+__device__ __forceinline__ void front_fix_body(const Lat<S, R>& L, const Geo& g, const Range2& r, int64_t tid) {
     int t, side;
-    if (!r.get(t, side)) return;
+    if (!r.at(tid, t, side)) return;
     const int l1 = g.l + 1, m = g.m, n = g.n;
     R lo[5], hi[5];
     if (side == 0 && t >= 1 && t <= m) {
@@ -102,9 +106,9 @@ __global__ void k_front_fix(Lat<S, R> L, Geo g, Range2 r) {
 
 // ---- rear wall, x = 0 ----------------------------------------------------------
 template <typename S, typename R>
-__global__ void k_rear(Lat<S, R> L, Geo g, Range2 r, int flag, R u_inflow) {
+__device__ __forceinline__ void rear_body(const Lat<S, R>& L, const Geo& g, const Range2& r, int flag, R u_inflow, int64_t tid) {
     int j, k;
-    if (!r.get(j, k)) return;
+    if (!r.at(tid, j, k)) return;
     const int l = g.l, m1 = g.m + 1;
     if (flag == 0) {  // periodic, :210-238 (SERIAL corner line :223)
         if (j == 0) { const R v = LD(1, l, 1, k); ST(1, 0, m1, k, v); return; }
@@ -141,9 +145,9 @@ __global__ void k_rear(Lat<S, R> L, Geo g, Range2 r, int flag, R u_inflow) {
 
 // ---- up wall, z = n+1 -------------------------------------------------------------
 template <typename S, typename R>
-__global__ void k_up(Lat<S, R> L, Geo g, Range2 r, int flag, R force) {
+__device__ __forceinline__ void up_body(const Lat<S, R>& L, const Geo& g, const Range2& r, int flag, R force, int64_t tid) {
     int i, j;
-    if (!r.get(i, j)) return;
+    if (!r.at(tid, i, j)) return;
     const int n = g.n, n1 = g.n + 1;
     if (flag == 0) {  // periodic, :385-409
         const R v2 = LD(2, i, j, 1), v9 = LD(9, i, j, 1), v11 = LD(11, i, j, 1), v15 = LD(15, i, j, 1),
@@ -174,9 +178,9 @@ __global__ void k_up(Lat<S, R> L, Geo g, Range2 r, int flag, R force) {
 
 // ---- down wall, z = 0 ---------------------------------------------------------------
 template <typename S, typename R>
-__global__ void k_down(Lat<S, R> L, Geo g, Range2 r, int flag) {
+__device__ __forceinline__ void down_body(const Lat<S, R>& L, const Geo& g, const Range2& r, int flag, int64_t tid) {
     int i, j;
-    if (!r.get(i, j)) return;
+    if (!r.at(tid, i, j)) return;
     const int n = g.n;
     if (flag == 0) {  // periodic, :472-496
         const R v4 = LD(4, i, j, n), v6 = LD(6, i, j, n), v7 = LD(7, i, j, n), v13 = LD(13, i, j, n),
@@ -207,9 +211,9 @@ __global__ void k_down(Lat<S, R> L, Geo g, Range2 r, int flag) {
 
 // ---- left wall, y = 0 ------------------------------------------------------------------
 template <typename S, typename R>
-__global__ void k_left(Lat<S, R> L, Geo g, Range2 r, int flag) {
+__device__ __forceinline__ void left_body(const Lat<S, R>& L, const Geo& g, const Range2& r, int flag, int64_t tid) {
     int i, k;
-    if (!r.get(i, k)) return;
+    if (!r.at(tid, i, k)) return;
     const int l = g.l, m = g.m;
     if (flag == 0) {  // periodic, :535-560 (corner line :547)
         if (i == 0) { const R v = LD(3, l, m, k); ST(3, 0, 0, k, v); return; }
@@ -241,9 +245,9 @@ __global__ void k_left(Lat<S, R> L, Geo g, Range2 r, int flag) {
 
 // ---- right wall, y = m+1 ------------------------------------------------------------------
 template <typename S, typename R>
-__global__ void k_right(Lat<S, R> L, Geo g, Range2 r, int flag) {
+__device__ __forceinline__ void right_body(const Lat<S, R>& L, const Geo& g, const Range2& r, int flag, int64_t tid) {
     int i, k;
-    if (!r.get(i, k)) return;
+    if (!r.at(tid, i, k)) return;
     const int m = g.m, m1 = g.m + 1, l1 = g.l + 1;
     if (flag == 0) {  // periodic, :600-625 (corner line :612)
         if (i == 0) { const R v = LD(10, 1, 1, k); ST(10, l1, m1, k, v); return; }
@@ -275,9 +279,9 @@ __global__ void k_right(Lat<S, R> L, Geo g, Range2 r, int flag) {
 
 // Free-slip edge fixes, CODE/SRC/bcond.bc.F90:663-690.
 template <typename S, typename R>
-__global__ void k_edge_fix(Lat<S, R> L, Geo g, Range2 r, int fixes) {
+__device__ __forceinline__ void edge_fix_body(const Lat<S, R>& L, const Geo& g, const Range2& r, int fixes, int64_t tid) {
     int i, dummy;
-    if (!r.get(i, dummy)) return;
+    if (!r.at(tid, i, dummy)) return;
     const int m = g.m, m1 = g.m + 1, n = g.n, n1 = g.n + 1;
     const R v1 = (fixes & 1) ? LD(18, i, 1, n) : R(0);
     const R v2 = (fixes & 2) ? LD(7, i, m, n) : R(0);
@@ -304,6 +308,131 @@ __global__ void k_edge_fix(Lat<S, R> L, Geo g, Range2 r, int fixes) {
 // wrapped node and its interior value is used.  The force of the state read
 // goes to series[itime % cap], itime read from device memory; with `advance`
 // the last block then increments the device step counter.
+
+// One kernel per halo block (the reference's blocks as separate launches).
+template <typename S, typename R>
+__global__ void k_front(Lat<S, R> L, Geo g, Range2 r, int flag) {
+    front_body<S, R>(L, g, r, flag, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+template <typename S, typename R>
+__global__ void k_front_fix(Lat<S, R> L, Geo g, Range2 r) {
+    front_fix_body<S, R>(L, g, r, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+template <typename S, typename R>
+__global__ void k_rear(Lat<S, R> L, Geo g, Range2 r, int flag, R u_inflow) {
+    rear_body<S, R>(L, g, r, flag, u_inflow, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+template <typename S, typename R>
+__global__ void k_up(Lat<S, R> L, Geo g, Range2 r, int flag, R force) {
+    up_body<S, R>(L, g, r, flag, force, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+template <typename S, typename R>
+__global__ void k_down(Lat<S, R> L, Geo g, Range2 r, int flag) {
+    down_body<S, R>(L, g, r, flag, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+template <typename S, typename R>
+__global__ void k_left(Lat<S, R> L, Geo g, Range2 r, int flag) {
+    left_body<S, R>(L, g, r, flag, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+template <typename S, typename R>
+__global__ void k_right(Lat<S, R> L, Geo g, Range2 r, int flag) {
+    right_body<S, R>(L, g, r, flag, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+template <typename S, typename R>
+__global__ void k_edge_fix(Lat<S, R> L, Geo g, Range2 r, int fixes) {
+    edge_fix_body<S, R>(L, g, r, fixes, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// ---- all halo blocks in one launch (opt-in: EUP_STEP_VARIANT bit 12) ------------------
+// Measured slower than one launch per block on B200 (768x384x384: 0.100 ms against 0.060 ms
+// of halo planes per step; 192x96x96 as well), kept as a tested alternative.
+// The blocks of one step as phases of a single kernel, in the same order, with a grid-wide
+// barrier between phases where the separate launches had a kernel boundary: every element of
+// a phase sees every store of the phases before it, exactly as with one launch per block, so
+// the results are the same bits.  The grid is launched cooperatively (all CTAs resident); the
+// barrier is this library's own (one arrival counter and one generation word per handle, in
+// device memory), and its wait is bounded: after kBarrierWaitNs it counts a timeout in the
+// barrier's third word, which the host reports, and goes on instead of waiting forever.
+enum : int { kBcFront = 0, kBcFrontFix, kBcRear, kBcUp, kBcDown, kBcLeft, kBcRight, kBcEdgeFix };
+struct BcPhase {
+    int kind, flag;
+    Range2 r;
+};
+template <typename R>
+struct BcPlan {
+    int n;
+    BcPhase ph[8];
+    R u_inflow, force;
+};
+
+constexpr uint64_t kBarrierWaitNs = 1000000000ull;
+
+__device__ __forceinline__ uint64_t bc_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// bar[0] arrivals, bar[1] generation, bar[2] timeouts (zero when the handle is created)
+__device__ __forceinline__ void grid_barrier(unsigned int* bar) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = bar + 1;
+        const unsigned int g0 = *gen;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            bar[0] = 0u;
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const uint64_t t0 = bc_ns();
+            while (*gen == g0) {
+                if (bc_ns() - t0 > kBarrierWaitNs) {
+                    atomicAdd(bar + 2, 1u);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+template <typename S, typename R>
+__global__ void __launch_bounds__(kTpb) k_bc_all(Lat<S, R> L, Geo g, BcPlan<R> plan, unsigned int* bar) {
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nt = (int64_t)gridDim.x * blockDim.x;
+    for (int p = 0; p < plan.n; ++p) {
+        const BcPhase ph = plan.ph[p];
+        const int64_t work = (int64_t)ph.r.na * ph.r.nb;
+        for (int64_t t = t0; t < work; t += nt) {
+            switch (ph.kind) {
+                case kBcFront: front_body<S, R>(L, g, ph.r, ph.flag, t); break;
+                case kBcFrontFix: front_fix_body<S, R>(L, g, ph.r, t); break;
+                case kBcRear: rear_body<S, R>(L, g, ph.r, ph.flag, plan.u_inflow, t); break;
+                case kBcUp: up_body<S, R>(L, g, ph.r, ph.flag, plan.force, t); break;
+                case kBcDown: down_body<S, R>(L, g, ph.r, ph.flag, t); break;
+                case kBcLeft: left_body<S, R>(L, g, ph.r, ph.flag, t); break;
+                case kBcRight: right_body<S, R>(L, g, ph.r, ph.flag, t); break;
+                default: edge_fix_body<S, R>(L, g, ph.r, ph.flag, t); break;
+            }
+        }
+        if (p + 1 < plan.n) grid_barrier(bar);
+    }
+}
+
+// Co-resident CTAs of k_bc_all per device and storage type (0: not measured / not usable).
+constexpr int kBcMaxDevices = 64;
+int g_bc_fused_blocks[kBcMaxDevices][4] = {};
+bool g_bc_fused_ok[kBcMaxDevices] = {};
+
+template <typename S> constexpr int bc_type_index() {
+    return sizeof(S) == 4 ? 0 : sizeof(S) == 8 ? 1 : std::is_same<S, __half>::value ? 2 : 3;
+}
+
+__global__ void k_coop_probe(unsigned int* bar) { grid_barrier(bar); }
+
 template <typename S, typename R>
 __global__ void k_bounce_drag(Lat<S, R> L, Geo g, int per_x, int per_y, int per_z, const int32_t* list,
                               const uint64_t* links, int64_t nlist, int do_bounce, Reduce red, double* series,
@@ -715,7 +844,53 @@ void launch_unpack_x(const Lat<S, R>& L, const Geo& g, int side, const R* in, cu
 }
 
 template <typename S, typename R>
-int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& ph, cudaStream_t st) {
+int launch_bc_fused(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& ph, unsigned int* bar,
+                    cudaStream_t st) {
+    const int l = g.l, m = g.m, n = g.n;
+    BcPlan<R> plan;
+    plan.n = 0;
+    plan.u_inflow = ph.u_inflow;
+    plan.force = ph.force;
+    auto add = [&](int kind, int flag, Range2 r) { plan.ph[plan.n++] = BcPhase{kind, flag, r}; };
+    if (bc[0] != 6) {
+        const int f = bc[0];
+        add(kBcFront, f, (f == 0) ? Range2{0, m + 1, 1, n} : Range2{1, m, 1, n});
+        if (f == 5) add(kBcFrontFix, 0, Range2{0, (m > n ? m : n) + 1, 0, 2});
+    }
+    if (bc[1] != 6) {
+        const int f = bc[1];
+        add(kBcRear, f, (f == 0) ? Range2{0, m + 1, 1, n} : (f == 1) ? Range2{1, m, 1, n} : Range2{0, m + 2, 0, n + 2});
+    }
+    add(kBcUp, bc[4], (bc[4] == 3) ? Range2{0, l + 2, 0, m + 2} : Range2{1, l, 1, m});
+    add(kBcDown, bc[5], Range2{1, l, 1, m});
+    add(kBcLeft, bc[3], (bc[3] == 0) ? Range2{0, l + 1, 1, n} : Range2{1, l, 1, n});
+    add(kBcRight, bc[2], (bc[2] == 0) ? Range2{0, l + 1, 1, n} : Range2{1, l, 1, n});
+    const int fixes = ((bc[3] == 3 && bc[4] == 3) ? 1 : 0) | ((bc[2] == 3 && bc[4] == 3) ? 2 : 0) |
+                      ((bc[2] == 3 && bc[5] == 3) ? 4 : 0) | ((bc[3] == 3 && bc[5] == 3) ? 8 : 0);
+    if (fixes) add(kBcEdgeFix, fixes, Range2{1, l, 0, 1});
+    int64_t need = 1;
+    for (int p = 0; p < plan.n; ++p) need = std::max<int64_t>(need, (plan.ph[p].r.size() + kTpb - 1) / kTpb);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kBcMaxDevices) return -1;
+    const int cap = g_bc_fused_blocks[dev][bc_type_index<S>()];
+    if (!g_bc_fused_ok[dev] || cap <= 0) return -1;
+    unsigned grid = (unsigned)std::min<int64_t>(need, cap);
+    Lat<S, R> Lc = L;
+    Geo gc = g;
+    void* args[] = {&Lc, &gc, &plan, &bar};
+    if (cudaLaunchCooperativeKernel((const void*)k_bc_all<S, R>, dim3(grid), dim3(kTpb), args, 0, st) != cudaSuccess)
+        return -1;
+    return 1;
+}
+
+template <typename S, typename R>
+int launch_bc(const Lat<S, R>& L, const Geo& g, const int bc[6], const Phys<R>& ph, cudaStream_t st,
+              unsigned int* bar) {
+    if (bar) {  // one cooperative launch for all blocks when the device allows it
+        const int n = launch_bc_fused<S, R>(L, g, bc, ph, bar, st);
+        if (n > 0) return n;
+        cudaGetLastError();  // a refused cooperative launch leaves nothing behind: use one launch per block
+    }
     const int l = g.l, m = g.m, n = g.n;
     int launches = 4;
     // front (an x-slab exchange face gets its plane from the neighbour instead)
@@ -849,7 +1024,8 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
 }
 
 #define EUP_INST(S, R)                                                                                 \
-    template int launch_bc<S, R>(const Lat<S, R>&, const Geo&, const int*, const Phys<R>&, cudaStream_t); \
+    template int launch_bc<S, R>(const Lat<S, R>&, const Geo&, const int*, const Phys<R>&, cudaStream_t,   \
+                                 unsigned int*);                                                          \
     template void launch_bounce_drag<S, R>(const Lat<S, R>&, const Geo&, const int*, const int32_t*,   \
                                            const uint64_t*, int64_t, bool, const Reduce&, double*,     \
                                            int64_t, int64_t*, bool, cudaStream_t);                     \
@@ -877,5 +1053,46 @@ EUP_INST(float, float)
 EUP_INST(double, double)
 EUP_INST(__half, float)
 EUP_INST(__nv_bfloat16, float)
+
+cudaError_t prepare_bc_fused(unsigned int* bar) {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kBcMaxDevices) return cudaSuccess;  // separate launches there
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    int coop = 0;
+    if ((e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev)) != cudaSuccess) return e;
+    const void* ks[4] = {(const void*)k_bc_all<float, float>, (const void*)k_bc_all<double, double>,
+                         (const void*)k_bc_all<__half, float>, (const void*)k_bc_all<__nv_bfloat16, float>};
+    for (int t = 0; t < 4; ++t) {
+        int per_sm = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks[t], kTpb, 0)) != cudaSuccess) return e;
+        g_bc_fused_blocks[dev][t] = per_sm * sms;
+    }
+    if (!coop) return cudaSuccess;
+    // a cooperative launch must survive stream capture (every step runs as a CUDA graph):
+    // capture one on a private stream, instantiate and run the graph once
+    cudaStream_t s = nullptr;
+    if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    void* args[] = {&bar};
+    const bool launched =
+        ok && cudaLaunchCooperativeKernel((const void*)k_coop_probe, dim3(2), dim3(32), args, 0, s) == cudaSuccess;
+    cudaGraph_t graph = nullptr;
+    ok = (cudaStreamEndCapture(s, &graph) == cudaSuccess) && launched && graph;
+    cudaGraphExec_t exec = nullptr;
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (ok) ok = cudaGraphLaunch(exec, s) == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess;
+    unsigned int word[3] = {1, 0, 1};
+    if (ok) ok = cudaMemcpy(word, bar, sizeof(word), cudaMemcpyDeviceToHost) == cudaSuccess;
+    // the probe's two CTAs met at the barrier: no timeout, arrivals back to zero, one generation
+    ok = ok && word[0] == 0 && word[1] == 1 && word[2] == 0;
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(s);
+    cudaGetLastError();
+    g_bc_fused_ok[dev] = ok;
+    return cudaMemset(bar, 0, 3 * sizeof(unsigned int));
+}
 
 }  // namespace eup

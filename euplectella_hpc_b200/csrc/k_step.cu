@@ -740,7 +740,8 @@ void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo
     // node per thread, bits 4-6: occupancy target of the two-node kernel (n + 3 blocks per SM),
     // bit 7: 16-bit storage staged in shared memory by bulk copies (l a multiple of 8; with
     // bit 11 two CTAs per SM instead of three); default: two nodes per thread (FP32
-    // arithmetic, l even), the pulls loaded into registers.  A split step (interior columns,
+    // arithmetic, l even), the pulls loaded into registers.  (Bit 12 concerns the halo
+    // kernels: all blocks in one cooperative launch instead of one launch per block.)  A split step (interior columns,
     // then the two x-face columns) uses the two-node or the one-node kernel.
     constexpr int VW = VecWidth<S>::value;
     if (part == kStreamAll) {

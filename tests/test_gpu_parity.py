@@ -330,7 +330,8 @@ def test_deviation_storage_against_fp64(eup, require_gpu, prec):
 @pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16", "bf16"])
 def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
     """Two nodes per thread (default, at several occupancies; for 16-bit storage variant 128
-    stages the pulls in shared memory instead of registers) vs one node per thread vs 16-byte and 8-byte vectorised stream-collide, CUDA
+    stages the pulls in shared memory instead of registers; 4096: every halo block in one
+    cooperative launch instead of one launch each) vs one node per thread vs 16-byte and 8-byte vectorised stream-collide, CUDA
     graphs vs plain launches: all paths give the same bits in every storage format."""
     l, m, n = 256, 20, 13
     code = {"fp32": eup.FP32, "fp64": eup.FP64, "fp16": eup.FP16_DEV, "bf16": eup.BF16_DEV}[prec]
@@ -339,7 +340,7 @@ def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
     a = eup.init_equilibrium(l, m, n, 0.05, 1e-3, 77, dt)
     cfg = eup.Config(l, m, n, bc=(5, 4, 3, 3, 0, 0), svisc=0.01, u_inflow=0.05, precision=code)
     res = []
-    for var in ("0", "1", "2", "3", "4", "6", "8", "10", "16", "48", "80", "128", "130", "144"):
+    for var in ("0", "1", "2", "3", "4", "6", "8", "10", "16", "48", "80", "128", "130", "144", "4096", "4098"):
         monkeypatch.setenv("EUP_STEP_VARIANT", var)
         with eup.Solver(cfg) as s:
             s.set_obstacles(obs)
@@ -352,13 +353,20 @@ def test_kernel_variants_bit_identical(eup, require_gpu, prec, monkeypatch):
         assert np.array_equal(f, res[0][1])
 
 
-def test_launch_count(eup, require_gpu):
+@pytest.mark.parametrize("variant", ["0", "4096"])
+def test_launch_count(eup, require_gpu, monkeypatch, variant):
+    monkeypatch.setenv("EUP_STEP_VARIANT", variant)
     l, m, n = 128, 12, 10
     obs = _block(l, m, n)
     with eup.Solver(eup.Config(l, m, n, bc=(5, 4, 3, 3, 3, 3), svisc=0.01, u_inflow=0.05)) as s:
         s.set_obstacles(obs)
         s.upload(eup.init_equilibrium(l, m, n, 0.05, 0, 1))
         s.step(4)
-        # per step: bounce-back/drag, front, front border fix, rear, up, down, left, right,
-        # free-slip edge fixes, stream-collide = 10; plus one drag of the final state
-        assert s.launches == 4 * 10 + 1
+        if variant == "4096":
+            # per step: bounce-back/drag, every halo block in one cooperative launch,
+            # stream-collide = 3; plus one drag of the final state
+            assert s.launches == 4 * 3 + 1
+        else:
+            # per step: bounce-back/drag, one launch per halo block (front, front border fix,
+            # rear, up, down, left, right, free-slip edge fixes), stream-collide = 10
+            assert s.launches == 4 * 10 + 1
