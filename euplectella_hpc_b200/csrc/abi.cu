@@ -7,6 +7,7 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/eup.h"
@@ -1280,6 +1281,39 @@ int revolve_repetition(int64_t n, int64_t c) {
 }
 
 enum : int { kActAdvance = 0, kActSnapshot = 1, kActRestore = 2, kActAdjoint = 3 };
+
+// CUDA graphs of the launch sequences an adjoint run repeats (a forward step between two given
+// buffers, an adjoint step from a given buffer), captured the first time a key is met and
+// launched from then on: a reverse sweep uses a few hundred distinct sequences thousands of
+// times.  With use == false the sequence is launched directly.
+struct GraphCache {
+    std::unordered_map<uint64_t, cudaGraphExec_t> exec;
+    ~GraphCache() {
+        for (auto& kv : exec) cudaGraphExecDestroy(kv.second);
+    }
+    template <typename F>
+    cudaError_t run(uint64_t key, cudaStream_t st, bool use, F&& enqueue) {
+        if (!use) {
+            enqueue();
+            return cudaGetLastError();
+        }
+        auto it = exec.find(key);
+        if (it == exec.end()) {
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return e;
+            enqueue();
+            e = cudaStreamEndCapture(st, &graph);
+            if (e != cudaSuccess) return e;
+            cudaGraphExec_t ge = nullptr;
+            e = cudaGraphInstantiate(&ge, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return e;
+            it = exec.emplace(key, ge).first;
+        }
+        return cudaGraphLaunch(it->second, st);
+    }
+};
 struct RevAct {
     int kind, arg;  // advance: steps; snapshot/restore: slot; adjoint: the step t reversed (from state t-1)
 };
@@ -1416,13 +1450,27 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     // ---- forward sweep (the handle's own state, force series recorded) ----
     const int64_t t0 = h->itime;
     const int w0 = slots, w1 = slots + 1;  // the working buffers
+    // every step as a CUDA graph (EUP_STEP_VARIANT bit 1: plain launches): the forward sweep
+    // uses the handle's own step graphs, the reverse sweep the cache below
+    const bool graphs = !(h->variant & 2);
+    int per_step = 0;
+    if (graphs) {
+        const cudaError_t e_cap = capture_graphs<S, R>(h, &per_step);
+        CK(h, e_cap);
+    }
+    GraphCache cache;
     CK(h, cudaEventRecord(ev[0], st));
     for (int s = 0; s < T; ++s) {
         if (store_at[(size_t)s] >= 0) CK(h, keep(store_at[(size_t)s]));
         if (s == T - 1) CK(h, keep(w0));
-        const Lat<S, R> src = make_lat<S, R>(h, h->cur), dst = make_lat<S, R>(h, h->cur ^ 1);
-        launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
-        launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, h->series, h->cap, h->d_itime, st);
+        if (graphs) {
+            CK(h, cudaGraphLaunch(h->graph[h->cur], st));
+        } else {
+            const Lat<S, R> src = make_lat<S, R>(h, h->cur), dst = make_lat<S, R>(h, h->cur ^ 1);
+            launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
+            launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, h->series, h->cap, h->d_itime,
+                                  st);
+        }
         h->cur ^= 1;
         h->itime += 1;
     }
@@ -1453,8 +1501,12 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
             for (int s = 0; s < act.arg; ++s) {
                 const int next = (s + 1 == act.arg && target >= 0) ? target : (cur == w0 ? w1 : w0);
                 const Lat<S, R> src = buf_lat(cur), dst = buf_lat(next);
-                launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
-                launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
+                const uint64_t key = ((uint64_t)1 << 60) | ((uint64_t)cur << 24) | (uint64_t)next;
+                const cudaError_t e_run = cache.run(key, st, graphs, [&] {
+                    launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
+                    launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
+                });
+                CK(h, e_run);
                 cur = next;
                 ++recomputed;
             }
@@ -1472,11 +1524,17 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
         } else {  // adjoint of step t from state t-1
             const int t = act.arg;
             const Lat<S, R> f = buf_lat(cur);
-            launch_bc<S, R>(f, g, bc, ph, st, bc_bar(h));  // the halo of step t, from state t-1
             const Lat<R, R> lin_ = lat_at<R, R>(h, lam.p + state * cur_lam),
                             lout = lat_at<R, R>(h, lam.p + state * (cur_lam ^ 1));
-            const R gam = (t > T - A) ? (R)gamma : R(0);
-            launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st);
+            const bool in_window = t > T - A;
+            const R gam = in_window ? (R)gamma : R(0);
+            const uint64_t key = ((uint64_t)2 << 60) | ((uint64_t)cur << 24) | ((uint64_t)cur_lam << 1) |
+                                 (uint64_t)in_window;
+            const cudaError_t e_run = cache.run(key, st, graphs, [&] {
+                launch_bc<S, R>(f, g, bc, ph, st, bc_bar(h));  // the halo of step t, from state t-1
+                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st);
+            });
+            CK(h, e_run);
             cur_lam ^= 1;
         }
     }

@@ -96,6 +96,26 @@ def test_adjoint_checkpoint_count_does_not_change_the_gradient(eup, require_gpu)
         assert J == out[0][0] and np.array_equal(g, out[0][1])
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_adjoint_graphs_equal_plain_launches(eup, require_gpu, monkeypatch, prec):
+    """The adjoint run's steps as cached CUDA graphs (default) and as plain launches
+    (EUP_STEP_VARIANT=2) give the same bits."""
+    code = eup.FP32 if prec == "fp32" else eup.FP16_DEV
+    out = []
+    for var in ("0", "2"):
+        monkeypatch.setenv("EUP_STEP_VARIANT", var)
+        cfg, ns = small_case(eup, code)
+        a = eup.init_equilibrium(L, M, N, 0.05, 1e-4, 11, np.float64)
+        with eup.Solver(cfg) as s:
+            s.set_solid_fraction(ns)
+            s.upload(a)
+            J, g, st = s.adjoint(T, A, checkpoints=5)
+            out.append((J, g, s.download(np.float64)))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+
+
 def test_fp32_adjoint_against_fp64_adjoint(eup, require_gpu):
     res = {}
     for code, dt in ((eup.FP64, np.float64), (eup.FP32, np.float32)):
