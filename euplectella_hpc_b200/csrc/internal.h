@@ -135,7 +135,8 @@ enum { kStreamAll = 0, kStreamInterior = 1, kStreamFaces = 2 };
 // Kernel attributes the stream-collide launches need (once per device, outside graph capture).
 cudaError_t prepare_stream_collide();
 // Number of bounded waits of the staged stream-collide kernel that ran out on this device
-// (each stopped its CTA's stores: the step's result is then incomplete).
+// since the last call (each stopped its CTA's stores: the step's result is then incomplete);
+// the count restarts from zero once read.
 cudaError_t staged_wait_timeouts(unsigned int* count);
 template <typename S, typename R>
 void launch_stream_collide(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g,

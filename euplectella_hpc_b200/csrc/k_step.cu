@@ -790,7 +790,12 @@ cudaError_t prepare_stream_collide() {
 }
 
 cudaError_t staged_wait_timeouts(unsigned int* count) {
-    return cudaMemcpyFromSymbol(count, g_staged_timeouts, sizeof(unsigned int));
+    cudaError_t e = cudaMemcpyFromSymbol(count, g_staged_timeouts, sizeof(unsigned int));
+    if (e == cudaSuccess && *count != 0) {  // reported once
+        const unsigned int zero = 0;
+        e = cudaMemcpyToSymbol(g_staged_timeouts, &zero, sizeof(unsigned int));
+    }
+    return e;
 }
 
 }  // namespace eup
