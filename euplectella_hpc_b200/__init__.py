@@ -42,7 +42,7 @@ EXPORTED = [
     "eup_get_cv_drag", "eup_save_state", "eup_restore_state", "eup_step_boundaries", "eup_step_stream",
     "eup_get_x_planes", "eup_set_x_planes", "eup_geometry_reference", "eup_voxelise", "eup_build_obstacles",
     "eup_get_obstacles", "eup_write_obstacles", "eup_step_stream_interior", "eup_step_stream_faces",
-    "eup_init_reference",
+    "eup_init_reference", "eup_adjoint_plan",
 ]
 
 
@@ -147,6 +147,7 @@ def _load():
         "eup_geometry_reticular_shell": ([i32, i32, i32, dbl, dbl, dbl, dbl, dbl, dbl, dbl, ctypes.c_uint64, vp],
                                          ctypes.c_int),
         "eup_mem_force_noalloc": ([i32, i32, i32, ctypes.c_int32 * 6, P19, i32, vp, vp, vp], ctypes.c_int),
+        "eup_adjoint_plan": ([i32, i32, vp, vp, vp], ctypes.c_int),
         "eup_set_solid_fraction": ([vp, vp], ctypes.c_int),
         "eup_geometry_ridged_shell": ([i32, i32, i32] + [dbl] * 12 + [ctypes.c_uint64, vp, vp], ctypes.c_int),
         "eup_get_region_sums": ([vp, vp, vp], ctypes.c_int),
@@ -472,6 +473,14 @@ class Solver:
 
 
 # ---- host utilities ------------------------------------------------------------
+
+def adjoint_plan(nsteps: int, checkpoints: int = 0) -> dict:
+    """The checkpoint schedule of Solver.adjoint for nsteps steps and `checkpoints` stored states
+    (0: 64), computed on the host: forward steps in all, recomputed in the reverse sweep, r."""
+    fwd, rec, rep = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    _check(lib.eup_adjoint_plan(int(nsteps), int(checkpoints), ctypes.byref(fwd), ctypes.byref(rec), ctypes.byref(rep)))
+    return {"forward_steps": fwd.value, "recomputed_steps": rec.value, "repetitions": rep.value}
+
 
 def init_equilibrium(l, m, n, u_in, amp, seed, dtype=np.float32) -> np.ndarray:
     """Synthetic initial state: equilibrium at rho=1, u = inlet + seeded perturbation, halos included."""

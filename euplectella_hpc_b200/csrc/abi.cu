@@ -1610,6 +1610,29 @@ int eup_set_solid_fraction(eup_handle* h, const double* ns) {
     return EUP_OK;
 }
 
+int eup_adjoint_plan(int32_t nsteps, int32_t checkpoints, int64_t* forward_steps, int64_t* recomputed,
+                     int32_t* repetitions) {
+    if (nsteps < 1 || checkpoints < 0 || !forward_steps || !recomputed || !repetitions)
+        return fail(nullptr, EUP_ERR_INVALID_ARG, "eup_adjoint_plan: need nsteps >= 1, checkpoints >= 0 and outputs");
+    int slots = checkpoints > 0 ? checkpoints : 64;
+    if (slots > nsteps) slots = nsteps;
+    std::vector<RevAct> acts;
+    std::vector<int> free;
+    for (int k = slots - 1; k >= 1; --k) free.push_back(k);
+    acts.push_back({kActSnapshot, 0});
+    revolve_schedule(0, nsteps, 0, free, acts);
+    int64_t total = 0, sweep = 0;
+    bool reversing = false;
+    for (const RevAct& a : acts) {
+        if (a.kind == kActAdjoint) reversing = true;
+        if (a.kind == kActAdvance) (reversing ? total : sweep) += a.arg;
+    }
+    *forward_steps = sweep + total;          // t(T, c): the first descent plus the recomputation
+    *recomputed = total;                     // what the reverse sweep recomputes (eup_adjoint_run's stats[2])
+    *repetitions = revolve_repetition(nsteps, slots);
+    return EUP_OK;
+}
+
 int eup_adjoint_run(eup_handle* h, const eup_adjoint_config* cfg, double* objective, double* grad_ns,
                     double stats[8]) {
     int rc = check_handle(h);

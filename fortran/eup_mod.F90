@@ -155,6 +155,15 @@
             real(c_double)                :: stats(8)
          end function
 
+         ! checkpoint schedule of eup_adjoint_run for nsteps steps and checkpoints states (host only)
+         integer(c_int) function eup_adjoint_plan(nsteps, checkpoints, forward_steps, recomputed, repetitions) &
+               bind(c, name="eup_adjoint_plan")
+            import :: c_int, c_int32_t, c_int64_t
+            integer(c_int32_t), value :: nsteps, checkpoints
+            integer(c_int64_t)        :: forward_steps, recomputed
+            integer(c_int32_t)        :: repetitions
+         end function
+
          ! x-slab step (one GPU per slab): boundaries, planes out, interior | exchange, planes in, faces
          integer(c_int) function eup_step_boundaries(h) bind(c, name="eup_step_boundaries")
             import :: c_int, c_ptr

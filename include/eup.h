@@ -410,6 +410,15 @@ typedef struct eup_adjoint_config {
 int eup_adjoint_run(eup_handle* h, const eup_adjoint_config* cfg, double* objective, double* grad_ns,
                     double stats[8]);
 
+/* No counterpart in the reference.  The checkpoint schedule eup_adjoint_run
+ * would follow for nsteps steps and `checkpoints` stored states (0 selects 64),
+ * built on the host without a GPU, to size the budget before a run:
+ * *forward_steps = forward steps of the whole schedule, t(nsteps, c) (the
+ * forward sweep's first nsteps-1 included), *recomputed = those of the reverse
+ * sweep (eup_adjoint_run's stats[2]), *repetitions = r. */
+int eup_adjoint_plan(int32_t nsteps, int32_t checkpoints, int64_t* forward_steps, int64_t* recomputed,
+                     int32_t* repetitions);
+
 /* ---- host utilities (no GPU) ---------------------------------------------- */
 
 /* Reads obs.RRRR.TTTTTTTT.bin (CODE/SRC/build.obs.F90:147-177): Fortran
