@@ -42,7 +42,7 @@ EXPORTED = [
     "eup_get_cv_drag", "eup_save_state", "eup_restore_state", "eup_step_boundaries", "eup_step_stream",
     "eup_get_x_planes", "eup_set_x_planes", "eup_geometry_reference", "eup_voxelise", "eup_build_obstacles",
     "eup_get_obstacles", "eup_write_obstacles", "eup_step_stream_interior", "eup_step_stream_faces",
-    "eup_init_reference", "eup_adjoint_plan",
+    "eup_init_reference", "eup_adjoint_plan", "eup_get_x_planes_view", "eup_set_x_planes_view",
 ]
 
 
@@ -158,6 +158,8 @@ def _load():
         "eup_save_state": ([vp, ctypes.c_char_p, i32], ctypes.c_int),
         "eup_step_boundaries": ([vp], ctypes.c_int), "eup_step_stream": ([vp], ctypes.c_int),
         "eup_get_x_planes": ([vp, i32, vp], ctypes.c_int), "eup_set_x_planes": ([vp, i32, vp], ctypes.c_int),
+        "eup_get_x_planes_view": ([vp, i32, ctypes.POINTER(vp)], ctypes.c_int),
+        "eup_set_x_planes_view": ([vp, i32, vp], ctypes.c_int),
         "eup_restore_state": ([vp, ctypes.c_char_p, i32], ctypes.c_int),
         "eup_adjoint_run": ([vp, ctypes.POINTER(AdjointConfig), ctypes.POINTER(dbl), vp, vp], ctypes.c_int),
         "eup_geometry_reference": ([i32, i32, i32, i32, i32, ctypes.POINTER(Geometry)], ctypes.c_int),
@@ -398,6 +400,18 @@ class Solver:
     def set_x_planes(self, side, dev_ptr):
         """Write received planes into the x = 0 (side 0) or x = l+1 (side 1) halo."""
         self._ck(lib.eup_set_x_planes(self._h, side, dev_ptr))
+
+    def x_planes_view(self, side) -> int:
+        """Device address of the plane message of an exchange face inside the handle's x-face
+        copy (written by the stream-collide epilogue, halo rows added by step_boundaries):
+        5 (m+2)(n+2) values, the five populations' m x n interior blocks, then their halo rows."""
+        p = ctypes.c_void_p()
+        self._ck(lib.eup_get_x_planes_view(self._h, side, ctypes.byref(p)))
+        return p.value
+
+    def set_x_planes_view(self, side, dev_ptr):
+        """Write a received message in the x_planes_view order into the x = 0 / x = l+1 halo."""
+        self._ck(lib.eup_set_x_planes_view(self._h, side, dev_ptr))
 
     def save_state(self, path, elem_bytes=4):
         """Checkpoint in the reference's raw format straight from the device."""

@@ -52,7 +52,7 @@ struct eup_handle {
     void* ns = nullptr;           // solid fraction n_s per interior node, arithmetic type
     int32_t* ns_list = nullptr;   // interior linear indices with n_s > 0, ascending
     int64_t ns_count = 0;
-    int64_t launches = 0;  // kernels launched by eup_step / eup_step_profiled
+    int64_t launches = 0;  // kernels launched by the step calls (split steps and plane pack/unpack too)
     bool mid_step = false;  // eup_step_boundaries done, eup_step_stream pending
     bool interior_done = false;  // eup_step_stream_interior done, eup_step_stream_faces pending
     int launches_per_step = 0;
@@ -186,6 +186,11 @@ int enqueue_one_step(eup_handle* h, int src_idx, PhaseEvents* pe, size_t s) {
 }
 
 // The two halves of a step of an x-slab lattice (the plane exchange goes between).
+// Bit 0: the x = 0 face (column x = 1, side 0) is an exchange face; bit 1: the x = l+1 face.
+int exchange_sides(const eup_handle* h) {
+    return (h->cfg.bc[EUP_REAR] == EUP_BC_EXCHANGE ? 1 : 0) | (h->cfg.bc[EUP_FRONT] == EUP_BC_EXCHANGE ? 2 : 0);
+}
+
 template <typename S, typename R>
 void enqueue_boundaries(eup_handle* h) {
     const Phys<R> ph = make_phys<R>(h);
@@ -194,6 +199,10 @@ void enqueue_boundaries(eup_handle* h) {
     launch_bounce_drag<S, R>(src, h->g, bc, h->blist, h->blinks, h->nblist, true, make_reduce(h), h->series,
                              h->cap, h->d_itime, true, h->stream);
     h->launches += 1 + launch_bc<S, R>(src, h->g, bc, ph, h->stream, bc_bar(h));
+    if (const int xs = exchange_sides(h)) {  // the plane messages' halo rows, after the halo kernels
+        launch_pack_x_rim<S, R>(src, h->g, xs, h->stream);
+        h->launches += 1;
+    }
 }
 
 template <typename S, typename R>
@@ -212,11 +221,19 @@ void enqueue_stream(eup_handle* h, int part) {
 template <typename S, typename R>
 void pack_x_dispatch(eup_handle* h, int side, void* dst) {
     launch_pack_x<S, R>(make_lat<S, R>(h, h->cur), h->g, side, static_cast<R*>(dst), h->stream);
+    h->launches += 1;
 }
 
 template <typename S, typename R>
 void unpack_x_dispatch(eup_handle* h, int side, const void* src) {
     launch_unpack_x<S, R>(make_lat<S, R>(h, h->cur), h->g, side, static_cast<const R*>(src), h->stream);
+    h->launches += 1;
+}
+
+template <typename S, typename R>
+void unpack_x_view_dispatch(eup_handle* h, int side, const void* src) {
+    launch_unpack_x_view<S, R>(make_lat<S, R>(h, h->cur), h->g, side, static_cast<const R*>(src), h->stream);
+    h->launches += 1;
 }
 
 template <typename S, typename R>
@@ -518,7 +535,7 @@ int eup_create(const eup_config* cfg, eup_handle** out) {
         return cleanup_fail(cuda_fail(h, e, "cudaMemset(halo barrier)"));
     if ((h->variant & 4096) && (e = prepare_bc_fused(h->bc_bar)) != cudaSuccess)
         return cleanup_fail(cuda_fail(h, e, "halo kernel set-up"));
-    const size_t xface_bytes = (size_t)2 * 18 * h->g.m * h->g.n * h->rbytes;
+    const size_t xface_bytes = (size_t)xface_elems(h->g) * h->rbytes;
     if ((e = cudaMalloc(&h->xface, xface_bytes)) != cudaSuccess)
         return cleanup_fail(cuda_fail(h, e, "cudaMalloc(x-face copy)"));
     cudaMemsetAsync(h->xface, 0, xface_bytes, h->stream);
@@ -956,6 +973,29 @@ int eup_set_x_planes(eup_handle* h, int32_t side, const void* src) {
     if (h->cfg.bc[side == 0 ? EUP_REAR : EUP_FRONT] != EUP_BC_EXCHANGE)
         return fail(h, EUP_ERR_INVALID_ARG, "eup_set_x_planes: that face is not an exchange face");
     DISPATCH(h, unpack_x_dispatch, h, side, src);
+    CK(h, cudaGetLastError());
+    return EUP_OK;
+}
+
+int eup_get_x_planes_view(eup_handle* h, int32_t side, const void** dev) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!dev || (side != 0 && side != 1))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_get_x_planes_view: bad side or null");
+    if (!((exchange_sides(h) >> side) & 1))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_get_x_planes_view: that face is not an exchange face");
+    *dev = static_cast<const char*>(h->xface) + (size_t)xface_send_offset(h->g, side) * h->rbytes;
+    return EUP_OK;
+}
+
+int eup_set_x_planes_view(eup_handle* h, int32_t side, const void* src) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!src || (side != 0 && side != 1))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_set_x_planes_view: bad side or null");
+    if (!((exchange_sides(h) >> side) & 1))
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_set_x_planes_view: that face is not an exchange face");
+    DISPATCH(h, unpack_x_view_dispatch, h, side, src);
     CK(h, cudaGetLastError());
     return EUP_OK;
 }
@@ -1418,7 +1458,7 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     // where the schedule stores a state writes it into the slot directly
     const size_t state = (size_t)Q * h->Nq;
     const size_t shell = (size_t)Q * g.G;
-    const size_t xfs = (size_t)2 * 18 * g.m * g.n;
+    const size_t xfs = (size_t)xface_elems(g);
     const int nbuf = slots + 2;
     DevBuf<S> bufs;
     DevBuf<R> xfaces, lam, gmu, wshell;

@@ -122,6 +122,10 @@ template <typename S, typename R>
 void launch_pack_x(const Lat<S, R>& L, const Geo& g, int side, R* out, cudaStream_t st);
 template <typename S, typename R>
 void launch_unpack_x(const Lat<S, R>& L, const Geo& g, int side, const R* in, cudaStream_t st);
+template <typename S, typename R>
+void launch_pack_x_rim(const Lat<S, R>& L, const Geo& g, int sides, cudaStream_t st);
+template <typename S, typename R>
+void launch_unpack_x_view(const Lat<S, R>& L, const Geo& g, int side, const R* in, cudaStream_t st);
 
 // x-face copy of the current lattice (needed once after an upload).
 template <typename S, typename R>

@@ -789,7 +789,7 @@ __global__ void k_fill_xface(Lat<S, R> L, Geo g) {
     const int64_t jk = t - sq * mn;
     const int side = sq / 18, q = sq - 18 * side;
     const int j = (int)(jk % g.m) + 1, k = (int)(jk / g.m) + 1;
-    L.xface[t] = lat_load(L, g, q, side ? g.l : 1, j, k);
+    L.xface[xface_idx(g, side, q, j, k)] = lat_load(L, g, q, side ? g.l : 1, j, k);
 }
 
 unsigned grid_for(int64_t work, int tpb, unsigned cap = 148u * 16u) {
@@ -818,6 +818,47 @@ __global__ void k_pack_x(Lat<S, R> L, Geo g, int side, R* out) {
     out[t] = bc_load(L, g, q, i, j, k);
 }
 
+// The rim of the x-face copy's plane messages: the five outgoing populations on the
+// halo rows of each exchange face column (sides: bit 0 = x = 1, bit 1 = x = l), read
+// after the halo kernels wrote them.
+template <typename S, typename R>
+__global__ void k_pack_x_rim(Lat<S, R> L, Geo g, int sides) {
+    const int64_t per = xface_rim_len(g) / 5;  // halo-row nodes of one face plane
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 10 * per) return;
+    const int side = (int)(t / (5 * per));
+    if (!((sides >> side) & 1)) return;
+    const int64_t r = t - side * 5 * per;
+    const int c = (int)(r / per);
+    int j, k;
+    xface_rim_node(g, r - c * per, &j, &k);
+    const int q = side ? c : 9 + c;
+    L.xface[side * xface_side_stride(g) + 18 * (int64_t)g.m * g.n + r] = lat_load(L, g, q, side ? g.l : 1, j, k);
+}
+
+// Received plane message in the x-face copy's order (five m*n blocks, then the rim)
+// into the x = 0 (side 0, q 0..4) or x = l+1 (side 1, q 9..13) halo plane.
+template <typename S, typename R>
+__global__ void k_unpack_x_view(Lat<S, R> L, Geo g, int side, const R* in) {
+    const int64_t mn = (int64_t)g.m * g.n, per = xface_rim_len(g) / 5;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 5 * (mn + per)) return;
+    int c, j, k;
+    if (t < 5 * mn) {
+        c = (int)(t / mn);
+        const int64_t jk = t - c * mn;
+        j = (int)(jk % g.m) + 1;
+        k = (int)(jk / g.m) + 1;
+    } else {
+        const int64_t r = t - 5 * mn;
+        c = (int)(r / per);
+        xface_rim_node(g, r - c * per, &j, &k);
+    }
+    const int q = side ? 9 + c : c;
+    const int i = side ? g.l + 1 : 0;
+    L.ghost[(int64_t)q * g.G + g.gidx(i, j, k)] = in[t];
+}
+
 template <typename S, typename R>
 __global__ void k_unpack_x(Lat<S, R> L, Geo g, int side, const R* in) {
     const int64_t plane = (int64_t)(g.m + 2) * (g.n + 2);
@@ -835,6 +876,18 @@ template <typename S, typename R>
 void launch_pack_x(const Lat<S, R>& L, const Geo& g, int side, R* out, cudaStream_t st) {
     const int64_t work = 5 * (int64_t)(g.m + 2) * (g.n + 2);
     k_pack_x<S, R><<<(unsigned)((work + kTpb - 1) / kTpb), kTpb, 0, st>>>(L, g, side, out);
+}
+
+template <typename S, typename R>
+void launch_pack_x_rim(const Lat<S, R>& L, const Geo& g, int sides, cudaStream_t st) {
+    const int64_t work = 2 * xface_rim_len(g);
+    k_pack_x_rim<S, R><<<(unsigned)((work + kTpb - 1) / kTpb), kTpb, 0, st>>>(L, g, sides);
+}
+
+template <typename S, typename R>
+void launch_unpack_x_view(const Lat<S, R>& L, const Geo& g, int side, const R* in, cudaStream_t st) {
+    const int64_t work = 5 * (int64_t)(g.m + 2) * (g.n + 2);
+    k_unpack_x_view<S, R><<<(unsigned)((work + kTpb - 1) / kTpb), kTpb, 0, st>>>(L, g, side, in);
 }
 
 template <typename S, typename R>
@@ -1032,6 +1085,8 @@ void launch_gather(const Lat<S, R>& L, const Geo& g, int q, T* staging, cudaStre
     template void launch_fill_xface<S, R>(const Lat<S, R>&, const Geo&, cudaStream_t);                 \
     template void launch_pack_x<S, R>(const Lat<S, R>&, const Geo&, int, R*, cudaStream_t);              \
     template void launch_unpack_x<S, R>(const Lat<S, R>&, const Geo&, int, const R*, cudaStream_t);      \
+    template void launch_pack_x_rim<S, R>(const Lat<S, R>&, const Geo&, int, cudaStream_t);              \
+    template void launch_unpack_x_view<S, R>(const Lat<S, R>&, const Geo&, int, const R*, cudaStream_t); \
     template void launch_line<S, R>(const Lat<S, R>&, const Geo&, int, int, int, double*, cudaStream_t);   \
     template void launch_plane_means<S, R>(const Lat<S, R>&, const Geo&, int, double*, cudaStream_t);     \
     template void launch_cv_drag<S, R>(const Lat<S, R>&, const Geo&, const int*, R, const Reduce&, double*, \

@@ -192,17 +192,57 @@ __host__ __device__ __forceinline__ void face_row(const Geo& g, int f, int* j, i
 // Pointers of one lattice (19 population arrays) plus the halo shell and the
 // x-face copy.  The x-face copy holds, for the interior columns x = 1 (side 0)
 // and x = l (side 1), the 18 moving populations exactly as a load from the
-// lattice returns them, laid out xface[(side*18 + q)*m*n + (j-1) + (k-1)*m].
-// The stream-collide kernel writes it for the state it produces and the
-// bounce-back kernel keeps it in step, so that halo kernels read these
-// columns coalesced in j instead of with a stride of l elements.
+// lattice returns them.  The stream-collide kernel writes it for the state it
+// produces and the bounce-back kernel keeps it in step, so that halo kernels
+// read these columns coalesced in j instead of with a stride of l elements.
+//
+// Layout per side: 18 slots of m*n values ((j-1) + (k-1)*m), then a rim of
+// 5 * (2(m+2) + 2n) values.  The slots are rotated so that the five
+// populations leaving through that side's face (side 0: cx = -1, q 9..13;
+// side 1: cx = +1, q 0..4) take the last five slots, in q order, right before
+// the rim; the rim holds the same five populations on the face column's halo
+// rows (k = 0 and k = n+1 for j = 0..m+1, then j = 0 and j = m+1 for
+// k = 1..n), packed after the halo kernels of an x-slab step.  Slots 13..17
+// and the rim are then one contiguous plane message of 5 (m+2)(n+2) values
+// that the stream-collide epilogue has already written: the send buffer of
+// the x-slab plane exchange, with no pack kernel over the plane.
 template <typename S, typename R>
 struct Lat {
     S* pop[Q];
     R* ghost;       // ghost[q*G + gidx]
-    R* xface;       // [2][18][m*n]
+    R* xface;       // [2][18 * m*n + rim]
     R scale, inv_scale;
 };
+
+constexpr int kXfaceSendSlot = 13;  // first of the five outgoing slots
+
+__host__ __device__ __forceinline__ constexpr int xface_slot(int side, int q) {
+    return side ? (q + 18 - 5) % 18 : (q + 18 - 14) % 18;
+}
+__host__ __device__ __forceinline__ int64_t xface_rim_len(const Geo& g) {
+    return 5 * (2 * (int64_t)(g.m + 2) + 2 * (int64_t)g.n);
+}
+__host__ __device__ __forceinline__ int64_t xface_side_stride(const Geo& g) {
+    return 18 * (int64_t)g.m * g.n + xface_rim_len(g);
+}
+// Elements of the whole x-face copy (both sides).
+__host__ __device__ __forceinline__ int64_t xface_elems(const Geo& g) { return 2 * xface_side_stride(g); }
+// Offset of side `side`'s plane message (slots 13..17 and the rim).
+__host__ __device__ __forceinline__ int64_t xface_send_offset(const Geo& g, int side) {
+    return side * xface_side_stride(g) + (int64_t)kXfaceSendSlot * g.m * g.n;
+}
+// Halo-row node (j, k) of the face plane at position p (0 <= p < 2(m+2) + 2n) of one
+// population's rim.
+__host__ __device__ __forceinline__ void xface_rim_node(const Geo& g, int64_t p, int* j, int* k) {
+    if (p < 2 * (int64_t)(g.m + 2)) {
+        *k = p < g.m + 2 ? 0 : g.n + 1;
+        *j = (int)(p < g.m + 2 ? p : p - (g.m + 2));
+    } else {
+        const int64_t e = p - 2 * (int64_t)(g.m + 2);
+        *j = e < g.n ? 0 : g.m + 1;
+        *k = (int)(e < g.n ? e : e - g.n) + 1;
+    }
+}
 
 template <typename S, typename R>
 __device__ __forceinline__ R lat_load(const Lat<S, R>& L, const Geo& g, int q, int i, int j, int k) {
@@ -211,7 +251,8 @@ __device__ __forceinline__ R lat_load(const Lat<S, R>& L, const Geo& g, int q, i
 }
 
 __host__ __device__ __forceinline__ int64_t xface_idx(const Geo& g, int side, int q, int j, int k) {
-    return (int64_t)(side * 18 + q) * ((int64_t)g.m * g.n) + (j - 1) + (int64_t)(k - 1) * g.m;
+    return side * xface_side_stride(g) + (int64_t)xface_slot(side, q) * ((int64_t)g.m * g.n) + (j - 1) +
+           (int64_t)(k - 1) * g.m;
 }
 
 // Load used by the halo kernels: x-face columns from the x-face copy.

@@ -4,14 +4,20 @@ The global lattice lx x ly x lz is cut along x into `world` slabs of nearly
 equal width; slab r holds nodes x0_r .. x0_r + nx_r - 1 on its own GPU.  The
 faces between slabs are flagged EXCHANGE: each step runs
 
-    bounce-back + halo planes          eup_step_boundaries   (every slab)
-    pack the 5 populations leaving     eup_get_x_planes      (both x faces)
+    bounce-back + halo planes          eup_step_boundaries   (every slab; with
+                                         an exchange face it also packs the halo
+                                         rows of the outgoing plane messages)
     stream-collide of x = 2..l-1       eup_step_stream_interior
       meanwhile send/recv to the       torch.distributed (NCCL: device buffers
       neighbours                       on a high-priority stream, ordered by
                                        events; gloo: staged through host memory)
-    unpack into the x halo             eup_set_x_planes
+    unpack into the x halo             eup_set_x_planes_view
     stream-collide of x = 1 and l      eup_step_stream_faces
+
+The messages are sent straight from the handle's x-face copy
+(eup_get_x_planes_view): the stream-collide kernel writes the face columns'
+populations there in its epilogue, so no kernel packs the planes
+(pack="kernel" selects the separate pack kernel, eup_get_x_planes, instead).
 
 Only 5 of the 19 populations cross a face ((ly+2)(lz+2) values each, the y/z
 halo rows included, so corner pulls see this step's y/z boundary values): the
@@ -78,6 +84,14 @@ def plane_size(cfg: Config) -> int:
     return PLANE_POPS * (cfg.ly + 2) * (cfg.lz + 2)
 
 
+class _DeviceArray:
+    """A device address seen by torch as a 1-D tensor (CUDA array interface), no copy."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                         "strides": None, "version": 2}
+
+
 class DistTransport:
     """Moves the face planes between neighbouring ranks with torch.distributed point-to-point
     operations.  NCCL: the buffers live on the GPU and the operations are ordered on the
@@ -110,18 +124,26 @@ class DistTransport:
 class SlabSolver:
     """Slab `rank` of a lattice cut along x, on the current process's GPU."""
 
-    def __init__(self, cfg: Config, rank: int, world: int, transport=None):
+    def __init__(self, cfg: Config, rank: int, world: int, transport=None, pack: str = "view"):
         import torch
+        if pack not in ("view", "kernel"):
+            raise ValueError("pack is 'view' or 'kernel'")
         self.torch = torch
         self.gcfg, self.rank, self.world = cfg, rank, world
         self.x0, self.nx = partition(cfg.lx, world)[rank]
         self.cfg = slab_config(cfg, rank, world)
         self.solver = Solver(self.cfg)
         self.transport = transport
+        self.pack = pack
         dt = torch.float64 if cfg.precision == FP64 else torch.float32
         dev = torch.device("cuda", cfg.device)
         n = plane_size(cfg)
         self.buf = {k: torch.zeros(n, dtype=dt, device=dev) for k in ("send_l", "send_r", "recv_l", "recv_r")}
+        if pack == "view":  # send straight from the x-face copy: these tensors alias the handle's memory
+            ts = "<f8" if dt == torch.float64 else "<f4"
+            for side, key, on in ((0, "send_l", self.has_left), (1, "send_r", self.has_right)):
+                if on:
+                    self.buf[key] = torch.as_tensor(_DeviceArray(self.solver.x_planes_view(side), n, ts), device=dev)
         staged = transport is not None and not getattr(transport, "nccl", True)
         self.host = {k: torch.zeros(n, dtype=dt, pin_memory=True) for k in self.buf} if staged else None
         self.stream = torch.cuda.ExternalStream(self.solver.stream())
@@ -153,16 +175,18 @@ class SlabSolver:
     # ---- one step in halves, for callers that interleave several slabs ----
     def begin(self):
         self.solver.step_boundaries()
-        if self.has_left:
-            self.solver.get_x_planes(0, self.buf["send_l"].data_ptr())
-        if self.has_right:
-            self.solver.get_x_planes(1, self.buf["send_r"].data_ptr())
+        if self.pack == "kernel":
+            if self.has_left:
+                self.solver.get_x_planes(0, self.buf["send_l"].data_ptr())
+            if self.has_right:
+                self.solver.get_x_planes(1, self.buf["send_r"].data_ptr())
 
     def _unpack(self):
+        unpack = self.solver.set_x_planes_view if self.pack == "view" else self.solver.set_x_planes
         if self.has_left:
-            self.solver.set_x_planes(0, self.buf["recv_l"].data_ptr())
+            unpack(0, self.buf["recv_l"].data_ptr())
         if self.has_right:
-            self.solver.set_x_planes(1, self.buf["recv_r"].data_ptr())
+            unpack(1, self.buf["recv_r"].data_ptr())
 
     def end(self):
         self._unpack()
@@ -193,7 +217,7 @@ class SlabSolver:
 
     def exchange_overlapped(self):
         """NCCL exchange on the high-priority stream while the solver's stream runs the interior
-        stream-collide: the exchange waits for the packed planes, the face columns for the
+        stream-collide: the exchange waits for the outgoing planes, the face columns for the
         received ones."""
         torch, b = self.torch, self.buf
         packed = torch.cuda.Event()

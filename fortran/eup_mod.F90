@@ -199,6 +199,20 @@
             type(c_ptr), value        :: src
          end function
 
+         integer(c_int) function eup_get_x_planes_view(h, side, dev) bind(c, name="eup_get_x_planes_view")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: side
+            type(c_ptr)               :: dev           ! out: device address, 5 (m+2)(n+2) reals
+         end function
+
+         integer(c_int) function eup_set_x_planes_view(h, side, src) bind(c, name="eup_set_x_planes_view")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value        :: h
+            integer(c_int32_t), value :: side
+            type(c_ptr), value        :: src
+         end function
+
          integer(c_int) function eup_init_reference(opt, l, m, n, glob, start, periodic, u0, elem_bytes, &
                                                      pops) bind(c, name="eup_init_reference")
             import :: c_int, c_int32_t, c_double, c_ptr

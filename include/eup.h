@@ -240,7 +240,8 @@ int eup_synchronize(eup_handle* h);
 int eup_get_stream(eup_handle* h, void** stream);
 
 /* Number of CUDA kernels the time-step entry points have launched on this
- * handle so far (bounce-back/drag, halo planes, stream-collide). */
+ * handle so far (bounce-back/drag, halo planes, stream-collide, and for an
+ * x slab the plane pack/unpack kernels). */
 int eup_get_launch_count(eup_handle* h, int64_t* launches);
 
 /* Current step counter (itime of the state held on the device). */
@@ -378,6 +379,22 @@ int eup_get_x_planes(eup_handle* h, int32_t side, void* dst);
 /* Writes received planes into the halo: side 0 fills x = 0 with a01..a05 (from
  * the left neighbour's side 1), side 1 fills x = l+1 with a10..a14. */
 int eup_set_x_planes(eup_handle* h, int32_t side, const void* src);
+
+/* The same plane message with no pack kernel: *dev receives a device pointer
+ * into the handle's own x-face copy, where the stream-collide kernel's
+ * epilogue writes the face columns' populations as it produces them (and the
+ * bounce-back keeps them in step) and eup_step_boundaries adds the halo rows
+ * after its halo kernels.  5 (m+2)(n+2) values in the arithmetic type: the
+ * five populations on rows j = 1..m, k = 1..n ((q', (j-1) + m (k-1))), then,
+ * per population, the halo rows k = 0 and k = n+1 (j = 0..m+1) and j = 0 and
+ * j = m+1 (k = 1..n).  Valid, and to be sent, between eup_step_boundaries and
+ * the next eup_step_stream / eup_step_stream_faces, which overwrites it; the
+ * pointer itself is fixed for the handle's life.  Only for an exchange face.
+ * Replaces the pack of CODE/SRC/bcond.comm.packed.F90:60-62 for x. */
+int eup_get_x_planes_view(eup_handle* h, int32_t side, const void** dev);
+/* Writes a received message in that order into the x = 0 (side 0) or x = l+1
+ * (side 1) halo plane, like eup_set_x_planes. */
+int eup_set_x_planes_view(eup_handle* h, int32_t side, const void* src);
 
 /* ---- partial bounce-back and its adjoint ----------------------------------- */
 /* No counterpart in the reference (its solids are all-or-nothing voxels).  A

@@ -32,15 +32,16 @@ def _single(eup, cfg, obs, a, steps, dt):
 
 
 @pytest.mark.parametrize("split", [False, True], ids=["sequential", "interior_then_faces"])
-@pytest.mark.parametrize("prec,world", [("fp32", 3), ("fp64", 2), ("fp16", 4)])
-def test_slabs_in_one_process_equal_single_lattice(eup, require_gpu, prec, world, split):
+@pytest.mark.parametrize("prec,world,pack", [("fp32", 3, "view"), ("fp64", 2, "view"), ("fp16", 4, "view"),
+                                             ("fp32", 3, "kernel"), ("fp16", 2, "kernel")])
+def test_slabs_in_one_process_equal_single_lattice(eup, require_gpu, prec, world, split, pack):
     from euplectella_hpc_b200.slabs import SlabSolver, gather_state, step_in_process
     code, dt = {"fp32": (eup.FP32, np.float32), "fp64": (eup.FP64, np.float64), "fp16": (eup.FP16_DEV, np.float32)}[prec]
     cfg, obs = _case(eup, code)
     a = eup.init_equilibrium(L, M, N, 0.05, 1e-3, 5, dt)
     steps = 30
     ref, f_ref = _single(eup, cfg, obs, a, steps, dt)
-    slabs = [SlabSolver(cfg, r, world) for r in range(world)]
+    slabs = [SlabSolver(cfg, r, world, pack=pack) for r in range(world)]
     try:
         for s in slabs:
             s.set_obstacles(obs)
@@ -94,6 +95,64 @@ def test_slab_guards(eup, require_gpu):
         bad[3, 4, 0] = 1                   # solid next to the rear exchange face
         with pytest.raises(eup.EupError):
             s.set_obstacles(bad)
+        assert s.x_planes_view(0) and s.x_planes_view(1)
+    with eup.Solver(slab_config(cfg, 0, 3)) as s:  # first slab: its x = 0 face is the inlet
+        assert s.x_planes_view(1)
+        with pytest.raises(eup.EupError):
+            s.x_planes_view(0)
+        with pytest.raises(eup.EupError):
+            s.set_x_planes_view(0, s.x_planes_view(1))
+        with pytest.raises(eup.EupError):
+            s.x_planes_view(2)
+
+
+def _view_as_planes(v, m, n):
+    """A plane message in the x-face copy's order -> (5, n+2, m+2) planes [c, k, j]."""
+    out = np.full((5, n + 2, m + 2), np.nan, v.dtype)
+    mn = m * n
+    out[:, 1:-1, 1:-1] = v[:5 * mn].reshape(5, n, m)
+    rim = v[5 * mn:].reshape(5, 2 * (m + 2) + 2 * n)
+    out[:, 0, :] = rim[:, :m + 2]
+    out[:, n + 1, :] = rim[:, m + 2:2 * (m + 2)]
+    out[:, 1:-1, 0] = rim[:, 2 * (m + 2):2 * (m + 2) + n]
+    out[:, 1:-1, m + 1] = rim[:, 2 * (m + 2) + n:]
+    return out
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "fp16", "bf16"])
+def test_plane_view_equals_pack_kernel(eup, require_gpu, prec):
+    """The plane messages read in place from the x-face copy (the stream-collide epilogue's
+    face columns, the halo rows packed by step_boundaries) hold, step after step, the values the
+    separate pack kernel gathers from the lattice, in the view's order."""
+    import torch
+    from euplectella_hpc_b200.slabs import SlabSolver, plane_size
+    code, dt = {"fp32": (eup.FP32, np.float32), "fp64": (eup.FP64, np.float64), "fp16": (eup.FP16_DEV, np.float32),
+                "bf16": (eup.BF16_DEV, np.float32)}[prec]
+    tdt = torch.float64 if prec == "fp64" else torch.float32
+    cfg, obs = _case(eup, code)
+    a = eup.init_equilibrium(L, M, N, 0.05, 1e-3, 5, dt)
+    s = SlabSolver(cfg, 1, 3)  # the middle slab: both x faces exchange
+    n = plane_size(cfg)
+    try:
+        s.set_obstacles(obs)
+        s.upload(a)
+        for _ in range(6):
+            s.begin()
+            for side, key in ((0, "send_l"), (1, "send_r")):
+                packed = torch.empty(n, dtype=tdt, device="cuda")
+                s.solver.get_x_planes(side, packed.data_ptr())
+                s.solver.synchronize()
+                want = packed.cpu().numpy().reshape(5, N + 2, M + 2)
+                got = _view_as_planes(s.buf[key].cpu().numpy(), M, N)
+                assert np.array_equal(got, want), (side, np.argwhere(got != want)[:4])
+                assert np.isfinite(got).all()
+            # close the slab on itself (finite, consistent planes) and finish the step
+            s.buf["recv_l"].copy_(s.buf["send_r"])
+            s.buf["recv_r"].copy_(s.buf["send_l"])
+            torch.cuda.synchronize()
+            s.end()
+    finally:
+        s.solver.close()
 
 
 def _free_port():
