@@ -404,13 +404,15 @@ class Solver:
     def x_planes_view(self, side) -> int:
         """Device address of the plane message of an exchange face inside the handle's x-face
         copy (written by the stream-collide epilogue, halo rows added by step_boundaries):
-        5 (m+2)(n+2) values, the five populations' m x n interior blocks, then their halo rows."""
+        5 (m+2)(n+2) values, the five populations' m x n interior blocks and their halo rows
+        (side 1: blocks then halo rows; side 0: halo rows then blocks)."""
         p = ctypes.c_void_p()
         self._ck(lib.eup_get_x_planes_view(self._h, side, ctypes.byref(p)))
         return p.value
 
     def set_x_planes_view(self, side, dev_ptr):
-        """Write a received message in the x_planes_view order into the x = 0 / x = l+1 halo."""
+        """Write a message from the neighbour's opposite side (its x_planes_view order) into the
+        x = 0 (side 0) / x = l+1 (side 1) halo."""
         self._ck(lib.eup_set_x_planes_view(self._h, side, dev_ptr))
 
     def save_state(self, path, elem_bytes=4):

@@ -823,34 +823,36 @@ __global__ void k_pack_x(Lat<S, R> L, Geo g, int side, R* out) {
 // after the halo kernels wrote them.
 template <typename S, typename R>
 __global__ void k_pack_x_rim(Lat<S, R> L, Geo g, int sides) {
-    const int64_t per = xface_rim_len(g) / 5;  // halo-row nodes of one face plane
+    const int64_t per = g.xr / 5;  // halo-row nodes of one face plane
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 10 * per) return;
-    const int side = (int)(t / (5 * per));
+    if (t >= 2 * g.xr) return;
+    const int side = (int)(t / g.xr);
     if (!((sides >> side) & 1)) return;
-    const int64_t r = t - side * 5 * per;
+    const int64_t r = t - side * g.xr;
     const int c = (int)(r / per);
     int j, k;
     xface_rim_node(g, r - c * per, &j, &k);
     const int q = side ? c : 9 + c;
-    L.xface[side * xface_side_stride(g) + 18 * (int64_t)g.m * g.n + r] = lat_load(L, g, q, side ? g.l : 1, j, k);
+    L.xface[xface_rim_offset(g, side) + r] = lat_load(L, g, q, side ? g.l : 1, j, k);
 }
 
-// Received plane message in the x-face copy's order (five m*n blocks, then the rim)
-// into the x = 0 (side 0, q 0..4) or x = l+1 (side 1, q 9..13) halo plane.
+// A received plane message into the x = 0 (side 0, q 0..4) or x = l+1 (side 1,
+// q 9..13) halo plane.  It left the neighbour's opposite side: into side 0 come
+// the five m*n blocks then the rim, into side 1 the rim then the blocks.
 template <typename S, typename R>
 __global__ void k_unpack_x_view(Lat<S, R> L, Geo g, int side, const R* in) {
-    const int64_t mn = (int64_t)g.m * g.n, per = xface_rim_len(g) / 5;
+    const int64_t mn = g.mn, per = g.xr / 5;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 5 * (mn + per)) return;
+    if (t >= 5 * mn + g.xr) return;
+    const int64_t b = side ? t - g.xr : t;  // position among the blocks (< 0: on the rim)
     int c, j, k;
-    if (t < 5 * mn) {
-        c = (int)(t / mn);
-        const int64_t jk = t - c * mn;
+    if (b >= 0 && b < 5 * mn) {
+        c = (int)(b / mn);
+        const int64_t jk = b - c * mn;
         j = (int)(jk % g.m) + 1;
         k = (int)(jk / g.m) + 1;
     } else {
-        const int64_t r = t - 5 * mn;
+        const int64_t r = side ? t : t - 5 * mn;
         c = (int)(r / per);
         xface_rim_node(g, r - c * per, &j, &k);
     }
@@ -880,7 +882,7 @@ void launch_pack_x(const Lat<S, R>& L, const Geo& g, int side, R* out, cudaStrea
 
 template <typename S, typename R>
 void launch_pack_x_rim(const Lat<S, R>& L, const Geo& g, int sides, cudaStream_t st) {
-    const int64_t work = 2 * xface_rim_len(g);
+    const int64_t work = 2 * g.xr;
     k_pack_x_rim<S, R><<<(unsigned)((work + kTpb - 1) / kTpb), kTpb, 0, st>>>(L, g, sides);
 }
 

@@ -146,6 +146,7 @@ struct Geo {
     int64_t N;       // l*m*n
     int64_t sx, sy, sz;         // face sizes
     int64_t ox0, oxl, oy0, oym, oz0, ozn, G;
+    int64_t mn, xr, xs;  // m*n; one rim of the x-face copy; elements per side (18 m*n + 2 rims)
 
     __host__ __device__ void init(int l_, int m_, int n_) {
         l = l_; m = m_; n = n_;
@@ -156,6 +157,9 @@ struct Geo {
         sz = (int64_t)l * m;
         ox0 = 0; oxl = sx; oy0 = 2 * sx; oym = oy0 + sy; oz0 = oym + sy; ozn = oz0 + sz;
         G = ozn + sz;
+        mn = (int64_t)m * n;
+        xr = 5 * (2 * (int64_t)(m + 2) + 2 * (int64_t)n);
+        xs = 18 * mn + 2 * xr;
     }
     __host__ __device__ __forceinline__ bool interior(int i, int j, int k) const {
         return i >= 1 && i <= l && j >= 1 && j <= m && k >= 1 && k <= n;
@@ -196,16 +200,18 @@ __host__ __device__ __forceinline__ void face_row(const Geo& g, int f, int* j, i
 // produces and the bounce-back kernel keeps it in step, so that halo kernels
 // read these columns coalesced in j instead of with a stride of l elements.
 //
-// Layout per side: 18 slots of m*n values ((j-1) + (k-1)*m), then a rim of
-// 5 * (2(m+2) + 2n) values.  The slots are rotated so that the five
-// populations leaving through that side's face (side 0: cx = -1, q 9..13;
-// side 1: cx = +1, q 0..4) take the last five slots, in q order, right before
-// the rim; the rim holds the same five populations on the face column's halo
-// rows (k = 0 and k = n+1 for j = 0..m+1, then j = 0 and j = m+1 for
-// k = 1..n), packed after the halo kernels of an x-slab step.  Slots 13..17
-// and the rim are then one contiguous plane message of 5 (m+2)(n+2) values
-// that the stream-collide epilogue has already written: the send buffer of
-// the x-slab plane exchange, with no pack kernel over the plane.
+// Layout per side: a rim, 18 slots of m*n values ((j-1) + (k-1)*m), a second
+// rim; each rim holds 5 * (2(m+2) + 2n) values and the two sides are one
+// constant stride apart.  The slot order, the same on both sides, puts the
+// five populations leaving through the x = 1 face (cx = -1, q 9..13) first and
+// those leaving through x = l (cx = +1, q 0..4) last.  Side 0's first rim and
+// side 1's second rim hold these populations on the face column's halo rows
+// (k = 0 and k = n+1 for j = 0..m+1, then j = 0 and j = m+1 for k = 1..n),
+// packed after the halo kernels of an x-slab step; the other two rims are
+// unused.  So side 0's rim + slots 0..4 and side 1's slots 13..17 + rim are
+// each one contiguous plane message of 5 (m+2)(n+2) values that the
+// stream-collide epilogue has already written: the send buffers of the
+// x-slab plane exchange, with no pack kernel over the plane.
 template <typename S, typename R>
 struct Lat {
     S* pop[Q];
@@ -214,22 +220,19 @@ struct Lat {
     R scale, inv_scale;
 };
 
-constexpr int kXfaceSendSlot = 13;  // first of the five outgoing slots
-
-__host__ __device__ __forceinline__ constexpr int xface_slot(int side, int q) {
-    return side ? (q + 18 - 5) % 18 : (q + 18 - 14) % 18;
-}
-__host__ __device__ __forceinline__ int64_t xface_rim_len(const Geo& g) {
-    return 5 * (2 * (int64_t)(g.m + 2) + 2 * (int64_t)g.n);
-}
-__host__ __device__ __forceinline__ int64_t xface_side_stride(const Geo& g) {
-    return 18 * (int64_t)g.m * g.n + xface_rim_len(g);
+// Slot of population q: q 9..13 -> 0..4, q 5..8 -> 5..8, q 14..17 -> 9..12, q 0..4 -> 13..17.
+__host__ __device__ __forceinline__ constexpr int xface_slot(int q) {
+    return q <= 4 ? q + 13 : (q >= 9 && q <= 13) ? q - 9 : (q <= 8 ? q : q - 5);
 }
 // Elements of the whole x-face copy (both sides).
-__host__ __device__ __forceinline__ int64_t xface_elems(const Geo& g) { return 2 * xface_side_stride(g); }
-// Offset of side `side`'s plane message (slots 13..17 and the rim).
+__host__ __device__ __forceinline__ int64_t xface_elems(const Geo& g) { return 2 * g.xs; }
+// Offset of side `side`'s plane message: side 0 = rim then q 9..13, side 1 = q 0..4 then rim.
 __host__ __device__ __forceinline__ int64_t xface_send_offset(const Geo& g, int side) {
-    return side * xface_side_stride(g) + (int64_t)kXfaceSendSlot * g.m * g.n;
+    return side ? g.xs + g.xr + 13 * g.mn : 0;
+}
+// Offset of the rim of side `side`'s plane message.
+__host__ __device__ __forceinline__ int64_t xface_rim_offset(const Geo& g, int side) {
+    return side ? g.xs + g.xr + 18 * g.mn : 0;
 }
 // Halo-row node (j, k) of the face plane at position p (0 <= p < 2(m+2) + 2n) of one
 // population's rim.
@@ -251,8 +254,7 @@ __device__ __forceinline__ R lat_load(const Lat<S, R>& L, const Geo& g, int q, i
 }
 
 __host__ __device__ __forceinline__ int64_t xface_idx(const Geo& g, int side, int q, int j, int k) {
-    return side * xface_side_stride(g) + (int64_t)xface_slot(side, q) * ((int64_t)g.m * g.n) + (j - 1) +
-           (int64_t)(k - 1) * g.m;
+    return side * g.xs + g.xr + (int64_t)xface_slot(q) * g.mn + (j - 1) + (int64_t)(k - 1) * g.m;
 }
 
 // Load used by the halo kernels: x-face columns from the x-face copy.

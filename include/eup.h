@@ -384,16 +384,19 @@ int eup_set_x_planes(eup_handle* h, int32_t side, const void* src);
  * into the handle's own x-face copy, where the stream-collide kernel's
  * epilogue writes the face columns' populations as it produces them (and the
  * bounce-back keeps them in step) and eup_step_boundaries adds the halo rows
- * after its halo kernels.  5 (m+2)(n+2) values in the arithmetic type: the
- * five populations on rows j = 1..m, k = 1..n ((q', (j-1) + m (k-1))), then,
- * per population, the halo rows k = 0 and k = n+1 (j = 0..m+1) and j = 0 and
- * j = m+1 (k = 1..n).  Valid, and to be sent, between eup_step_boundaries and
- * the next eup_step_stream / eup_step_stream_faces, which overwrites it; the
+ * after its halo kernels.  5 (m+2)(n+2) values in the arithmetic type, in two
+ * parts: the blocks, the five populations on rows j = 1..m, k = 1..n
+ * ((q', (j-1) + m (k-1))); and the rim, per population the halo rows k = 0 and
+ * k = n+1 (j = 0..m+1), then j = 0 and j = m+1 (k = 1..n).  Side 1 (x = l,
+ * a01..a05) holds the blocks then the rim, side 0 (x = 1, a10..a14) the rim
+ * then the blocks.  Valid, and to be sent, between eup_step_boundaries and the
+ * next eup_step_stream / eup_step_stream_faces, which overwrites it; the
  * pointer itself is fixed for the handle's life.  Only for an exchange face.
  * Replaces the pack of CODE/SRC/bcond.comm.packed.F90:60-62 for x. */
 int eup_get_x_planes_view(eup_handle* h, int32_t side, const void** dev);
-/* Writes a received message in that order into the x = 0 (side 0) or x = l+1
- * (side 1) halo plane, like eup_set_x_planes. */
+/* Writes a message from the neighbour's opposite side, in that side's order,
+ * into the x = 0 (side 0) or x = l+1 (side 1) halo plane, like
+ * eup_set_x_planes. */
 int eup_set_x_planes_view(eup_handle* h, int32_t side, const void* src);
 
 /* ---- partial bounce-back and its adjoint ----------------------------------- */

@@ -106,12 +106,14 @@ def test_slab_guards(eup, require_gpu):
             s.x_planes_view(2)
 
 
-def _view_as_planes(v, m, n):
-    """A plane message in the x-face copy's order -> (5, n+2, m+2) planes [c, k, j]."""
+def _view_as_planes(v, m, n, side):
+    """A plane message in the x-face copy's order (side 1: blocks then rim; side 0: rim then
+    blocks) -> (5, n+2, m+2) planes [c, k, j]."""
     out = np.full((5, n + 2, m + 2), np.nan, v.dtype)
-    mn = m * n
-    out[:, 1:-1, 1:-1] = v[:5 * mn].reshape(5, n, m)
-    rim = v[5 * mn:].reshape(5, 2 * (m + 2) + 2 * n)
+    mn, nr = m * n, 5 * (2 * (m + 2) + 2 * n)
+    blocks, rim = (v[:5 * mn], v[5 * mn:]) if side else (v[nr:], v[:nr])
+    out[:, 1:-1, 1:-1] = blocks.reshape(5, n, m)
+    rim = rim.reshape(5, 2 * (m + 2) + 2 * n)
     out[:, 0, :] = rim[:, :m + 2]
     out[:, n + 1, :] = rim[:, m + 2:2 * (m + 2)]
     out[:, 1:-1, 0] = rim[:, 2 * (m + 2):2 * (m + 2) + n]
@@ -143,7 +145,7 @@ def test_plane_view_equals_pack_kernel(eup, require_gpu, prec):
                 s.solver.get_x_planes(side, packed.data_ptr())
                 s.solver.synchronize()
                 want = packed.cpu().numpy().reshape(5, N + 2, M + 2)
-                got = _view_as_planes(s.buf[key].cpu().numpy(), M, N)
+                got = _view_as_planes(s.buf[key].cpu().numpy(), M, N, side)
                 assert np.array_equal(got, want), (side, np.argwhere(got != want)[:4])
                 assert np.isfinite(got).all()
             # close the slab on itself (finite, consistent planes) and finish the step
