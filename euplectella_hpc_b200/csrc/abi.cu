@@ -44,6 +44,13 @@ struct eup_handle {
     unsigned int* bc_bar = nullptr; // grid barrier of the single-launch halo kernel: arrivals, generation, timeouts
     void* staging = nullptr;
     size_t staging_bytes = 0;
+    // state transfers: a second staging buffer and a copy stream, so that the host copy of
+    // one population overlaps the scatter (gather) of the previous one; events 0/1: copy of
+    // buffer 0/1 done, 2/3: kernel on buffer 0/1 done
+    void* staging2 = nullptr;
+    size_t staging2_bytes = 0;
+    cudaStream_t xfer = nullptr;
+    cudaEvent_t xev[4] = {nullptr, nullptr, nullptr, nullptr};
     int64_t itime = 0, series_first = 0;
     bool has_state = false;
     double scale = 1.0;
@@ -316,23 +323,22 @@ void fill_xface_dispatch(eup_handle* h) {
 }
 
 template <typename S, typename R, typename T>
-void enqueue_upload_q(eup_handle* h, int q) {
-    launch_scatter<S, R, T>(make_lat<S, R>(h, h->cur), h->g, q, static_cast<const T*>(h->staging), h->d_bad,
-                            h->stream);
+void enqueue_upload_q(eup_handle* h, int q, const void* buf) {
+    launch_scatter<S, R, T>(make_lat<S, R>(h, h->cur), h->g, q, static_cast<const T*>(buf), h->d_bad, h->stream);
 }
 template <typename S, typename R, typename T>
-void enqueue_download_q(eup_handle* h, int q) {
-    launch_gather<S, R, T>(make_lat<S, R>(h, h->cur), h->g, q, static_cast<T*>(h->staging), h->stream);
+void enqueue_download_q(eup_handle* h, int q, void* buf) {
+    launch_gather<S, R, T>(make_lat<S, R>(h, h->cur), h->g, q, static_cast<T*>(buf), h->stream);
 }
 template <typename S, typename R>
-void upload_q(eup_handle* h, int q, int eb) {
-    if (eb == 4) enqueue_upload_q<S, R, float>(h, q);
-    else enqueue_upload_q<S, R, double>(h, q);
+void upload_q(eup_handle* h, int q, int eb, const void* buf) {
+    if (eb == 4) enqueue_upload_q<S, R, float>(h, q, buf);
+    else enqueue_upload_q<S, R, double>(h, q, buf);
 }
 template <typename S, typename R>
-void download_q(eup_handle* h, int q, int eb) {
-    if (eb == 4) enqueue_download_q<S, R, float>(h, q);
-    else enqueue_download_q<S, R, double>(h, q);
+void download_q(eup_handle* h, int q, int eb, void* buf) {
+    if (eb == 4) enqueue_download_q<S, R, float>(h, q, buf);
+    else enqueue_download_q<S, R, double>(h, q, buf);
 }
 template <typename S, typename R>
 void monitor_dispatch(eup_handle* h) {
@@ -376,6 +382,24 @@ int finish_state(eup_handle* h, int64_t itime) {
     else DISPATCH(h, enqueue_drag_only, h);
     CK(h, cudaGetLastError());
     CK(h, cudaStreamSynchronize(h->stream));
+    return EUP_OK;
+}
+
+// The copy stream, its events and the second staging buffer of the state transfers.
+int ensure_xfer(eup_handle* h, size_t bytes) {
+    if (!h->xfer) {
+        CK(h, cudaStreamCreateWithFlags(&h->xfer, cudaStreamNonBlocking));
+        for (auto& e : h->xev) CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if (h->staging2_bytes >= bytes) return EUP_OK;
+    if (h->staging2) {
+        CK(h, cudaStreamSynchronize(h->xfer));
+        cudaFree(h->staging2);
+    }
+    h->staging2 = nullptr;
+    h->staging2_bytes = 0;
+    CK(h, cudaMalloc(&h->staging2, bytes));
+    h->staging2_bytes = bytes;
     return EUP_OK;
 }
 
@@ -551,12 +575,16 @@ int eup_destroy(eup_handle* h) {
     if (!h) return EUP_OK;
     cudaSetDevice(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->xfer) cudaStreamSynchronize(h->xfer);
     drop_graphs(h);
     void* ptrs[] = {h->lat[0], h->lat[1], h->ghost, h->bits, h->blist, h->blinks, h->partials, h->counter,
                     h->series, h->dscratch, h->staging, h->xface, h->d_itime, h->ns, h->d_bad, h->ns_list,
-                    h->bc_bar};
+                    h->bc_bar, h->staging2};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (cudaEvent_t e : h->xev)
+        if (e) cudaEventDestroy(e);
+    if (h->xfer) cudaStreamDestroy(h->xfer);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return EUP_OK;
@@ -776,11 +804,19 @@ int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, in
         if (!pops[q]) return fail(h, EUP_ERR_INVALID_ARG, "eup_upload: null population array");
     const Geo& g = h->g;
     const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * elem_bytes;
-    if ((rc = ensure_staging(h, bytes))) return rc;
+    if ((rc = ensure_staging(h, bytes)) || (rc = ensure_xfer(h, bytes))) return rc;
     if ((rc = begin_upload_check(h))) return rc;
-    for (int q = 0; q < Q; ++q) {
-        CK(h, cudaMemcpyAsync(h->staging, pops[q], bytes, cudaMemcpyHostToDevice, h->stream));
-        DISPATCH(h, upload_q, h, q, elem_bytes);
+    void* buf[2] = {h->staging, h->staging2};
+    CK(h, cudaEventRecord(h->xev[2], h->stream));  // earlier work on the stream may use the buffers
+    CK(h, cudaEventRecord(h->xev[3], h->stream));
+    for (int q = 0; q < Q; ++q) {  // copy of q (copy stream) beside the scatter of q - 1
+        const int b = q & 1;
+        CK(h, cudaStreamWaitEvent(h->xfer, h->xev[2 + b], 0));
+        CK(h, cudaMemcpyAsync(buf[b], pops[q], bytes, cudaMemcpyHostToDevice, h->xfer));
+        CK(h, cudaEventRecord(h->xev[b], h->xfer));
+        CK(h, cudaStreamWaitEvent(h->stream, h->xev[b], 0));
+        DISPATCH(h, upload_q, h, q, elem_bytes, buf[b]);
+        CK(h, cudaEventRecord(h->xev[2 + b], h->stream));
     }
     if ((rc = end_upload_check(h, "eup_upload"))) return rc;
     return finish_state(h, itime);
@@ -798,7 +834,7 @@ int eup_init_state(eup_handle* h, double u_in, double amp, uint64_t seed, int64_
     for (int q = 0; q < Q; ++q) {
         if (eb == 8) launch_init_population<double>(static_cast<double*>(h->staging), g, q, u_in, amp, seed, h->stream);
         else launch_init_population<float>(static_cast<float*>(h->staging), g, q, u_in, amp, seed, h->stream);
-        DISPATCH(h, upload_q, h, q, eb);
+        DISPATCH(h, upload_q, h, q, eb, h->staging);
     }
     if ((rc = end_upload_check(h, "eup_init_state"))) return rc;
     return finish_state(h, itime);
@@ -822,7 +858,7 @@ int eup_save_state(eup_handle* h, const char* path, int32_t elem_bytes) {
     if (!f) out = fail(h, EUP_ERR_IO, std::string("eup_save_state: cannot create ") + path);
     else if (!eup_internal_write_record(f, &it, 4)) out = fail(h, EUP_ERR_IO, "eup_save_state: write failed");
     for (int q = 0; q < Q && out == EUP_OK; ++q) {
-        DISPATCH(h, download_q, h, q, elem_bytes);
+        DISPATCH(h, download_q, h, q, elem_bytes, h->staging);
         cudaError_t e = cudaMemcpyAsync(pinned, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) out = cuda_fail(h, e, "eup_save_state");
@@ -861,7 +897,7 @@ int eup_restore_state(eup_handle* h, const char* path, int32_t elem_bytes) {
         }
         e = cudaMemcpyAsync(h->staging, pinned, bytes, cudaMemcpyHostToDevice, h->stream);
         if (e == cudaSuccess) {
-            DISPATCH(h, upload_q, h, q, elem_bytes);
+            DISPATCH(h, upload_q, h, q, elem_bytes, h->staging);
             e = cudaStreamSynchronize(h->stream);  // the pinned buffer is refilled next
         }
         if (e != cudaSuccess) out = cuda_fail(h, e, "eup_restore_state");
@@ -883,12 +919,21 @@ int eup_download(eup_handle* h, void* const pops[19], int32_t elem_bytes) {
         if (!pops[q]) return fail(h, EUP_ERR_INVALID_ARG, "eup_download: null population array");
     const Geo& g = h->g;
     const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * elem_bytes;
-    if ((rc = ensure_staging(h, bytes))) return rc;
-    for (int q = 0; q < Q; ++q) {
-        DISPATCH(h, download_q, h, q, elem_bytes);
-        CK(h, cudaMemcpyAsync(pops[q], h->staging, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if ((rc = ensure_staging(h, bytes)) || (rc = ensure_xfer(h, bytes))) return rc;
+    void* buf[2] = {h->staging, h->staging2};
+    CK(h, cudaEventRecord(h->xev[0], h->xfer));  // earlier copies may still read the buffers
+    CK(h, cudaEventRecord(h->xev[1], h->xfer));
+    for (int q = 0; q < Q; ++q) {  // gather of q beside the copy of q - 1 (copy stream)
+        const int b = q & 1;
+        CK(h, cudaStreamWaitEvent(h->stream, h->xev[b], 0));
+        DISPATCH(h, download_q, h, q, elem_bytes, buf[b]);
+        CK(h, cudaEventRecord(h->xev[2 + b], h->stream));
+        CK(h, cudaStreamWaitEvent(h->xfer, h->xev[2 + b], 0));
+        CK(h, cudaMemcpyAsync(pops[q], buf[b], bytes, cudaMemcpyDeviceToHost, h->xfer));
+        CK(h, cudaEventRecord(h->xev[b], h->xfer));
     }
     CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->xfer));
     CK(h, cudaStreamSynchronize(h->stream));
     return EUP_OK;
 }

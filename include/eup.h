@@ -185,7 +185,10 @@ int eup_write_obstacles(eup_handle* h, const char* path);
  * restart path (CODE/SRC/restore_raw.F90:43-63).  Sets the step counter.
  * A value that is not finite (NaN, Inf) anywhere in the 19 arrays is
  * EUP_ERR_INVALID_ARG naming the populations; the handle then holds no state
- * (eup_restore_state and eup_init_state check the same way). */
+ * (eup_restore_state and eup_init_state check the same way).  The host copy of
+ * each population overlaps the device-side conversion of the previous one
+ * (two staging buffers, a copy stream of the handle's own): page-locked host
+ * arrays move at the host link's full rate. */
 int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, int64_t itime);
 
 /* The seeded equilibrium state of eup_init_equilibrium generated on the
@@ -212,7 +215,8 @@ int eup_restore_state(eup_handle* h, const char* path, int32_t elem_bytes);
 /* Copies the current state back into 19 haloed host arrays: the interior from
  * the lattice, the halo from the halo shell, exactly what the reference's
  * arrays hold after a step.  Replaces the device-to-host copies of
- * CODE/SRC/diagnostic.F90:47-58,110-120,163-174 and CODE/SRC/bgk3d.F90:153. */
+ * CODE/SRC/diagnostic.F90:47-58,110-120,163-174 and CODE/SRC/bgk3d.F90:153.
+ * Like eup_upload, each population's copy overlaps the gather of the next. */
 int eup_download(eup_handle* h, void* const pops[19], int32_t elem_bytes);
 
 /* ---- time step ------------------------------------------------------------ */
