@@ -403,6 +403,16 @@ int ensure_xfer(eup_handle* h, size_t bytes) {
     return EUP_OK;
 }
 
+// End of a double-buffered state transfer: both streams drained whatever happened, so that
+// no copy touches the caller's host arrays after the call returns; the first error wins.
+int end_transfer(eup_handle* h, cudaError_t e, const char* who) {
+    if (e == cudaSuccess) e = cudaGetLastError();
+    const cudaError_t ex = cudaStreamSynchronize(h->xfer);
+    const cudaError_t es = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = ex != cudaSuccess ? ex : es;
+    return e == cudaSuccess ? EUP_OK : cuda_fail(h, e, who);
+}
+
 int ensure_staging(eup_handle* h, size_t bytes) {
     if (h->staging_bytes >= bytes) return EUP_OK;
     if (h->staging) cudaFree(h->staging);
@@ -807,17 +817,21 @@ int eup_upload(eup_handle* h, const void* const pops[19], int32_t elem_bytes, in
     if ((rc = ensure_staging(h, bytes)) || (rc = ensure_xfer(h, bytes))) return rc;
     if ((rc = begin_upload_check(h))) return rc;
     void* buf[2] = {h->staging, h->staging2};
-    CK(h, cudaEventRecord(h->xev[2], h->stream));  // earlier work on the stream may use the buffers
-    CK(h, cudaEventRecord(h->xev[3], h->stream));
-    for (int q = 0; q < Q; ++q) {  // copy of q (copy stream) beside the scatter of q - 1
+    // earlier work on the stream may use the buffers
+    cudaError_t e = cudaEventRecord(h->xev[2], h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(h->xev[3], h->stream);
+    for (int q = 0; q < Q && e == cudaSuccess; ++q) {  // copy of q (copy stream) beside the scatter of q - 1
         const int b = q & 1;
-        CK(h, cudaStreamWaitEvent(h->xfer, h->xev[2 + b], 0));
-        CK(h, cudaMemcpyAsync(buf[b], pops[q], bytes, cudaMemcpyHostToDevice, h->xfer));
-        CK(h, cudaEventRecord(h->xev[b], h->xfer));
-        CK(h, cudaStreamWaitEvent(h->stream, h->xev[b], 0));
-        DISPATCH(h, upload_q, h, q, elem_bytes, buf[b]);
-        CK(h, cudaEventRecord(h->xev[2 + b], h->stream));
+        e = cudaStreamWaitEvent(h->xfer, h->xev[2 + b], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(buf[b], pops[q], bytes, cudaMemcpyHostToDevice, h->xfer);
+        if (e == cudaSuccess) e = cudaEventRecord(h->xev[b], h->xfer);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(h->stream, h->xev[b], 0);
+        if (e == cudaSuccess) {
+            DISPATCH(h, upload_q, h, q, elem_bytes, buf[b]);
+            e = cudaEventRecord(h->xev[2 + b], h->stream);
+        }
     }
+    if ((rc = end_transfer(h, e, "eup_upload"))) return rc;
     if ((rc = end_upload_check(h, "eup_upload"))) return rc;
     return finish_state(h, itime);
 }
@@ -921,21 +935,21 @@ int eup_download(eup_handle* h, void* const pops[19], int32_t elem_bytes) {
     const size_t bytes = (size_t)(g.l + 2) * (g.m + 2) * (g.n + 2) * elem_bytes;
     if ((rc = ensure_staging(h, bytes)) || (rc = ensure_xfer(h, bytes))) return rc;
     void* buf[2] = {h->staging, h->staging2};
-    CK(h, cudaEventRecord(h->xev[0], h->xfer));  // earlier copies may still read the buffers
-    CK(h, cudaEventRecord(h->xev[1], h->xfer));
-    for (int q = 0; q < Q; ++q) {  // gather of q beside the copy of q - 1 (copy stream)
+    // earlier copies may still read the buffers
+    cudaError_t e = cudaEventRecord(h->xev[0], h->xfer);
+    if (e == cudaSuccess) e = cudaEventRecord(h->xev[1], h->xfer);
+    for (int q = 0; q < Q && e == cudaSuccess; ++q) {  // gather of q beside the copy of q - 1 (copy stream)
         const int b = q & 1;
-        CK(h, cudaStreamWaitEvent(h->stream, h->xev[b], 0));
-        DISPATCH(h, download_q, h, q, elem_bytes, buf[b]);
-        CK(h, cudaEventRecord(h->xev[2 + b], h->stream));
-        CK(h, cudaStreamWaitEvent(h->xfer, h->xev[2 + b], 0));
-        CK(h, cudaMemcpyAsync(pops[q], buf[b], bytes, cudaMemcpyDeviceToHost, h->xfer));
-        CK(h, cudaEventRecord(h->xev[b], h->xfer));
+        e = cudaStreamWaitEvent(h->stream, h->xev[b], 0);
+        if (e == cudaSuccess) {
+            DISPATCH(h, download_q, h, q, elem_bytes, buf[b]);
+            e = cudaEventRecord(h->xev[2 + b], h->stream);
+        }
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(h->xfer, h->xev[2 + b], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(pops[q], buf[b], bytes, cudaMemcpyDeviceToHost, h->xfer);
+        if (e == cudaSuccess) e = cudaEventRecord(h->xev[b], h->xfer);
     }
-    CK(h, cudaGetLastError());
-    CK(h, cudaStreamSynchronize(h->xfer));
-    CK(h, cudaStreamSynchronize(h->stream));
-    return EUP_OK;
+    return end_transfer(h, e, "eup_download");
 }
 
 int eup_step(eup_handle* h, int32_t nsteps) {
