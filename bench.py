@@ -474,7 +474,12 @@ def adjoint_cost(device):
         with E.Solver(cfg) as s:
             s.set_solid_fraction(wl.ns)
             s.upload(a)
+            s.step(3)  # graphs captured outside the timed steps
             fwd_ms = _timed_steps(s, T, torch)[0] * T
+        with E.Solver(cfg) as s:  # warm-up: a short adjoint run loads the kernels it uses
+            s.set_solid_fraction(wl.ns)
+            s.upload(a)
+            s.adjoint(64, 16, 8)
         with E.Solver(cfg) as s:
             s.set_solid_fraction(wl.ns)
             s.upload(a)
@@ -490,6 +495,7 @@ def adjoint_cost(device):
             with E.Solver(cfg) as s:
                 s.set_obstacles((wl.ns > 0.5).astype(np.int32))
                 s.upload(a)
+                s.step(3)
                 plain_ms = _timed_steps(s, T, torch)[0] * T
             row["plain_forward_ms"] = plain_ms
             row["adjoint_over_plain_forward"] = adj_ms / plain_ms

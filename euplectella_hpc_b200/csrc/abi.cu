@@ -1405,7 +1405,8 @@ struct GraphCache {
             e = cudaStreamEndCapture(st, &graph);
             if (e != cudaSuccess) return e;
             cudaGraphExec_t ge = nullptr;
-            e = cudaGraphInstantiate(&ge, graph, 0);
+            // kernels keep the priority of the stream they were captured from
+            e = cudaGraphInstantiate(&ge, graph, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(graph);
             if (e != cudaSuccess) return e;
             it = exec.emplace(key, ge).first;
@@ -1415,6 +1416,29 @@ struct GraphCache {
 };
 struct RevAct {
     int kind, arg;  // advance: steps; snapshot/restore: slot; adjoint: the step t reversed (from state t-1)
+};
+
+// A high-priority second stream and two events: an adjoint step forks its boundary part
+// (halo kernels, boundary-plane nodes, halo transposes) onto it, beside the interior kernel.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    SideStream() = default;
+    SideStream(const SideStream&) = delete;
+    SideStream& operator=(const SideStream&) = delete;
+    ~SideStream() {
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (s) cudaStreamDestroy(s);
+    }
+    cudaError_t create() {
+        int least = 0, greatest = 0;
+        cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+        return e;
+    }
 };
 
 // Reverse steps a+1 .. b with the working state at a (also held in slot_a) and `free` slots.
@@ -1473,6 +1497,8 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     const Phys<R> ph = make_phys<R>(h);
     const R* ns = static_cast<const R*>(h->ns);
     cudaStream_t st = h->stream;
+    SideStream side;
+    CK(h, side.create());
 
     HaloAdjointTables tab;
     std::string why;
@@ -1630,8 +1656,16 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
             const uint64_t key = ((uint64_t)2 << 60) | ((uint64_t)cur << 24) | ((uint64_t)cur_lam << 1) |
                                  (uint64_t)in_window;
             const cudaError_t e_run = cache.run(key, st, graphs, [&] {
-                launch_bc<S, R>(f, g, bc, ph, st, bc_bar(h));  // the halo of step t, from state t-1
-                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st);
+                // the interior nodes need neither the halo nor the boundary part's results: the
+                // boundary part (the halo of step t from state t-1, the boundary-plane nodes, the
+                // halo transposes) runs on the side stream beside them
+                cudaEventRecord(side.fork, st);
+                cudaStreamWaitEvent(side.s, side.fork, 0);
+                launch_bc<S, R>(f, g, bc, ph, side.s, bc_bar(h));
+                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, side.s, kAdjBoundary);
+                cudaEventRecord(side.join, side.s);
+                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjInterior);
+                cudaStreamWaitEvent(st, side.join, 0);
             });
             CK(h, e_run);
             cur_lam ^= 1;

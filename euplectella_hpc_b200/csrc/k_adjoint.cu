@@ -652,14 +652,15 @@ void launch_pbb_step(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, c
 template <typename S, typename R>
 void launch_pbb_adjoint(const Lat<S, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
                         const Lat<R, R>& lam_out, R* gmu, double* grad, R gamma, const HaloAdjointDevice& t,
-                        cudaStream_t st) {
+                        cudaStream_t st, int parts) {
     // resident blocks of 128 per SM the registers are sized for: FP32 arithmetic 6 (80
     // registers), FP64 4
-    if (g.l > 2 && g.m > 2 && g.n > 2) {
+    if ((parts & kAdjInterior) && g.l > 2 && g.m > 2 && g.n > 2) {
         const dim3 grid((unsigned)((g.l - 2 + 127) / 128), (unsigned)(g.m - 2), (unsigned)(g.n - 2));
         k_pbb_adjoint<S, R, sizeof(R) == 4 ? 6 : 4><<<grid, 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu, grad,
                                                                            gamma);
     }
+    if (!(parts & kAdjBoundary)) return;
     const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
     const int nfr = nz * g.m + (g.n > 2 ? (g.n - 2) * ny : 0);
     const int64_t inner_rows = (g.m > 2 && g.n > 2) ? (int64_t)(g.m - 2) * (g.n - 2) : 0;
@@ -681,7 +682,7 @@ void launch_pbb_adjoint(const Lat<S, R>& f, const Geo& g, const Phys<R>& ph, con
                                         cudaStream_t);                                                             \
     template void launch_pbb_adjoint<S, R>(const Lat<S, R>&, const Geo&, const Phys<R>&, const R*,                \
                                            const Lat<R, R>&, const Lat<R, R>&, R*, double*, R,                     \
-                                           const HaloAdjointDevice&, cudaStream_t);
+                                           const HaloAdjointDevice&, cudaStream_t, int);
 EUP_PBB_INST(float, float)
 EUP_PBB_INST(double, double)
 EUP_PBB_INST(__half, float)
