@@ -1390,28 +1390,33 @@ struct GraphCache {
     ~GraphCache() {
         for (auto& kv : exec) cudaGraphExecDestroy(kv.second);
     }
+    // Captures (on st, which may hold pending work) and instantiates the sequence of key.
+    template <typename F>
+    cudaError_t prepare(uint64_t key, cudaStream_t st, F&& enqueue) {
+        if (exec.count(key)) return cudaSuccess;
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        enqueue();
+        e = cudaStreamEndCapture(st, &graph);
+        if (e != cudaSuccess) return e;
+        cudaGraphExec_t ge = nullptr;
+        // kernels keep the priority of the stream they were captured from
+        e = cudaGraphInstantiate(&ge, graph, cudaGraphInstantiateFlagUseNodePriority);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return e;
+        exec.emplace(key, ge);
+        return cudaSuccess;
+    }
     template <typename F>
     cudaError_t run(uint64_t key, cudaStream_t st, bool use, F&& enqueue) {
         if (!use) {
             enqueue();
             return cudaGetLastError();
         }
-        auto it = exec.find(key);
-        if (it == exec.end()) {
-            cudaGraph_t graph = nullptr;
-            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-            if (e != cudaSuccess) return e;
-            enqueue();
-            e = cudaStreamEndCapture(st, &graph);
-            if (e != cudaSuccess) return e;
-            cudaGraphExec_t ge = nullptr;
-            // kernels keep the priority of the stream they were captured from
-            e = cudaGraphInstantiate(&ge, graph, cudaGraphInstantiateFlagUseNodePriority);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) return e;
-            it = exec.emplace(key, ge).first;
-        }
-        return cudaGraphLaunch(it->second, st);
+        const cudaError_t e = prepare(key, st, enqueue);
+        if (e != cudaSuccess) return e;
+        return cudaGraphLaunch(exec.find(key)->second, st);
     }
 };
 struct RevAct {
@@ -1497,8 +1502,11 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     const Phys<R> ph = make_phys<R>(h);
     const R* ns = static_cast<const R*>(h->ns);
     cudaStream_t st = h->stream;
+    // EUP_STEP_VARIANT bit 18: every adjoint step in one stream (the reference order of its
+    // kernels, against which the forked step is tested bit for bit)
+    const bool serial = (h->variant & 262144) != 0;
     SideStream side;
-    CK(h, side.create());
+    if (!serial) CK(h, side.create());
 
     HaloAdjointTables tab;
     std::string why;
@@ -1602,22 +1610,19 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     CK(h, cudaMemcpyAsync(wshell.p, h->ghost, sizeof(R) * shell, cudaMemcpyDeviceToDevice, st));
     CK(h, cudaEventRecord(ev[1], st));
     CK(h, cudaGetLastError());
-    // objective: mean C_d over the last A steps (steps T-A+1 .. T)
-    std::vector<double> fser((size_t)3 * T);
-    CK(h, cudaStreamSynchronize(st));
-    for (int s = 1; s <= T; ++s) {
-        const int64_t pos = (t0 + s) % h->cap;
-        CK(h, cudaMemcpy(&fser[3 * (size_t)(s - 1)], h->series + 3 * pos, sizeof(double) * 3, cudaMemcpyDeviceToHost));
-    }
-    double J = 0.0;
-    for (int s = T - A + 1; s <= T; ++s) J += fser[3 * (size_t)(s - 1)];
-    J *= gamma;
-    if (!std::isfinite(J)) return fail(h, EUP_ERR_DIVERGED, "eup_adjoint_run: forward run diverged");
 
     // ---- reverse sweep: the rest of the schedule ----
+    // Walked twice: first without launching, capturing and instantiating every distinct step
+    // graph while the device still runs the forward sweep, then enqueueing the steps behind it.
+    // The sweep needs nothing from the host's reading of the objective, which comes after.
+    int64_t recomputed = 0;
+    auto reverse = [&](bool dry) -> int {
     int cur = w0;           // buffer holding the working state (state T-1 now)
     int cur_lam = 0;        // lam[cur_lam] = adjoint of the state after the step being reversed
-    int64_t recomputed = 0;
+    auto step = [&](uint64_t key, auto&& enqueue) -> cudaError_t {
+        if (!dry) return cache.run(key, st, graphs, enqueue);
+        return graphs ? cache.prepare(key, st, enqueue) : cudaSuccess;
+    };
     for (size_t a = first_adj; a < acts.size(); ++a) {
         const RevAct act = acts[a];
         if (act.kind == kActAdvance) {
@@ -1627,21 +1632,23 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
                 const int next = (s + 1 == act.arg && target >= 0) ? target : (cur == w0 ? w1 : w0);
                 const Lat<S, R> src = buf_lat(cur), dst = buf_lat(next);
                 const uint64_t key = ((uint64_t)1 << 60) | ((uint64_t)cur << 24) | (uint64_t)next;
-                const cudaError_t e_run = cache.run(key, st, graphs, [&] {
+                const cudaError_t e_run = step(key, [&] {
                     launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
                     launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
                 });
                 CK(h, e_run);
                 cur = next;
-                ++recomputed;
+                if (!dry) ++recomputed;
             }
             if (target >= 0) ++a;  // the store is done
         } else if (act.kind == kActSnapshot) {
             if (cur != act.arg) {  // not reached in these schedules: a store always follows a forward step
-                CK(h, cudaMemcpyAsync(bufs.p + state * act.arg, bufs.p + state * cur, sizeof(S) * state,
-                                      cudaMemcpyDeviceToDevice, st));
-                CK(h, cudaMemcpyAsync(xfaces.p + xfs * act.arg, xfaces.p + xfs * cur, sizeof(R) * xfs,
-                                      cudaMemcpyDeviceToDevice, st));
+                if (!dry) {
+                    CK(h, cudaMemcpyAsync(bufs.p + state * act.arg, bufs.p + state * cur, sizeof(S) * state,
+                                          cudaMemcpyDeviceToDevice, st));
+                    CK(h, cudaMemcpyAsync(xfaces.p + xfs * act.arg, xfaces.p + xfs * cur, sizeof(R) * xfs,
+                                          cudaMemcpyDeviceToDevice, st));
+                }
                 cur = act.arg;
             }
         } else if (act.kind == kActRestore) {
@@ -1655,26 +1662,57 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
             const R gam = in_window ? (R)gamma : R(0);
             const uint64_t key = ((uint64_t)2 << 60) | ((uint64_t)cur << 24) | ((uint64_t)cur_lam << 1) |
                                  (uint64_t)in_window;
-            const cudaError_t e_run = cache.run(key, st, graphs, [&] {
-                // the interior nodes need neither the halo nor the boundary part's results: the
-                // boundary part (the halo of step t from state t-1, the boundary-plane nodes, the
-                // halo transposes) runs on the side stream beside them
+            const cudaError_t e_run = step(key, [&] {
+                if (serial) {
+                    launch_bc<S, R>(f, g, bc, ph, st, bc_bar(h));  // the halo of step t, from state t-1
+                    launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjAll);
+                    return;
+                }
+                // the interior nodes read no halo value and write other slots than the
+                // boundary-plane nodes: the halo of step t (from state t-1) and the boundary-plane
+                // nodes run on the side stream beside them; the halo transposes after both
                 cudaEventRecord(side.fork, st);
                 cudaStreamWaitEvent(side.s, side.fork, 0);
                 launch_bc<S, R>(f, g, bc, ph, side.s, bc_bar(h));
-                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, side.s, kAdjBoundary);
+                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, side.s, kAdjFaces);
                 cudaEventRecord(side.join, side.s);
                 launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjInterior);
                 cudaStreamWaitEvent(st, side.join, 0);
+                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjTransposes);
             });
             CK(h, e_run);
             cur_lam ^= 1;
         }
     }
+    return EUP_OK;
+    };
+    int rc = reverse(true);
+    if (rc == EUP_OK) rc = reverse(false);
+    if (rc != EUP_OK) {
+        cudaStreamSynchronize(st);
+        return rc;
+    }
     CK(h, cudaEventRecord(ev[2], st));
     CK(h, cudaGetLastError());
     CK(h, cudaMemcpyAsync(grad_out, grad.p, sizeof(double) * g.N, cudaMemcpyDeviceToHost, st));
+    // objective: mean C_d over the last A steps (steps T-A+1 .. T), from the series the forward
+    // sweep recorded (the reverse sweep records none): at most two runs of the ring buffer
+    // (A <= its capacity, checked on entry)
+    std::vector<double> fser((size_t)3 * A);
+    {
+        const int64_t first = (t0 + T - A + 1) % h->cap;
+        const int64_t n1 = std::min<int64_t>(A, h->cap - first);
+        CK(h, cudaMemcpyAsync(fser.data(), h->series + 3 * first, sizeof(double) * 3 * n1, cudaMemcpyDeviceToHost,
+                              st));
+        if (n1 < A)
+            CK(h, cudaMemcpyAsync(fser.data() + 3 * n1, h->series, sizeof(double) * 3 * (A - n1),
+                                  cudaMemcpyDeviceToHost, st));
+    }
     CK(h, cudaStreamSynchronize(st));
+    double J = 0.0;
+    for (int s = 0; s < A; ++s) J += fser[3 * (size_t)s];
+    J *= gamma;
+    if (!std::isfinite(J)) return fail(h, EUP_ERR_DIVERGED, "eup_adjoint_run: forward run diverged");
     float fwd_ms = 0.f, rev_ms = 0.f;
     cudaEventElapsedTime(&fwd_ms, ev[0], ev[1]);
     cudaEventElapsedTime(&rev_ms, ev[1], ev[2]);
@@ -1777,6 +1815,8 @@ int eup_adjoint_run(eup_handle* h, const eup_adjoint_config* cfg, double* object
         return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: need 1 <= avg_steps <= nsteps, checkpoints >= 0");
     if (!(h->cfg.cd_rho0 > 0 && h->cfg.cd_uref != 0 && h->cfg.cd_length > 0 && h->cfg.cd_span > 0))
         return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: drag normalisation not set in eup_config");
+    if (cfg->avg_steps > h->cap)
+        return fail(h, EUP_ERR_INVALID_ARG, "eup_adjoint_run: avg_steps exceeds the force history capacity");
     switch (h->prec) {
         case EUP_FP64: return adjoint_run<double, double>(h, cfg, objective, grad_ns, stats);
         case EUP_FP16_DEV: return adjoint_run<__half, float>(h, cfg, objective, grad_ns, stats);

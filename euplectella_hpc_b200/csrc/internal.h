@@ -243,11 +243,14 @@ void launch_pbb_step(const Lat<S, R>& src, const Lat<S, R>& dst, const Geo& g, c
                      const int32_t* ns_list, int64_t ns_count, const Reduce& red, double* series, int64_t cap,
                      int64_t* d_itime, cudaStream_t st);
 // Adjoint of one partial-bounce-back step from state f (its halo shell holding the step's
-// halo values); the adjoint fields lam are in the arithmetic type.  parts: kAdjInterior,
-// the nodes 2..l-1 x 2..m-1 x 2..n-1, which read neither the halo shell nor anything the
-// other part writes, and kAdjBoundary, the boundary-plane nodes and the halo transposes
-// (these need the step's halo values); the two may run on different streams.
-enum { kAdjInterior = 1, kAdjBoundary = 2, kAdjAll = 3 };
+// halo values); the adjoint fields lam are in the arithmetic type.  The adjoint is pushed:
+// node x writes lam_out_q at the node x - c_q it pulled from, each slot once.  parts:
+// kAdjInterior, the nodes 2..l-1 x 2..m-1 x 2..n-1, which read no halo value; kAdjFaces,
+// the boundary-plane nodes (they read the step's halo values and write the halo part gmu);
+// these two write disjoint slots and may run on different streams.  kAdjTransposes adds the
+// halo adjoints back onto the interior slots they were copied from or computed from; it
+// runs after both, since those slots may be ones the interior part writes.
+enum { kAdjInterior = 1, kAdjFaces = 2, kAdjTransposes = 4, kAdjAll = 7 };
 template <typename S, typename R>
 void launch_pbb_adjoint(const Lat<S, R>& f, const Geo& g, const Phys<R>& ph, const R* ns, const Lat<R, R>& lam_in,
                         const Lat<R, R>& lam_out, R* gmu, double* grad, R gamma, const HaloAdjointDevice& t,

@@ -660,13 +660,15 @@ void launch_pbb_adjoint(const Lat<S, R>& f, const Geo& g, const Phys<R>& ph, con
         k_pbb_adjoint<S, R, sizeof(R) == 4 ? 6 : 4><<<grid, 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu, grad,
                                                                            gamma);
     }
-    if (!(parts & kAdjBoundary)) return;
-    const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
-    const int nfr = nz * g.m + (g.n > 2 ? (g.n - 2) * ny : 0);
-    const int64_t inner_rows = (g.m > 2 && g.n > 2) ? (int64_t)(g.m - 2) * (g.n - 2) : 0;
-    const int64_t nitems = (int64_t)nfr * g.l + inner_rows * (g.l == 1 ? 1 : 2);
-    k_pbb_adjoint_faces<S, R><<<(unsigned)((nitems + 127) / 128), 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out, gmu,
-                                                                                 grad, gamma, nfr, nitems);
+    if (parts & kAdjFaces) {
+        const int nz = g.n >= 2 ? 2 : 1, ny = g.m >= 2 ? 2 : 1;
+        const int nfr = nz * g.m + (g.n > 2 ? (g.n - 2) * ny : 0);
+        const int64_t inner_rows = (g.m > 2 && g.n > 2) ? (int64_t)(g.m - 2) * (g.n - 2) : 0;
+        const int64_t nitems = (int64_t)nfr * g.l + inner_rows * (g.l == 1 ? 1 : 2);
+        k_pbb_adjoint_faces<S, R><<<(unsigned)((nitems + 127) / 128), 128, 0, st>>>(f, g, ph, ns, lam_in, lam_out,
+                                                                                     gmu, grad, gamma, nfr, nitems);
+    }
+    if (!(parts & kAdjTransposes)) return;
     if (t.ncopy > 0)
         // small blocks: a few thousand threads still spread over every SM
         k_adj_copy<R><<<(unsigned)((t.ncopy + 63) / 64), 64, 0, st>>>(g, t.copy_key, t.copy_start, t.copy_slot,

@@ -415,7 +415,8 @@ int eup_set_solid_fraction(eup_handle* h, const double* ns);
 
 typedef struct eup_adjoint_config {
     int32_t nsteps;       /* forward steps T from the current state */
-    int32_t avg_steps;    /* objective: mean C_d over the last avg_steps steps */
+    int32_t avg_steps;    /* objective: mean C_d over the last avg_steps steps (at most the
+                             handle's force history, eup_config.series_capacity) */
     int32_t checkpoints;  /* stored states (snapshot slots); 0 selects 64 */
     int32_t reserved;
 } eup_adjoint_config;

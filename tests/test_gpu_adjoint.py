@@ -116,6 +116,34 @@ def test_adjoint_graphs_equal_plain_launches(eup, require_gpu, monkeypatch, prec
     assert np.array_equal(out[0][2], out[1][2])
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_forked_adjoint_step_equals_serial(eup, require_gpu, monkeypatch, prec):
+    """An adjoint step runs its interior nodes beside the halo blocks and boundary-plane nodes
+    (two branches of the step graph), then the halo transposes; it must give the bits of the
+    same kernels in one stream (EUP_STEP_VARIANT bit 18).  On the bench's 192x96x96 channel
+    (inflow, outflow, free-slip y, periodic z: copied and computed halo values whose adjoints are
+    added back onto slots the interior kernel writes), where the kernels are long enough to
+    overlap, with graphs and with plain launches."""
+    from euplectella_hpc_b200 import workloads
+    code, dt = (eup.FP32, np.float32) if prec == "fp32" else (eup.FP64, np.float64)
+    wl = workloads.pbb_cylinder_channel(steps=40, avg_steps=20, precision=code)
+    a = wl.initial_state(dt)
+    out = {}
+    for var in ("262144", "0", "2"):
+        monkeypatch.setenv("EUP_STEP_VARIANT", var)
+        with eup.Solver(wl.cfg) as s:
+            s.set_solid_fraction(wl.ns)
+            s.upload(a)
+            out[var] = s.adjoint(40, 20, checkpoints=6)[:2]
+    J0, g0 = out["262144"]
+    assert np.isfinite(g0).all() and np.abs(g0).max() > 0
+    for var in ("0", "2"):
+        J, g = out[var]
+        assert J == J0, var
+        bad = g != g0
+        assert not bad.any(), (var, int(bad.sum()), float(np.abs(g - g0).max()), float(np.abs(g0).max()))
+
+
 def test_fp32_adjoint_against_fp64_adjoint(eup, require_gpu):
     res = {}
     for code, dt in ((eup.FP64, np.float64), (eup.FP32, np.float32)):
