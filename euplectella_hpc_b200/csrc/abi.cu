@@ -1617,74 +1617,76 @@ int adjoint_run(eup_handle* h, const eup_adjoint_config* ac, double* objective, 
     // The sweep needs nothing from the host's reading of the objective, which comes after.
     int64_t recomputed = 0;
     auto reverse = [&](bool dry) -> int {
-    int cur = w0;           // buffer holding the working state (state T-1 now)
-    int cur_lam = 0;        // lam[cur_lam] = adjoint of the state after the step being reversed
-    auto step = [&](uint64_t key, auto&& enqueue) -> cudaError_t {
-        if (!dry) return cache.run(key, st, graphs, enqueue);
-        return graphs ? cache.prepare(key, st, enqueue) : cudaSuccess;
-    };
-    for (size_t a = first_adj; a < acts.size(); ++a) {
-        const RevAct act = acts[a];
-        if (act.kind == kActAdvance) {
-            // the last step goes straight into the slot the next action stores
-            const int target = (a + 1 < acts.size() && acts[a + 1].kind == kActSnapshot) ? acts[a + 1].arg : -1;
-            for (int s = 0; s < act.arg; ++s) {
-                const int next = (s + 1 == act.arg && target >= 0) ? target : (cur == w0 ? w1 : w0);
-                const Lat<S, R> src = buf_lat(cur), dst = buf_lat(next);
-                const uint64_t key = ((uint64_t)1 << 60) | ((uint64_t)cur << 24) | (uint64_t)next;
+        int cur = w0;           // buffer holding the working state (state T-1 now)
+        int cur_lam = 0;        // lam[cur_lam] = adjoint of the state after the step being reversed
+        auto step = [&](uint64_t key, auto&& enqueue) -> cudaError_t {
+            if (!dry) return cache.run(key, st, graphs, enqueue);
+            return graphs ? cache.prepare(key, st, enqueue) : cudaSuccess;
+        };
+        for (size_t a = first_adj; a < acts.size(); ++a) {
+            const RevAct act = acts[a];
+            if (act.kind == kActAdvance) {
+                // the last step goes straight into the slot the next action stores
+                const int target =
+                    (a + 1 < acts.size() && acts[a + 1].kind == kActSnapshot) ? acts[a + 1].arg : -1;
+                for (int s = 0; s < act.arg; ++s) {
+                    const int next = (s + 1 == act.arg && target >= 0) ? target : (cur == w0 ? w1 : w0);
+                    const Lat<S, R> src = buf_lat(cur), dst = buf_lat(next);
+                    const uint64_t key = ((uint64_t)1 << 60) | ((uint64_t)cur << 24) | (uint64_t)next;
+                    const cudaError_t e_run = step(key, [&] {
+                        launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
+                        launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr,
+                                              st);
+                    });
+                    CK(h, e_run);
+                    cur = next;
+                    if (!dry) ++recomputed;
+                }
+                if (target >= 0) ++a;  // the store is done
+            } else if (act.kind == kActSnapshot) {
+                if (cur != act.arg) {  // not reached in these schedules: a store always follows a forward step
+                    if (!dry) {
+                        CK(h, cudaMemcpyAsync(bufs.p + state * act.arg, bufs.p + state * cur, sizeof(S) * state,
+                                              cudaMemcpyDeviceToDevice, st));
+                        CK(h, cudaMemcpyAsync(xfaces.p + xfs * act.arg, xfaces.p + xfs * cur, sizeof(R) * xfs,
+                                              cudaMemcpyDeviceToDevice, st));
+                    }
+                    cur = act.arg;
+                }
+            } else if (act.kind == kActRestore) {
+                cur = act.arg;  // read in place; forward steps write elsewhere
+            } else {  // adjoint of step t from state t-1
+                const int t = act.arg;
+                const Lat<S, R> f = buf_lat(cur);
+                const Lat<R, R> lin_ = lat_at<R, R>(h, lam.p + state * cur_lam),
+                                lout = lat_at<R, R>(h, lam.p + state * (cur_lam ^ 1));
+                const bool in_window = t > T - A;
+                const R gam = in_window ? (R)gamma : R(0);
+                const uint64_t key = ((uint64_t)2 << 60) | ((uint64_t)cur << 24) | ((uint64_t)cur_lam << 1) |
+                                     (uint64_t)in_window;
                 const cudaError_t e_run = step(key, [&] {
-                    launch_bc<S, R>(src, g, bc, ph, st, bc_bar(h));
-                    launch_pbb_step<S, R>(src, dst, g, ph, ns, h->ns_list, h->ns_count, red, nullptr, 0, nullptr, st);
+                    if (serial) {
+                        launch_bc<S, R>(f, g, bc, ph, st, bc_bar(h));  // the halo of step t, from state t-1
+                        launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjAll);
+                        return;
+                    }
+                    // the interior nodes read no halo value and write other slots than the
+                    // boundary-plane nodes: the halo of step t (from state t-1) and the boundary-plane
+                    // nodes run on the side stream beside them; the halo transposes after both
+                    cudaEventRecord(side.fork, st);
+                    cudaStreamWaitEvent(side.s, side.fork, 0);
+                    launch_bc<S, R>(f, g, bc, ph, side.s, bc_bar(h));
+                    launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, side.s, kAdjFaces);
+                    cudaEventRecord(side.join, side.s);
+                    launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjInterior);
+                    cudaStreamWaitEvent(st, side.join, 0);
+                    launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjTransposes);
                 });
                 CK(h, e_run);
-                cur = next;
-                if (!dry) ++recomputed;
+                cur_lam ^= 1;
             }
-            if (target >= 0) ++a;  // the store is done
-        } else if (act.kind == kActSnapshot) {
-            if (cur != act.arg) {  // not reached in these schedules: a store always follows a forward step
-                if (!dry) {
-                    CK(h, cudaMemcpyAsync(bufs.p + state * act.arg, bufs.p + state * cur, sizeof(S) * state,
-                                          cudaMemcpyDeviceToDevice, st));
-                    CK(h, cudaMemcpyAsync(xfaces.p + xfs * act.arg, xfaces.p + xfs * cur, sizeof(R) * xfs,
-                                          cudaMemcpyDeviceToDevice, st));
-                }
-                cur = act.arg;
-            }
-        } else if (act.kind == kActRestore) {
-            cur = act.arg;  // read in place; forward steps write elsewhere
-        } else {  // adjoint of step t from state t-1
-            const int t = act.arg;
-            const Lat<S, R> f = buf_lat(cur);
-            const Lat<R, R> lin_ = lat_at<R, R>(h, lam.p + state * cur_lam),
-                            lout = lat_at<R, R>(h, lam.p + state * (cur_lam ^ 1));
-            const bool in_window = t > T - A;
-            const R gam = in_window ? (R)gamma : R(0);
-            const uint64_t key = ((uint64_t)2 << 60) | ((uint64_t)cur << 24) | ((uint64_t)cur_lam << 1) |
-                                 (uint64_t)in_window;
-            const cudaError_t e_run = step(key, [&] {
-                if (serial) {
-                    launch_bc<S, R>(f, g, bc, ph, st, bc_bar(h));  // the halo of step t, from state t-1
-                    launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjAll);
-                    return;
-                }
-                // the interior nodes read no halo value and write other slots than the
-                // boundary-plane nodes: the halo of step t (from state t-1) and the boundary-plane
-                // nodes run on the side stream beside them; the halo transposes after both
-                cudaEventRecord(side.fork, st);
-                cudaStreamWaitEvent(side.s, side.fork, 0);
-                launch_bc<S, R>(f, g, bc, ph, side.s, bc_bar(h));
-                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, side.s, kAdjFaces);
-                cudaEventRecord(side.join, side.s);
-                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjInterior);
-                cudaStreamWaitEvent(st, side.join, 0);
-                launch_pbb_adjoint<S, R>(f, g, ph, ns, lin_, lout, gmu.p, grad.p, gam, td, st, kAdjTransposes);
-            });
-            CK(h, e_run);
-            cur_lam ^= 1;
         }
-    }
-    return EUP_OK;
+        return EUP_OK;
     };
     int rc = reverse(true);
     if (rc == EUP_OK) rc = reverse(false);
