@@ -387,9 +387,20 @@ int finish_state(eup_handle* h, int64_t itime) {
 
 // The copy stream, its events and the second staging buffer of the state transfers.
 int ensure_xfer(eup_handle* h, size_t bytes) {
-    if (!h->xfer) {
-        CK(h, cudaStreamCreateWithFlags(&h->xfer, cudaStreamNonBlocking));
-        for (auto& e : h->xev) CK(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (!h->xfer) {  // all or nothing: the handle keeps no half-made set
+        cudaStream_t s = nullptr;
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+        cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        for (auto& x : ev)
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            for (auto& x : ev)
+                if (x) cudaEventDestroy(x);
+            if (s) cudaStreamDestroy(s);
+            return cuda_fail(h, e, "state transfer stream");
+        }
+        h->xfer = s;
+        for (int i = 0; i < 4; ++i) h->xev[i] = ev[i];
     }
     if (h->staging2_bytes >= bytes) return EUP_OK;
     if (h->staging2) {
