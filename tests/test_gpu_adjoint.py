@@ -83,8 +83,12 @@ def test_adjoint_matches_central_differences_fp64(eup, require_gpu):
     assert rel.max() < 1e-3, (ad, fd, rel)
 
 
-def test_adjoint_checkpoint_count_does_not_change_the_gradient(eup, require_gpu):
-    cfg, ns = small_case(eup, eup.FP64)
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "fp16"])
+def test_adjoint_checkpoint_count_does_not_change_the_gradient(eup, require_gpu, prec):
+    """3 stored states (most steps recomputed, without the force) against 16 and against all
+    150 (none recomputed): the recomputed states, and so J and the gradient, are the same bits."""
+    code = {"fp64": eup.FP64, "fp32": eup.FP32, "fp16": eup.FP16_DEV}[prec]
+    cfg, ns = small_case(eup, code)
     a = eup.init_equilibrium(L, M, N, 0.05, 1e-4, 11, np.float64)
     out = []
     for ck in (3, 16, 150):
